@@ -1,0 +1,171 @@
+/*
+ * tgh.h -- the C ABI of the B200-native generalized-harmonic time-stepping path.
+ *
+ * One shared library (libtgh_b200.so, built from treegeneralizedharmonic.jl_b200/csrc)
+ * implements the verbs of TreeGeneralizedHarmonic.jl's stepping path on one GPU:
+ *
+ *   reference verb (TreeGeneralizedHarmonic.jl)          this ABI
+ *   ---------------------------------------------------   -----------------------------
+ *   GHProblem(U, schedule, case; q, t, interior)           tgh_problem_create
+ *     src/evolution.jl:1034-1149
+ *   prepare!(p, u, t)          src/evolution.jl:1349       tgh_prepare
+ *   rhs!(du, p, t; matter)     src/evolution.jl:1386       tgh_rhs
+ *   gh_rhs!(du, u, p, t)       src/evolution.jl:1327       tgh_gh_rhs
+ *   settle!(p, u, t)           src/evolution.jl:1370       tgh_settle
+ *   stage_limit!(u, p, t)      src/stepping.jl:91          tgh_stage_limit
+ *   step_limit!(u, p, t)       src/stepping.jl:97          tgh_step_limit
+ *   max_speed(p, u, t)         src/evolution.jl:1539       tgh_max_speed
+ *   initial_state!(u, p, t)    src/stepping.jl:110         tgh_initial_state
+ *   IRK.step!(gh_integrator(...)) src/stepping.jl:208-225  tgh_rk4_step (plain per-block form)
+ *                                                          tgh_step_batched (fused, graph-captured form)
+ *   error_norms / gh_error_kernel! src/constraints.jl:311-396, 716-792
+ *                                                          tgh_error_norm
+ *
+ * Conventions (all as in the reference):
+ *  - The state vector holds, per block, (N+1)^3 owned points (closed blocks: both face
+ *    planes are owned) for 20 variables: h_ab in 0..9 and Pi_ab in 10..19, packed
+ *    (tt,tx,ty,tz,xx,xy,xz,yy,yz,zz); x fastest, then y, z, variable, block
+ *    (src/evolution.jl:170-178, src/pointwise.jl:22-26).
+ *  - u / du pointers passed to the verbs are DEVICE pointers owned by the caller
+ *    (a CuArray, a torch tensor, ...), holding tgh_state_length() doubles.
+ *  - The problem owns its ghosted working array, the sampled gauge source and all
+ *    scratch; no verb allocates device memory after tgh_problem_create.
+ *  - rhs reads the working array as the last prepare left it; max_speed, settle,
+ *    initial_state and error_norm overwrite it (src/evolution.jl:1376-1384).
+ *  - Every entry point returns a status code and never aborts; tgh_last_error gives
+ *    the message of the last failure on that problem.
+ *  - A problem is bound to one CUDA stream (given at create) and is not thread-safe.
+ */
+#ifndef TGH_H
+#define TGH_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define TGH_NVARS 20
+#define TGH_NC 10
+
+/* status codes (the reference throws ArgumentError with a message instead) */
+enum {
+  TGH_OK = 0,
+  TGH_ERR_ARG = 1,        /* construction checks, src/evolution.jl:1039-1136 */
+  TGH_ERR_NONFINITE = 2,  /* non-finite evolved data, src/evolution.jl:1540-1548 */
+  TGH_ERR_SPEED = 3,      /* speed not finite and positive, src/evolution.jl:1551-1558 */
+  TGH_ERR_RADII = 4,      /* interior radius checks, src/interior.jl:1104-1153 */
+  TGH_ERR_TIMEOUT = 5,    /* a bounded device-side wait gave up */
+  TGH_ERR_CUDA = 6,       /* a CUDA runtime call failed */
+  TGH_ERR_NOMEM = 7
+};
+
+/* backgrounds (SpacetimeMetrics metrics named by the reference's cases) */
+enum {
+  TGH_BG_MINKOWSKI = 0,          /* h = 0 */
+  TGH_BG_GAUGE_WAVE = 1,         /* ds^2 = -H dt^2 + H dx^2 + dy^2 + dz^2, H = 1 - A sin(2pi(x-t)/d) */
+  TGH_BG_SHIFTED_MINKOWSKI = 2,  /* flat space in t^ = t + A w tanh(x/w) */
+  TGH_BG_KERR_SCHILD = 3         /* Kerr-Schild (M, a), spin about +z */
+};
+
+/* gauge source kinds: GHProblem's HASH switch (src/evolution.jl:1099) */
+enum { TGH_GAUGE_NONE = 0, TGH_GAUGE_SAMPLED = 1, TGH_GAUGE_KERR_SCHILD = 2 };
+/* constraint-damping profile (src/gauge.jl:1094-1147) */
+enum { TGH_DAMP_CONSTANT = 0, TGH_DAMP_GAUSSIAN = 1 };
+/* Kreiss-Oliger amplitude (src/gauge.jl:1180-1266) */
+enum { TGH_DISS_CONSTANT = 0, TGH_DISS_HORIZON = 1 };
+/* interior variant (src/interior.jl:178-238): :none, :damped, :frozen, :pasted */
+enum { TGH_INT_NONE = 0, TGH_INT_DAMPED = 1, TGH_INT_FROZEN = 2, TGH_INT_PASTED = 3 };
+/* arithmetic of the right-hand side */
+enum { TGH_PREC_FP64 = 0, TGH_PREC_MIXED = 1 };
+
+typedef struct {
+  int kind;              /* TGH_BG_* */
+  double A, d;           /* gauge wave (A, wavelength d); shifted Minkowski (A, w) */
+  double M, a;           /* Kerr-Schild mass and spin parameter */
+  double boost[3];       /* boost(metric, u): evaluated at Lambda(u) x, the hole moves at -u */
+  double translate[4];   /* translate(metric, (t, x, y, z)), applied after the boost */
+} tgh_background;
+
+/* Everything a GHCase + GHProblem carry that the kernels read
+ * (src/initialdata.jl:158-311, src/evolution.jl:995-1149). */
+typedef struct {
+  int q;                       /* even order 2..8; ghost width G = q/2 + 1 */
+  tgh_background bg;
+  int gauge;                   /* TGH_GAUGE_* */
+  double ks_M;                 /* KerrSchildSource(M, spin, velocity), src/gauge.jl:257-290 */
+  double ks_spin[3];
+  double ks_velocity[3];
+  int damping;                 /* TGH_DAMP_* */
+  double gamma0;               /* ConstantDamping */
+  double damp_near, damp_far, damp_width, damp_c0[3], damp_v[3]; /* GaussianDamping */
+  double gamma2;
+  int dissipation;             /* TGH_DISS_* */
+  double eps_ko;               /* constant epsilon */
+  double eps_out, eps_in, eps_r1, eps_rh, eps_c0[3], eps_v[3];   /* HorizonDissipation */
+  int interior;                /* TGH_INT_* */
+  double int_c0[3], int_v[3];  /* HoleCenter(c0, v) */
+  double r0, r1, rho_max, w_ramp, rho_ramp;
+  int precision;               /* TGH_PREC_*: FP64, or FP32 offset-metric stencils + algebra */
+} tgh_config;
+
+/* A forest's leaves: closed vertex-centered blocks of N cells per edge (N+1 points).
+ * Level l has spacing h0 / 2^l; a block's points sit at lo + (corner + i) * h_l,
+ * i = 0..N, corner in the level's cell index space (a multiple of N).
+ * The leaves tile the domain [lo, lo + cells0 * h0]. */
+typedef struct {
+  int N;
+  int nblocks;
+  double lo[3];
+  double h0;
+  int cells0[3];               /* level-0 domain extent in cells per axis */
+  int periodic[3];
+  const int32_t* level;        /* [nblocks] */
+  const int32_t* corner;       /* [3 * nblocks] */
+} tgh_mesh;
+
+typedef struct tgh_problem tgh_problem;
+
+/* --- construction (GHProblem, src/evolution.jl:1034-1149) --- */
+int tgh_problem_create(const tgh_config* cfg, const tgh_mesh* mesh, void* cuda_stream,
+                       int margin_check, tgh_problem** out);
+void tgh_problem_destroy(tgh_problem* p);
+const char* tgh_last_error(const tgh_problem* p);
+/* doubles in one state vector: (N+1)^3 * 20 * nblocks */
+size_t tgh_state_length(const tgh_problem* p);
+/* doubles in the ghosted working array: (N+2G+1)^3 * 20 * nblocks */
+size_t tgh_work_length(const tgh_problem* p);
+/* copy the working array (device to device) for inspection */
+int tgh_copy_work(tgh_problem* p, double* dst);
+
+/* --- the verbs (src/evolution.jl:1327-1390, src/stepping.jl:91-125) --- */
+int tgh_prepare(tgh_problem* p, const double* u, double t);
+/* matter: nullable device pointer, 10 values per owned point in state layout
+ * (rho, S_x, S_y, S_z, S_xx, S_xy, S_xz, S_yy, S_yz, S_zz); the GH-3 adapter
+ * of src/evolution.jl:1288-1316 sampled at the owned points. */
+int tgh_rhs(tgh_problem* p, double* du, double t, const double* matter);
+int tgh_gh_rhs(tgh_problem* p, double* du, const double* u, double t, const double* matter);
+int tgh_settle(tgh_problem* p, double* u, double t);
+int tgh_stage_limit(tgh_problem* p, double* u, double t);
+int tgh_step_limit(tgh_problem* p, double* u, double t);
+int tgh_max_speed(tgh_problem* p, const double* u, double t, double* lambda);
+int tgh_initial_state(tgh_problem* p, double* u, double t);
+
+/* --- one classical RK4 step (IMEXRungeKutta RK4 via gh_integrator, src/stepping.jl:208-225) ---
+ * plain form: per stage one ghost fill, one right-hand-side launch, one stage update */
+int tgh_rk4_step(tgh_problem* p, double* u, double t, double dt);
+/* batched form: the state stays ghosted on the device; each stage is one fill launch and
+ * one right-hand-side launch with the RK4 epilogue fused in; nsteps steps are captured
+ * once as a CUDA graph and replayed. u is read before the first step and written after
+ * the last. */
+int tgh_step_batched(tgh_problem* p, double* u, double t, double dt, int nsteps);
+
+/* --- analysis (src/constraints.jl:311-396, 716-792) ---
+ * masked, volume-weighted L2 and max of |u - u_exact| over the evolved primaries */
+int tgh_error_norm(tgh_problem* p, const double* u, double t, double* l2, double* linf);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,946 @@
+// TEST INFRASTRUCTURE: the CPU oracle of the generalized-harmonic stepping path.
+// Only tests/, __graft_entry__.smoke() and bench.py's cpu_baseline leg may load
+// liboracle.so (through ctypes); the product library never links or calls it.
+//
+// A plain FP64 restatement of the reference's algorithm:
+//   gh_rhs_kernel! / gh_rhs_point! / gh_rhs_head / _dth / gh_rhs_pi   src/evolution.jl:258-695
+//   axis_stencil, mixed_stencil (summation order)                     src/evolution.jl:192-219
+//   host_rhs_at (the expanded reference spelling)                     test/evolution_tests.jl:37-89
+//   rhs_scale                                                         test/evolution_tests.jl:97-108
+//   gh_speed_kernel!, max_speed(p,u,t)                                src/evolution.jl:932-949, 1539-1560
+//   gh_error_kernel!, masked volume-weighted L2                       src/constraints.jl:311-396, 716-792
+//   sample_gauge_source!, gauge_at                                    src/gauge.jl:156-212
+//   initial_state!, stage_limit!, gh_paste_kernel!                    src/stepping.jl:91-115, src/evolution.jl:888-905
+// and of the un-vendored packages under it (no exact pin; compat bounds only):
+//   TreeAMR 0.3: closed vertex-centered blocks, scatter!, fill_ghosts! (same-level copies
+//     from the primary copy, restriction by injection, the Dirichlet CellBoundary hook,
+//     tensor-product Lagrange prolongation of order p = q + 2, coarsest level first),
+//     semantics from CODE.md:406-466, 713-777 of the reference. The fill is written here as
+//     a recursive definition of the value at any lattice point of any level.
+//   IMEXRungeKutta 1.2: classical RK4 with the limiter on the three stage values and the
+//     step's result (CODE.md:3415-3434); the accumulation order is this oracle's choice.
+#include <omp.h>
+
+#include <cmath>
+#include <cstdint>
+#include <cstring>
+#include <limits>
+#include <type_traits>
+#include <stdexcept>
+#include <string>
+#include <unordered_map>
+#include <vector>
+
+#include "physics.hpp"
+#include "pointwise.hpp"
+#include "spacetime.hpp"
+#include "stencils.hpp"
+
+namespace orc {
+
+static const int NV = 20;
+
+struct Problem {
+  tgh_config cfg;
+  int q, G, N, N1, W, nb, maxlevel = 0;
+  double lo[3], h0;
+  int cells0[3], periodic[3];
+  std::vector<int> level, corner;                     // per leaf
+  std::vector<std::unordered_map<int64_t, int>> lut;  // per level: block coordinate -> leaf
+  Stencils st;
+  std::vector<double> wP;  // prolongation weights at the half-way point (p = q + 2 points)
+  Interior in;
+  Profiles pr;
+  KSSource ks;
+  bool diss = false;
+  std::vector<double> work, Hsrc;
+  std::vector<double> ustate;  // the state the last prepare scattered
+  double t_prep = 0.0;
+  std::string err;
+
+  explicit Problem(int q_) : st(q_) {}
+  size_t npt_state() const { return (size_t)N1 * N1 * N1; }
+  size_t npt_work() const { return (size_t)W * W * W; }
+  double spacing(int l) const { return std::ldexp(h0, -l); }
+  int64_t key(int bx, int by, int bz) const {
+    return ((int64_t)bx * 1048576 + by) * 1048576 + bz;
+  }
+  void position(int l, const int64_t n[3], double x[3]) const {
+    double h = spacing(l);
+    for (int d = 0; d < 3; ++d) x[d] = lo[d] + (double)n[d] * h;
+  }
+};
+
+// ---- the primary owner of a lattice point: finest level first, lower face first ----
+static bool find_owner(const Problem& P, int l, const int64_t nin[3], int& leaf, int loc[3]) {
+  for (int k = P.maxlevel; k >= l; --k) {
+    int64_t m[3], per[3];
+    for (int d = 0; d < 3; ++d) {
+      m[d] = nin[d] << (k - l);
+      per[d] = (int64_t)P.cells0[d] << k;
+    }
+    int64_t cand[3][2];
+    int nc[3];
+    for (int d = 0; d < 3; ++d) {
+      int64_t c = m[d] >= 0 ? m[d] / P.N : -((-m[d] + P.N - 1) / P.N);
+      nc[d] = 0;
+      cand[d][nc[d]++] = c;
+      if (m[d] % P.N == 0) cand[d][nc[d]++] = c - 1;
+      (void)per;
+    }
+    for (int iz = 0; iz < nc[2]; ++iz)
+      for (int iy = 0; iy < nc[1]; ++iy)
+        for (int ix = 0; ix < nc[0]; ++ix) {
+          auto it = P.lut[k].find(P.key((int)cand[0][ix], (int)cand[1][iy], (int)cand[2][iz]));
+          if (it == P.lut[k].end()) continue;
+          leaf = it->second;
+          for (int d = 0; d < 3; ++d) loc[d] = (int)(m[d] - P.corner[3 * leaf + d]);
+          return true;
+        }
+  }
+  return false;
+}
+
+static void hook_value(const Problem& P, double t, const double x[3], double out[NV]) {
+  double xc[3], dh[3][NC], dg[NC];
+  P.in.core_position(t, x, xc);
+  background_state(P.cfg.bg, t, xc, out, out + NC, dh, dg);
+}
+
+// The value of all 20 variables at lattice point n of level l, as a filled working
+// array holds it: the hook outside the domain, the primary copy where a leaf of this or a
+// finer level owns the point (injection from the finer one), and otherwise the
+// tensor-product Lagrange prolongation of the next coarser level (x summed innermost).
+static void value20(const Problem& P, const std::vector<double>& u, double t, int l,
+                    const int64_t nin[3], double out[NV]) {
+  int64_t n[3];
+  for (int d = 0; d < 3; ++d) {
+    n[d] = nin[d];
+    int64_t per = (int64_t)P.cells0[d] << l;
+    if (P.periodic[d]) {
+      n[d] %= per;
+      if (n[d] < 0) n[d] += per;
+    }
+  }
+  for (int d = 0; d < 3; ++d) {
+    int64_t per = (int64_t)P.cells0[d] << l;
+    if (!P.periodic[d] && (n[d] < 0 || n[d] > per)) {
+      double x[3];
+      P.position(l, n, x);
+      hook_value(P, t, x, out);
+      return;
+    }
+  }
+  int leaf, loc[3];
+  if (find_owner(P, l, n, leaf, loc)) {
+    size_t base = (size_t)leaf * NV * P.npt_state() + loc[0] + P.N1 * (loc[1] + (size_t)P.N1 * loc[2]);
+    for (int v = 0; v < NV; ++v) out[v] = u[base + v * P.npt_state()];
+    return;
+  }
+  if (l == 0) throw std::runtime_error("lattice point not covered by the forest");
+  // prolongation from level l-1
+  int64_t idx[3][16];
+  double w[3][16];
+  int cnt[3];
+  const int p = (int)P.wP.size();
+  for (int d = 0; d < 3; ++d) {
+    if (n[d] % 2 == 0) {
+      cnt[d] = 1;
+      idx[d][0] = n[d] / 2;
+      w[d][0] = 1.0;
+    } else {
+      int64_t base = (n[d] - 1) / 2 - (p / 2 - 1);
+      cnt[d] = p;
+      for (int k = 0; k < p; ++k) {
+        idx[d][k] = base + k;
+        w[d][k] = P.wP[k];
+      }
+    }
+  }
+  double sz[NV];
+  for (int v = 0; v < NV; ++v) sz[v] = 0.0;
+  for (int kz = 0; kz < cnt[2]; ++kz) {
+    double sy[NV];
+    for (int v = 0; v < NV; ++v) sy[v] = 0.0;
+    for (int ky = 0; ky < cnt[1]; ++ky) {
+      double sx[NV];
+      for (int v = 0; v < NV; ++v) sx[v] = 0.0;
+      for (int kx = 0; kx < cnt[0]; ++kx) {
+        int64_t m[3] = {idx[0][kx], idx[1][ky], idx[2][kz]};
+        double c[NV];
+        value20(P, u, t, l - 1, m, c);
+        for (int v = 0; v < NV; ++v) sx[v] = kx == 0 ? w[0][kx] * c[v] : sx[v] + w[0][kx] * c[v];
+      }
+      for (int v = 0; v < NV; ++v) sy[v] = ky == 0 ? w[1][ky] * sx[v] : sy[v] + w[1][ky] * sx[v];
+    }
+    for (int v = 0; v < NV; ++v) sz[v] = kz == 0 ? w[2][kz] * sy[v] : sz[v] + w[2][kz] * sy[v];
+  }
+  for (int v = 0; v < NV; ++v) out[v] = sz[v];
+}
+
+// prepare!: scatter + fill_ghosts! with the hook at t (src/evolution.jl:1349-1357)
+static void prepare(Problem& P, const double* u, double t) {
+  size_t L = P.npt_state() * NV * P.nb;
+  P.ustate.assign(u, u + L);
+  P.t_prep = t;
+  P.work.assign(P.npt_work() * NV * P.nb, 0.0);
+#pragma omp parallel for schedule(dynamic)
+  for (int b = 0; b < P.nb; ++b) {
+    const int l = P.level[b];
+    double vals[NV];
+    for (int k = 0; k < P.W; ++k)
+      for (int j = 0; j < P.W; ++j)
+        for (int i = 0; i < P.W; ++i) {
+          int64_t n[3] = {(int64_t)P.corner[3 * b] + i - P.G, (int64_t)P.corner[3 * b + 1] + j - P.G,
+                          (int64_t)P.corner[3 * b + 2] + k - P.G};
+          value20(P, P.ustate, t, l, n, vals);
+          size_t base = (size_t)b * NV * P.npt_work() + i + P.W * (j + (size_t)P.W * k);
+          for (int v = 0; v < NV; ++v) P.work[base + v * P.npt_work()] = vals[v];
+        }
+  }
+}
+
+// ---- the right-hand side at one owned point (src/evolution.jl:258-388, 448-695) ----
+struct PointCtx {
+  const double* wk;  // this block's working array
+  size_t sv;         // per-variable stride
+  int st[3];         // per-axis strides
+  size_t var;        // the point's linear index
+};
+
+template <class T = double>
+static inline T axis_stencil(const std::vector<double>& w, const double* wk, size_t base, long stride) {
+  const int n = (int)w.size(), r = (n - 1) / 2;
+  T s = T(w[0]) * T(wk[base + (long)(-r) * stride]);
+  for (int k = 1; k < n; ++k) s = s + T(w[k]) * T(wk[base + (long)(k - r) * stride]);
+  return s;
+}
+template <class T = double>
+static inline T mixed_stencil(const std::vector<double>& w, const double* wk, size_t base, long s1, long s2) {
+  const int n = (int)w.size(), r = (n - 1) / 2;
+  T outer = T(0.0);
+  for (int a = 0; a < n; ++a) {
+    T inner = T(w[0]) * T(wk[base + (long)(a - r) * s1 + (long)(-r) * s2]);
+    for (int e = 1; e < n; ++e) inner = inner + T(w[e]) * T(wk[base + (long)(a - r) * s1 + (long)(e - r) * s2]);
+    outer = a == 0 ? T(w[0]) * inner : outer + T(w[a]) * inner;
+  }
+  return outer;
+}
+
+template <class T>
+static void gauge_at_point(const Problem& P, int b, const int I[3], const T* h, const T* dth,
+                           const T* const dh[3], T Hl[4], T dHl[4][4]) {
+  if (P.cfg.gauge == TGH_GAUGE_NONE) {
+    for (int a = 0; a < 4; ++a) {
+      Hl[a] = T(0.0);
+      for (int c = 0; c < 4; ++c) dHl[a][c] = T(0.0);
+    }
+  } else if (P.cfg.gauge == TGH_GAUGE_SAMPLED) {
+    size_t o = (size_t)b * NV * P.npt_state() + I[0] + P.N1 * (I[1] + (size_t)P.N1 * I[2]);
+    for (int a = 0; a < 4; ++a) Hl[a] = T(P.Hsrc[o + a * P.npt_state()]);
+    for (int k = 0; k < 16; ++k) dHl[k % 4][k / 4] = T(P.Hsrc[o + (4 + k) * P.npt_state()]);
+  } else {
+    if constexpr (std::is_same<T, double>::value) {
+      algebraic_gauge_source(P.ks, h, dth, dh, Hl, dHl);
+    } else {
+      throw std::runtime_error("op counting covers the none and sampled gauge sources");
+    }
+  }
+}
+
+// F(u) at one owned point as two vectors (gh_rhs_at_point, src/evolution.jl:423-435)
+template <class T>
+static void rhs_at_point(const Problem& P, const PointCtx& c, int b, const int I[3], const double x[3],
+                         double t, const double* matter, T dth_out[NC], T dtPi_out[NC]) {
+  const double h = P.spacing(P.level[b]);
+  const T inv_h = T(1.0) / T(h);
+  const T inv_h2 = inv_h * inv_h;
+  const T g0 = T(P.pr.damping_rate(t, x));
+  const T eh = T(P.pr.dissipation_rate(t, x)) * inv_h;
+  const double* wk = c.wk;
+  T hv[NC], Pv[NC], dhs[3][NC];
+  for (int v = 0; v < NC; ++v) {
+    hv[v] = T(wk[c.var + v * c.sv]);
+    Pv[v] = T(wk[c.var + (NC + v) * c.sv]);
+  }
+  for (int d = 0; d < 3; ++d)
+    for (int v = 0; v < NC; ++v) dhs[d][v] = inv_h * axis_stencil<T>(P.st.w1, wk, c.var + v * c.sv, c.st[d]);
+  const T* dh[3] = {dhs[0], dhs[1], dhs[2]};
+  Coef<T> C;
+  metric_quantities(hv, C);
+  const T a_div = C.alpha / C.sqrtg;
+  T dth[NC];
+  for (int v = 0; v < NC; ++v) {
+    T s = C.beta[0] * dh[0][v] + C.beta[1] * dh[1][v] + C.beta[2] * dh[2][v] + a_div * Pv[v];
+    if (P.diss) {
+      size_t bh = c.var + v * c.sv;
+      s = s + eh * (axis_stencil<T>(P.st.wD, wk, bh, c.st[0]) + axis_stencil<T>(P.st.wD, wk, bh, c.st[1]) +
+                    axis_stencil<T>(P.st.wD, wk, bh, c.st[2]));
+    }
+    dth[v] = s;
+  }
+  T Hl[4], dHl[4][4];
+  gauge_at_point<T>(P, b, I, hv, dth, dh, Hl, dHl);
+  T msrc[NC];
+  gh_node_source_lean(C, dth, dh, Hl, dHl, g0, T(P.cfg.gamma2), msrc);
+  if constexpr (std::is_same<T, double>::value) if (matter) {
+    size_t o = (size_t)b * 10 * P.npt_state() + I[0] + P.N1 * (I[1] + (size_t)P.N1 * I[2]);
+    double m[10];
+    for (int k = 0; k < 10; ++k) m[k] = matter[o + k * P.npt_state()];
+    double S3[3] = {m[1], m[2], m[3]};
+    double Sij[3][3] = {{m[4], m[5], m[6]}, {m[5], m[7], m[8]}, {m[6], m[8], m[9]}};
+    double ms[NC];
+    matter_source(C, m[0], S3, Sij, ms);
+    for (int v = 0; v < NC; ++v) msrc[v] = msrc[v] + ms[v];
+  }
+  T am = C.alpha * C.sqrtg;
+  T A[3][3];
+  for (int i = 0; i < 3; ++i)
+    for (int j = 0; j < 3; ++j) A[i][j] = am * C.gamu[i][j];
+  T divb, divA[3];
+  metric_divergences(C, dh, divb, divA);
+  for (int v = 0; v < NC; ++v) dth_out[v] = dth[v];
+  // gh_rhs_pi, one component at a time (src/evolution.jl:324-354)
+  for (int v = 0; v < NC; ++v) {
+    size_t bh = c.var + v * c.sv, bP = bh + NC * c.sv;
+    T Pi_v = T(wk[bP]);
+    T d1 = inv_h * axis_stencil<T>(P.st.w1, wk, bh, c.st[0]);
+    T d2 = inv_h * axis_stencil<T>(P.st.w1, wk, bh, c.st[1]);
+    T d3 = inv_h * axis_stencil<T>(P.st.w1, wk, bh, c.st[2]);
+    T p1 = inv_h * axis_stencil<T>(P.st.w1, wk, bP, c.st[0]);
+    T p2 = inv_h * axis_stencil<T>(P.st.w1, wk, bP, c.st[1]);
+    T p3 = inv_h * axis_stencil<T>(P.st.w1, wk, bP, c.st[2]);
+    T s = C.beta[0] * p1 + C.beta[1] * p2 + C.beta[2] * p3 + divb * Pi_v + divA[0] * d1 +
+               divA[1] * d2 + divA[2] * d3;
+    s = s + (A[0][0] * (inv_h2 * axis_stencil<T>(P.st.w2, wk, bh, c.st[0])) +
+             A[1][1] * (inv_h2 * axis_stencil<T>(P.st.w2, wk, bh, c.st[1])) +
+             A[2][2] * (inv_h2 * axis_stencil<T>(P.st.w2, wk, bh, c.st[2])));
+    T dxy = inv_h2 * mixed_stencil<T>(P.st.w1, wk, bh, c.st[0], c.st[1]);
+    T dxz = inv_h2 * mixed_stencil<T>(P.st.w1, wk, bh, c.st[0], c.st[2]);
+    T dyz = inv_h2 * mixed_stencil<T>(P.st.w1, wk, bh, c.st[1], c.st[2]);
+    s = s + T(2.0) * (A[0][1] * dxy + A[0][2] * dxz + A[1][2] * dyz);
+    if (P.diss)
+      s = s + eh * (axis_stencil<T>(P.st.wD, wk, bP, c.st[0]) + axis_stencil<T>(P.st.wD, wk, bP, c.st[1]) +
+                    axis_stencil<T>(P.st.wD, wk, bP, c.st[2]));
+    dtPi_out[v] = s + msrc[v];
+  }
+}
+
+// gh_rhs_point! (src/evolution.jl:448-695), the sphere interior's branches
+static void rhs_point(const Problem& P, int b, const int I[3], double t, const double* matter, double out[NV]) {
+  PointCtx c;
+  c.wk = P.work.data() + (size_t)b * NV * P.npt_work();
+  c.sv = P.npt_work();
+  c.st[0] = 1;
+  c.st[1] = P.W;
+  c.st[2] = P.W * P.W;
+  c.var = (size_t)(I[0] + P.G) + P.W * ((size_t)(I[1] + P.G) + (size_t)P.W * (I[2] + P.G));
+  int64_t n[3] = {(int64_t)P.corner[3 * b] + I[0], (int64_t)P.corner[3 * b + 1] + I[1],
+                  (int64_t)P.corner[3 * b + 2] + I[2]};
+  double x[3];
+  P.position(P.level[b], n, x);
+  if (P.in.variant == TGH_INT_NONE) {
+    rhs_at_point(P, c, b, I, x, t, matter, out, out + NC);
+    return;
+  }
+  const Interior& ia = P.in;
+  double r = ia.radius(t, x);
+  if (ia.is_frozen(r)) {
+    if (ia.core_follows()) {
+      double rho = ia.core_rate(), dl = ia.layer_rate_step();
+      double xc[3], hd[NC], Pd[NC], dhd[3][NC], dgd[NC], dthd[NC], dtPd[NC], hu[NC], dhr[NC];
+      ia.core_position(t, x, xc);
+      background_state(P.cfg.bg, t, xc, hd, Pd, dhd, dgd);
+      core_target_rate(ia, P.cfg.bg, t, x, dl, dthd, dtPd);
+      for (int v = 0; v < NC; ++v) hu[v] = c.wk[c.var + v * c.sv];
+      core_relaxation_rate(hu, hd, rho, dthd, dhr);
+      for (int v = 0; v < NC; ++v) {
+        out[v] = dhr[v];
+        out[NC + v] = dtPd[v] - rho * (c.wk[c.var + (NC + v) * c.sv] - Pd[v]);
+      }
+    } else {
+      for (int v = 0; v < NV; ++v) out[v] = 0.0;
+    }
+    return;
+  }
+  double F[NV];
+  rhs_at_point(P, c, b, I, x, t, matter, F, F + NC);
+  if (ia.is_outside(r)) {
+    for (int v = 0; v < NV; ++v) out[v] = F[v];
+    return;
+  }
+  double w, rho;
+  ia.profiles(r, w, rho);
+  if (ia.core_follows()) {
+    double hm[NC], Pm[NC], dthm[NC], dtPm[NC];
+    background_state_rate(P.cfg.bg, t, x, ia.layer_rate_step(), hm, Pm, dthm, dtPm);
+    double om = 1.0 - w;
+    for (int v = 0; v < NC; ++v) {
+      out[v] = w * F[v] + om * dthm[v] - rho * (c.wk[c.var + v * c.sv] - hm[v]);
+      out[NC + v] = w * F[NC + v] + om * dtPm[v] - rho * (c.wk[c.var + (NC + v) * c.sv] - Pm[v]);
+    }
+  } else {
+    double he[NC], Pe[NC], dh[3][NC], dg[NC];
+    background_state(P.cfg.bg, t, x, he, Pe, dh, dg);
+    for (int v = 0; v < NC; ++v) {
+      out[v] = w * F[v] - rho * (c.wk[c.var + v * c.sv] - he[v]);
+      out[NC + v] = w * F[NC + v] - rho * (c.wk[c.var + (NC + v) * c.sv] - Pe[v]);
+    }
+  }
+}
+
+static void rhs(Problem& P, double* du, double t, const double* matter) {
+  const size_t S = P.npt_state();
+#pragma omp parallel for schedule(dynamic) collapse(2)
+  for (int b = 0; b < P.nb; ++b)
+    for (int k = 0; k < P.N1; ++k) {
+      double out[NV];
+      for (int j = 0; j < P.N1; ++j)
+        for (int i = 0; i < P.N1; ++i) {
+          int I[3] = {i, j, k};
+          rhs_point(P, b, I, t, matter, out);
+          size_t o = (size_t)b * NV * S + i + P.N1 * (j + (size_t)P.N1 * k);
+          for (int v = 0; v < NV; ++v) du[o + v * S] = out[v];
+        }
+    }
+}
+
+// The state the case puts at x: case_state_tuple (src/initialdata.jl:1816-1830)
+static void exact_state(const Problem& P, double t, const double x[3], double out[NV]) { hook_value(P, t, x, out); }
+
+// gh_paste_kernel! (src/evolution.jl:888-905), the :pasted variant's limiter
+static void stage_limit(Problem& P, double* u, double t) {
+  if (P.in.variant != TGH_INT_PASTED) return;
+  const size_t S = P.npt_state();
+#pragma omp parallel for schedule(dynamic)
+  for (int b = 0; b < P.nb; ++b)
+    for (int k = 0; k < P.N1; ++k)
+      for (int j = 0; j < P.N1; ++j)
+        for (int i = 0; i < P.N1; ++i) {
+          int64_t n[3] = {(int64_t)P.corner[3 * b] + i, (int64_t)P.corner[3 * b + 1] + j,
+                          (int64_t)P.corner[3 * b + 2] + k};
+          double x[3];
+          P.position(P.level[b], n, x);
+          if (P.in.is_outside(P.in.radius(t, x))) continue;
+          double vals[NV];
+          exact_state(P, t, x, vals);
+          size_t o = (size_t)b * NV * S + i + P.N1 * (j + (size_t)P.N1 * k);
+          for (int v = 0; v < NV; ++v) u[o + v * S] = vals[v];
+        }
+}
+
+static void initial_state(Problem& P, double* u, double t) {
+  const size_t S = P.npt_state();
+#pragma omp parallel for schedule(dynamic)
+  for (int b = 0; b < P.nb; ++b)
+    for (int k = 0; k < P.N1; ++k)
+      for (int j = 0; j < P.N1; ++j)
+        for (int i = 0; i < P.N1; ++i) {
+          int64_t n[3] = {(int64_t)P.corner[3 * b] + i, (int64_t)P.corner[3 * b + 1] + j,
+                          (int64_t)P.corner[3 * b + 2] + k};
+          double x[3], vals[NV];
+          P.position(P.level[b], n, x);
+          exact_state(P, t, x, vals);
+          size_t o = (size_t)b * NV * S + i + P.N1 * (j + (size_t)P.N1 * k);
+          for (int v = 0; v < NV; ++v) u[o + v * S] = vals[v];
+        }
+  stage_limit(P, u, t);
+}
+
+static bool is_evolved(const Problem& P, double t, const double x[3]) {
+  return P.in.variant == TGH_INT_NONE ? true : P.in.radius(t, x) >= P.in.r1;
+}
+
+// max_speed(p, u, t) (src/evolution.jl:1539-1560 with gh_speed_kernel! :932-949)
+static int max_speed(Problem& P, const double* u, double t, double* lam) {
+  const size_t S = P.npt_state();
+  long nbad = 0;
+  double best = 0.0;
+  bool nan = false;
+  for (int b = 0; b < P.nb; ++b)
+    for (int k = 0; k < P.N1; ++k)
+      for (int j = 0; j < P.N1; ++j)
+        for (int i = 0; i < P.N1; ++i) {
+          int64_t n[3] = {(int64_t)P.corner[3 * b] + i, (int64_t)P.corner[3 * b + 1] + j,
+                          (int64_t)P.corner[3 * b + 2] + k};
+          double x[3];
+          P.position(P.level[b], n, x);
+          if (!is_evolved(P, t, x)) continue;
+          size_t o = (size_t)b * NV * S + i + P.N1 * (j + (size_t)P.N1 * k);
+          double hv[NC];
+          for (int v = 0; v < NV; ++v)
+            if (!std::isfinite(u[o + v * S])) ++nbad;
+          for (int v = 0; v < NC; ++v) hv[v] = u[o + v * S];
+          Coef<double> C;
+          metric_quantities(hv, C);
+          double l = C.alpha * std::sqrt(C.gamu[0][0] + C.gamu[1][1] + C.gamu[2][2]) +
+                     std::sqrt(C.beta[0] * C.beta[0] + C.beta[1] * C.beta[1] + C.beta[2] * C.beta[2]);
+          if (std::isnan(l)) nan = true;
+          if (l > best) best = l;
+        }
+  if (nbad > 0) {
+    P.err = "the state is not finite where it is evolved: " + std::to_string(nbad) + " values";
+    return TGH_ERR_NONFINITE;
+  }
+  *lam = nan ? NAN : best;
+  if (!(std::isfinite(*lam) && *lam > 0)) {
+    P.err = "the maximum characteristic speed is not finite and positive";
+    return TGH_ERR_SPEED;
+  }
+  return TGH_OK;
+}
+
+// RK4 with the accumulation order this oracle and the product share:
+//   acc = u + (dt/6) k1;  y2 = u + (dt/2) k1
+//   acc = acc + (dt/3) k2;  y3 = u + (dt/2) k2
+//   acc = acc + (dt/3) k3;  y4 = u + dt k3
+//   u_new = acc + (dt/6) k4          each update one fused multiply-add
+static void rk4_step(Problem& P, double* u, double t, double dt) {
+  const size_t L = P.npt_state() * NV * P.nb;
+  std::vector<double> k(L), acc(L), y(L), u0(u, u + L);
+  const double b16 = dt / 6.0, b13 = dt / 3.0, a12 = 0.5 * dt;
+  const double tm = t + 0.5 * dt, te = t + dt;
+  prepare(P, u0.data(), t);
+  rhs(P, k.data(), t, nullptr);
+  for (size_t i = 0; i < L; ++i) {
+    acc[i] = std::fma(b16, k[i], u0[i]);
+    y[i] = std::fma(a12, k[i], u0[i]);
+  }
+  stage_limit(P, y.data(), tm);
+  prepare(P, y.data(), tm);
+  rhs(P, k.data(), tm, nullptr);
+  for (size_t i = 0; i < L; ++i) {
+    acc[i] = std::fma(b13, k[i], acc[i]);
+    y[i] = std::fma(a12, k[i], u0[i]);
+  }
+  stage_limit(P, y.data(), tm);
+  prepare(P, y.data(), tm);
+  rhs(P, k.data(), tm, nullptr);
+  for (size_t i = 0; i < L; ++i) {
+    acc[i] = std::fma(b13, k[i], acc[i]);
+    y[i] = std::fma(dt, k[i], u0[i]);
+  }
+  stage_limit(P, y.data(), te);
+  prepare(P, y.data(), te);
+  rhs(P, k.data(), te, nullptr);
+  for (size_t i = 0; i < L; ++i) u[i] = std::fma(b16, k[i], acc[i]);
+  stage_limit(P, u, te);
+}
+
+// the masked, volume-weighted L2 and max of |u - u_exact| over evolved primaries, read
+// from the settled working array (src/constraints.jl:311-396, 716-792)
+static void error_norm(Problem& P, const double* u, double t, double* l2, double* linf) {
+  prepare(P, u, t);
+  double s2 = 0.0, vol = 0.0, mx = 0.0;
+  for (int b = 0; b < P.nb; ++b) {
+    double h = P.spacing(P.level[b]);
+    double w = h * h * h;
+    for (int k = 0; k < P.N1; ++k)
+      for (int j = 0; j < P.N1; ++j)
+        for (int i = 0; i < P.N1; ++i) {
+          int64_t n[3] = {(int64_t)P.corner[3 * b] + i, (int64_t)P.corner[3 * b + 1] + j,
+                          (int64_t)P.corner[3 * b + 2] + k};
+          int leaf, loc[3];
+          if (!find_owner(P, P.level[b], n, leaf, loc) || leaf != b) continue;
+          double x[3];
+          P.position(P.level[b], n, x);
+          if (!is_evolved(P, t, x)) continue;
+          double ex[NV];
+          exact_state(P, t, x, ex);
+          size_t o = (size_t)b * NV * P.npt_work() + (i + P.G) + P.W * ((j + P.G) + (size_t)P.W * (k + P.G));
+          double e2 = 0.0;
+          for (int v = 0; v < NV; ++v) {
+            double d = P.work[o + v * P.npt_work()] - ex[v];
+            e2 = v == 0 ? d * d : e2 + d * d;
+          }
+          double e = std::sqrt(e2);
+          s2 += e * e * w;
+          vol += w;
+          if (e > mx) mx = e;
+        }
+  }
+  *l2 = vol == 0.0 ? 0.0 : std::sqrt(s2 / vol);
+  *linf = mx;
+}
+
+}  // namespace orc
+
+using namespace orc;
+
+extern "C" {
+
+void* orc_create(const tgh_config* cfg, const tgh_mesh* m, int margin_check, char* errbuf, int errlen) {
+  (void)margin_check;
+  try {
+    if (cfg->q < 2 || cfg->q % 2 != 0 || cfg->q > 8) throw std::invalid_argument("q must be even in 2..8");
+    Problem* P = new Problem(cfg->q);
+    P->cfg = *cfg;
+    P->q = cfg->q;
+    P->G = cfg->q / 2 + 1;
+    P->N = m->N;
+    P->N1 = m->N + 1;
+    P->W = m->N + 2 * P->G + 1;
+    P->nb = m->nblocks;
+    P->h0 = m->h0;
+    for (int d = 0; d < 3; ++d) {
+      P->lo[d] = m->lo[d];
+      P->cells0[d] = m->cells0[d];
+      P->periodic[d] = m->periodic[d];
+    }
+    P->level.assign(m->level, m->level + m->nblocks);
+    P->corner.assign(m->corner, m->corner + 3 * m->nblocks);
+    for (int b = 0; b < P->nb; ++b) P->maxlevel = std::max(P->maxlevel, P->level[b]);
+    P->lut.resize(P->maxlevel + 1);
+    for (int b = 0; b < P->nb; ++b)
+      P->lut[P->level[b]][P->key(P->corner[3 * b] / P->N, P->corner[3 * b + 1] / P->N, P->corner[3 * b + 2] / P->N)] = b;
+    // prolongation weights: Lagrange on p = q + 2 nodes, at the midpoint of the middle pair
+    {
+      const int p = cfg->q + 2;
+      std::vector<Rat> ns;
+      for (int k = 0; k < p; ++k) ns.push_back(Rat(2 * (k - (p / 2 - 1)) - 1, 2));
+      P->wP = to_double(lagrange_derivative_weights(ns, 0));
+    }
+    P->in.variant = cfg->interior;
+    for (int i = 0; i < 3; ++i) {
+      P->in.c0[i] = cfg->int_c0[i];
+      P->in.v[i] = cfg->int_v[i];
+    }
+    P->in.r0 = cfg->r0;
+    P->in.r1 = cfg->r1;
+    P->in.rho_max = cfg->rho_max;
+    P->in.w_ramp = cfg->w_ramp;
+    P->in.rho_ramp = cfg->rho_ramp;
+    P->pr.damping = cfg->damping;
+    P->pr.gamma0 = cfg->gamma0;
+    P->pr.dn = cfg->damp_near;
+    P->pr.df = cfg->damp_far;
+    P->pr.dw = cfg->damp_width;
+    P->pr.dissipation = cfg->dissipation;
+    P->pr.eps = cfg->eps_ko;
+    P->pr.eo = cfg->eps_out;
+    P->pr.ei = cfg->eps_in;
+    P->pr.er1 = cfg->eps_r1;
+    P->pr.erh = cfg->eps_rh;
+    for (int i = 0; i < 3; ++i) {
+      P->pr.dc0[i] = cfg->damp_c0[i];
+      P->pr.dv[i] = cfg->damp_v[i];
+      P->pr.ec0[i] = cfg->eps_c0[i];
+      P->pr.ev[i] = cfg->eps_v[i];
+    }
+    P->diss = P->pr.has_dissipation();
+    P->ks = make_ks_source(cfg->ks_M, cfg->ks_spin, cfg->ks_velocity);
+    if (cfg->gauge == TGH_GAUGE_SAMPLED) {
+      // sample_gauge_source! at t = 0 with the core rule (src/gauge.jl:156-170)
+      const size_t S = P->npt_state();
+      P->Hsrc.assign(S * NV * P->nb, 0.0);
+#pragma omp parallel for schedule(dynamic)
+      for (int b = 0; b < P->nb; ++b)
+        for (int k = 0; k < P->N1; ++k)
+          for (int j = 0; j < P->N1; ++j)
+            for (int i = 0; i < P->N1; ++i) {
+              int64_t n[3] = {(int64_t)P->corner[3 * b] + i, (int64_t)P->corner[3 * b + 1] + j,
+                              (int64_t)P->corner[3 * b + 2] + k};
+              double x[3], xc[3];
+              P->position(P->level[b], n, x);
+              P->in.core_position(0.0, x, xc);
+              double p4[4] = {0.0, xc[0], xc[1], xc[2]}, Hl[4], dHl[4][4];
+              gauge_source_grad(cfg->bg, p4, Hl, dHl);
+              size_t o = (size_t)b * NV * S + i + P->N1 * (j + (size_t)P->N1 * k);
+              for (int a = 0; a < 4; ++a) P->Hsrc[o + a * S] = Hl[a];
+              for (int kk = 0; kk < 16; ++kk) P->Hsrc[o + (4 + kk) * S] = dHl[kk % 4][kk / 4];
+            }
+    }
+    return P;
+  } catch (const std::exception& e) {
+    if (errbuf && errlen > 0) {
+      std::strncpy(errbuf, e.what(), errlen - 1);
+      errbuf[errlen - 1] = 0;
+    }
+    return nullptr;
+  }
+}
+
+void orc_destroy(void* p) { delete (Problem*)p; }
+const char* orc_last_error(void* p) { return ((Problem*)p)->err.c_str(); }
+size_t orc_state_length(void* p) { Problem* P = (Problem*)p; return P->npt_state() * NV * P->nb; }
+size_t orc_work_length(void* p) { Problem* P = (Problem*)p; return P->npt_work() * NV * P->nb; }
+void orc_set_threads(int n) { omp_set_num_threads(n); }
+int orc_get_threads(void) { return omp_get_max_threads(); }
+
+int orc_prepare(void* p, const double* u, double t) {
+  try { prepare(*(Problem*)p, u, t); } catch (const std::exception& e) { ((Problem*)p)->err = e.what(); return TGH_ERR_ARG; }
+  return TGH_OK;
+}
+int orc_rhs(void* p, double* du, double t, const double* matter) { rhs(*(Problem*)p, du, t, matter); return TGH_OK; }
+int orc_gh_rhs(void* p, double* du, const double* u, double t, const double* matter) {
+  int s = orc_prepare(p, u, t);
+  if (s) return s;
+  return orc_rhs(p, du, t, matter);
+}
+int orc_copy_work(void* p, double* dst) {
+  Problem* P = (Problem*)p;
+  std::memcpy(dst, P->work.data(), P->work.size() * sizeof(double));
+  return TGH_OK;
+}
+int orc_copy_hsrc(void* p, double* dst) {
+  Problem* P = (Problem*)p;
+  std::memcpy(dst, P->Hsrc.data(), P->Hsrc.size() * sizeof(double));
+  return TGH_OK;
+}
+int orc_initial_state(void* p, double* u, double t) { initial_state(*(Problem*)p, u, t); return TGH_OK; }
+int orc_stage_limit(void* p, double* u, double t) { stage_limit(*(Problem*)p, u, t); return TGH_OK; }
+int orc_max_speed(void* p, const double* u, double t, double* lam) { return max_speed(*(Problem*)p, u, t, lam); }
+int orc_rk4_step(void* p, double* u, double t, double dt) {
+  try { rk4_step(*(Problem*)p, u, t, dt); } catch (const std::exception& e) { ((Problem*)p)->err = e.what(); return TGH_ERR_ARG; }
+  return TGH_OK;
+}
+int orc_error_norm(void* p, const double* u, double t, double* l2, double* linf) {
+  error_norm(*(Problem*)p, u, t, l2, linf);
+  return TGH_OK;
+}
+
+// test/evolution_tests.jl:37-89: the expanded reference spelling at one owned point of
+// the current working array, with the dissipation correction of the source.
+int orc_host_rhs_at(void* p, int b, int i, int j, int k, double t, double out[20]) {
+  Problem& P = *(Problem*)p;
+  const double h = P.spacing(P.level[b]);
+  const double* wk = P.work.data() + (size_t)b * NV * P.npt_work();
+  const size_t sv = P.npt_work();
+  const long st[3] = {1, P.W, (long)P.W * P.W};
+  const size_t var = (size_t)(i + P.G) + P.W * ((size_t)(j + P.G) + (size_t)P.W * (k + P.G));
+  int64_t n[3] = {(int64_t)P.corner[3 * b] + i, (int64_t)P.corner[3 * b + 1] + j, (int64_t)P.corner[3 * b + 2] + k};
+  double x[3];
+  P.position(P.level[b], n, x);
+  double g0 = P.pr.damping_rate(t, x);
+  double hv[NC], Pv[NC], dhs[3][NC], dPs[3][NC], dds[6][NC];
+  for (int v = 0; v < NC; ++v) {
+    hv[v] = wk[var + v * sv];
+    Pv[v] = wk[var + (NC + v) * sv];
+    for (int d = 0; d < 3; ++d) {
+      dhs[d][v] = axis_stencil(P.st.w1, wk, var + v * sv, st[d]) / h;
+      dPs[d][v] = axis_stencil(P.st.w1, wk, var + (NC + v) * sv, st[d]) / h;
+    }
+    const int pairs[6][2] = {{0, 0}, {0, 1}, {0, 2}, {1, 1}, {1, 2}, {2, 2}};
+    for (int m = 0; m < 6; ++m) {
+      int d1 = pairs[m][0], d2 = pairs[m][1];
+      dds[m][v] = d1 == d2 ? axis_stencil(P.st.w2, wk, var + v * sv, st[d1]) / (h * h)
+                           : mixed_stencil(P.st.w1, wk, var + v * sv, st[d1], st[d2]) / (h * h);
+    }
+  }
+  const double* dh[3] = {dhs[0], dhs[1], dhs[2]};
+  const double* dP[3] = {dPs[0], dPs[1], dPs[2]};
+  const double* dd[6] = {dds[0], dds[1], dds[2], dds[3], dds[4], dds[5]};
+  double Hl[4], dHl[4][4];
+  int I[3] = {i, j, k};
+  double dth0[NC];
+  {
+    // gauge source: the sampled field, or the closed form from the undissipated d_t h
+    Coef<double> C;
+    metric_quantities(hv, C);
+    double a_div = C.alpha / C.sqrtg;
+    for (int v = 0; v < NC; ++v)
+      dth0[v] = C.beta[0] * dh[0][v] + C.beta[1] * dh[1][v] + C.beta[2] * dh[2][v] + a_div * Pv[v];
+  }
+  double eps = P.pr.dissipation_rate(t, x);
+  double Qh[NC], QP[NC];
+  for (int v = 0; v < NC; ++v) {
+    Qh[v] = (eps / h) * ((axis_stencil(P.st.wD, wk, var + v * sv, st[0]) + axis_stencil(P.st.wD, wk, var + v * sv, st[1])) +
+                         axis_stencil(P.st.wD, wk, var + v * sv, st[2]));
+    QP[v] = (eps / h) * ((axis_stencil(P.st.wD, wk, var + (NC + v) * sv, st[0]) +
+                          axis_stencil(P.st.wD, wk, var + (NC + v) * sv, st[1])) +
+                         axis_stencil(P.st.wD, wk, var + (NC + v) * sv, st[2]));
+  }
+  double dthq[NC];
+  for (int v = 0; v < NC; ++v) dthq[v] = P.diss ? dth0[v] + Qh[v] : dth0[v];
+  gauge_at_point(P, b, I, hv, dthq, dh, Hl, dHl);
+  double dth[NC], dtP[NC];
+  gh_node_rhs_expanded(hv, Pv, dh, dP, dd, Hl, dHl, g0, P.cfg.gamma2, dth, dtP);
+  if (P.diss) {
+    Coef<double> C;
+    metric_quantities(hv, C);
+    double dg1[4][4][4], dg2[4][4][4], s1[NC], s2[NC], dtq[NC];
+    for (int v = 0; v < NC; ++v) dtq[v] = dth[v] + Qh[v];
+    dg4(dtq, dh, dg1);
+    dg4(dth, dh, dg2);
+    gh_node_source(C, dg1, Hl, dHl, g0, P.cfg.gamma2, s1);
+    gh_node_source(C, dg2, Hl, dHl, g0, P.cfg.gamma2, s2);
+    for (int v = 0; v < NC; ++v) {
+      dth[v] = dth[v] + Qh[v];
+      dtP[v] = dtP[v] + QP[v] + (s1[v] - s2[v]);
+    }
+  }
+  for (int v = 0; v < NC; ++v) {
+    out[v] = dth[v];
+    out[NC + v] = dtP[v];
+  }
+  return TGH_OK;
+}
+
+// test/evolution_tests.jl:97-108
+double orc_rhs_scale(void* p, int b, int i, int j, int k) {
+  Problem& P = *(Problem*)p;
+  const double h = P.spacing(P.level[b]);
+  const double* wk = P.work.data() + (size_t)b * NV * P.npt_work();
+  const size_t sv = P.npt_work();
+  const long st[3] = {1, P.W, (long)P.W * P.W};
+  const size_t var = (size_t)(i + P.G) + P.W * ((size_t)(j + P.G) + (size_t)P.W * (k + P.G));
+  double s = 0.0;
+  for (int v = 0; v < NV; ++v)
+    for (int d = 0; d < 3; ++d) {
+      double a = std::fabs(axis_stencil(P.st.w2, wk, var + v * sv, st[d])) / (h * h);
+      double c = std::fabs(wk[var + v * sv]);
+      s = std::max(s, std::max(a, c));
+    }
+  return std::max(s, 1.0);
+}
+
+// ---- pointwise entry points for the unit tests ----
+int orc_weights(int q, int m, int64_t* num, int64_t* den) {
+  std::vector<Rat> w = m == 0 ? rational_dissipation_weights(q) : rational_derivative_weights(q, m);
+  for (size_t i = 0; i < w.size(); ++i) {
+    num[i] = (int64_t)w[i].n;
+    den[i] = (int64_t)w[i].d;
+  }
+  return (int)w.size();
+}
+int orc_weights_double(int q, int m, double* out) {
+  std::vector<Rat> w = m == 0 ? rational_dissipation_weights(q) : rational_derivative_weights(q, m);
+  std::vector<double> d = to_double(w);
+  for (size_t i = 0; i < d.size(); ++i) out[i] = d[i];
+  return (int)d.size();
+}
+// out: g4[16], gu4[16], alpha, beta[3], gamu[9], sqrtg
+void orc_metric_quantities(const double* h, double* out) {
+  Coef<double> C;
+  metric_quantities(h, C);
+  for (int a = 0; a < 4; ++a)
+    for (int b = 0; b < 4; ++b) {
+      out[a * 4 + b] = C.g4[a][b];
+      out[16 + a * 4 + b] = C.gu4[a][b];
+    }
+  out[32] = C.alpha;
+  for (int i = 0; i < 3; ++i) out[33 + i] = C.beta[i];
+  for (int i = 0; i < 3; ++i)
+    for (int j = 0; j < 3; ++j) out[36 + 3 * i + j] = C.gamu[i][j];
+  out[45] = C.sqrtg;
+}
+// dh: [3][10]; dHl: [4][4] row-major dHl[a][b] = d_a H_b; which: 0 lean, 1 reference spelling
+void orc_source(int which, const double* h, const double* dth, const double* dh, const double* Hl,
+                const double* dHl, double g0, double g2, double* msrc) {
+  Coef<double> C;
+  metric_quantities(h, C);
+  const double* d3[3] = {dh, dh + 10, dh + 20};
+  double H[4][4];
+  for (int a = 0; a < 4; ++a)
+    for (int b = 0; b < 4; ++b) H[a][b] = dHl[a * 4 + b];
+  if (which == 0) {
+    gh_node_source_lean(C, dth, d3, Hl, H, g0, g2, msrc);
+  } else {
+    double dg[4][4][4];
+    dg4(dth, d3, dg);
+    gh_node_source(C, dg, Hl, H, g0, g2, msrc);
+  }
+}
+// divergences: which 0 lean (metric_divergences), 1 contraction of metric_derivatives
+void orc_divergences(int which, const double* h, const double* dh, double* out4) {
+  Coef<double> C;
+  metric_quantities(h, C);
+  const double* d3[3] = {dh, dh + 10, dh + 20};
+  if (which == 0) {
+    metric_divergences(C, d3, out4[0], out4 + 1);
+  } else {
+    double dal[3], db[3][3], dA[3][3][3];
+    metric_derivatives(C, d3, dal, db, dA);
+    out4[0] = (db[0][0] + db[1][1]) + db[2][2];
+    for (int j = 0; j < 3; ++j) out4[1 + j] = (dA[0][0][j] + dA[1][1][j]) + dA[2][2][j];
+  }
+}
+void orc_dmetric(const tgh_background* bg, const double* p4, double* g16, double* dg64) {
+  double g[4][4], dg[4][4][4];
+  dmetric(*bg, p4, g, dg);
+  for (int a = 0; a < 4; ++a)
+    for (int b = 0; b < 4; ++b) {
+      g16[a * 4 + b] = g[a][b];
+      for (int c = 0; c < 4; ++c) dg64[(a * 4 + b) * 4 + c] = dg[a][b][c];
+    }
+}
+void orc_background_state(const tgh_background* bg, double t, const double* x3, double* h, double* Pi, double* dh30,
+                          double* dtg) {
+  double dh[3][NC];
+  background_state(*bg, t, x3, h, Pi, dh, dtg);
+  for (int d = 0; d < 3; ++d)
+    for (int v = 0; v < NC; ++v) dh30[d * NC + v] = dh[d][v];
+}
+void orc_gauge_source_grad(const tgh_background* bg, const double* p4, double* Hl, double* dHl16) {
+  double dH[4][4];
+  gauge_source_grad(*bg, p4, Hl, dH);
+  for (int a = 0; a < 4; ++a)
+    for (int b = 0; b < 4; ++b) dHl16[a * 4 + b] = dH[a][b];
+}
+void orc_algebraic_gauge_source(double M, const double* spin, const double* vel, const double* h, const double* dth,
+                                const double* dh30, double* Hl, double* dHl16) {
+  KSSource k = make_ks_source(M, spin, vel);
+  const double* d3[3] = {dh30, dh30 + 10, dh30 + 20};
+  double dH[4][4];
+  algebraic_gauge_source(k, h, dth, d3, Hl, dH);
+  for (int a = 0; a < 4; ++a)
+    for (int b = 0; b < 4; ++b) dHl16[a * 4 + b] = dH[a][b];
+}
+double orc_smoothstep(double s) { return smoothstep(s); }
+
+}  // extern "C"
+
+// ---- an op-counting scalar: the algorithmic FP64 work of one right-hand-side point ----
+namespace orc {
+struct Cnt {
+  double v;
+  static long nadd, nmul, ndiv, nsqrt;
+  Cnt() : v(0) {}
+  Cnt(double x) : v(x) {}
+};
+long Cnt::nadd = 0, Cnt::nmul = 0, Cnt::ndiv = 0, Cnt::nsqrt = 0;
+static inline Cnt operator+(Cnt a, Cnt b) { ++Cnt::nadd; return Cnt(a.v + b.v); }
+static inline Cnt operator-(Cnt a, Cnt b) { ++Cnt::nadd; return Cnt(a.v - b.v); }
+static inline Cnt operator-(Cnt a) { return Cnt(-a.v); }
+static inline Cnt operator*(Cnt a, Cnt b) {
+  // products by an exact zero weight (the first derivative's center tap) are not work
+  if (a.v != 0.0 && b.v != 0.0) ++Cnt::nmul;
+  return Cnt(a.v * b.v);
+}
+static inline Cnt operator/(Cnt a, Cnt b) { ++Cnt::ndiv; return Cnt(a.v / b.v); }
+static inline bool operator!=(Cnt a, Cnt b) { return a.v != b.v; }
+static inline Cnt sqrt(Cnt a) { ++Cnt::nsqrt; return Cnt(std::sqrt(a.v)); }
+}  // namespace orc
+
+extern "C" {
+// Counts the floating-point operations of F(u) at one interior owned point of block 0 of a
+// prepared problem (no interior branches). out: adds, multiplies, divides, square roots.
+// A multiply feeding an add is counted as two operations (an FMA is 2 flops).
+int orc_count_flops(void* p, double t, long* out) {
+  Problem& P = *(Problem*)p;
+  PointCtx c;
+  c.wk = P.work.data();
+  c.sv = P.npt_work();
+  c.st[0] = 1;
+  c.st[1] = P.W;
+  c.st[2] = P.W * P.W;
+  const int I[3] = {P.N / 2, P.N / 2, P.N / 2};
+  c.var = (size_t)(I[0] + P.G) + P.W * ((size_t)(I[1] + P.G) + (size_t)P.W * (I[2] + P.G));
+  int64_t n[3] = {(int64_t)P.corner[0] + I[0], (int64_t)P.corner[1] + I[1], (int64_t)P.corner[2] + I[2]};
+  double x[3];
+  P.position(P.level[0], n, x);
+  Cnt::nadd = Cnt::nmul = Cnt::ndiv = Cnt::nsqrt = 0;
+  Cnt a[NC], b[NC];
+  try {
+    rhs_at_point<Cnt>(P, c, 0, I, x, t, nullptr, a, b);
+  } catch (const std::exception& e) {
+    P.err = e.what();
+    return TGH_ERR_ARG;
+  }
+  out[0] = Cnt::nadd;
+  out[1] = Cnt::nmul;
+  out[2] = Cnt::ndiv;
+  out[3] = Cnt::nsqrt;
+  return TGH_OK;
+}
+}

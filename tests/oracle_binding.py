@@ -1,0 +1,205 @@
+"""ctypes binding of the CPU oracle (oracle/_build/liboracle.so): test infrastructure only."""
+import ctypes
+import subprocess
+from pathlib import Path
+
+import numpy as np
+
+from conftest import load_package
+
+ROOT = Path(__file__).resolve().parent.parent
+LIB = ROOT / "oracle" / "_build" / "liboracle.so"
+
+_D = ctypes.c_double
+_VP = ctypes.c_void_p
+_DP = ctypes.POINTER(ctypes.c_double)
+
+
+def _dp(a):
+    return a.ctypes.data_as(_DP)
+
+
+class Oracle:
+    _inst = None
+
+    def __init__(self, lib):
+        self.lib = lib
+        abi = load_package()._abi
+        self.abi = abi
+        sig = {
+            "orc_create": (_VP, [ctypes.POINTER(abi.Config), ctypes.POINTER(abi.Mesh), ctypes.c_int, ctypes.c_char_p,
+                                 ctypes.c_int]),
+            "orc_destroy": (None, [_VP]),
+            "orc_last_error": (ctypes.c_char_p, [_VP]),
+            "orc_state_length": (ctypes.c_size_t, [_VP]),
+            "orc_work_length": (ctypes.c_size_t, [_VP]),
+            "orc_set_threads": (None, [ctypes.c_int]),
+            "orc_get_threads": (ctypes.c_int, []),
+            "orc_prepare": (ctypes.c_int, [_VP, _DP, _D]),
+            "orc_rhs": (ctypes.c_int, [_VP, _DP, _D, _DP]),
+            "orc_gh_rhs": (ctypes.c_int, [_VP, _DP, _DP, _D, _DP]),
+            "orc_copy_work": (ctypes.c_int, [_VP, _DP]),
+            "orc_copy_hsrc": (ctypes.c_int, [_VP, _DP]),
+            "orc_initial_state": (ctypes.c_int, [_VP, _DP, _D]),
+            "orc_stage_limit": (ctypes.c_int, [_VP, _DP, _D]),
+            "orc_max_speed": (ctypes.c_int, [_VP, _DP, _D, _DP]),
+            "orc_rk4_step": (ctypes.c_int, [_VP, _DP, _D, _D]),
+            "orc_error_norm": (ctypes.c_int, [_VP, _DP, _D, _DP, _DP]),
+            "orc_host_rhs_at": (ctypes.c_int, [_VP, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, _D, _DP]),
+            "orc_rhs_scale": (_D, [_VP, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int]),
+            "orc_weights": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_int64),
+                                           ctypes.POINTER(ctypes.c_int64)]),
+            "orc_weights_double": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, _DP]),
+            "orc_metric_quantities": (None, [_DP, _DP]),
+            "orc_source": (None, [ctypes.c_int, _DP, _DP, _DP, _DP, _DP, _D, _D, _DP]),
+            "orc_divergences": (None, [ctypes.c_int, _DP, _DP, _DP]),
+            "orc_dmetric": (None, [ctypes.POINTER(abi.Background), _DP, _DP, _DP]),
+            "orc_background_state": (None, [ctypes.POINTER(abi.Background), _D, _DP, _DP, _DP, _DP, _DP]),
+            "orc_gauge_source_grad": (None, [ctypes.POINTER(abi.Background), _DP, _DP, _DP]),
+            "orc_algebraic_gauge_source": (None, [_D, _DP, _DP, _DP, _DP, _DP, _DP, _DP]),
+            "orc_smoothstep": (_D, [_D]),
+        }
+        for name, (res, args) in sig.items():
+            fn = getattr(lib, name)
+            fn.restype = res
+            fn.argtypes = args
+
+    @classmethod
+    def load(cls):
+        if cls._inst is None:
+            if not LIB.exists():
+                subprocess.run(["make", "-C", str(ROOT / "oracle")], check=True, capture_output=True)
+            cls._inst = cls(ctypes.CDLL(str(LIB)))
+        return cls._inst
+
+    def problem(self, case, forest, q, margin_check=False):
+        return OracleProblem(self, case, forest, q, margin_check)
+
+    # pointwise helpers
+    def weights(self, q, m):
+        num = (ctypes.c_int64 * 16)()
+        den = (ctypes.c_int64 * 16)()
+        n = self.lib.orc_weights(q, m, num, den)
+        return [(num[i], den[i]) for i in range(n)]
+
+    def weights_double(self, q, m):
+        out = np.zeros(16)
+        n = self.lib.orc_weights_double(q, m, _dp(out))
+        return out[:n]
+
+    def metric_quantities(self, h):
+        out = np.zeros(46)
+        self.lib.orc_metric_quantities(_dp(np.ascontiguousarray(h, dtype=float)), _dp(out))
+        return dict(g4=out[:16].reshape(4, 4), gu4=out[16:32].reshape(4, 4), alpha=out[32], beta=out[33:36],
+                    gamu=out[36:45].reshape(3, 3), sqrtg=out[45])
+
+    def source(self, which, h, dth, dh, Hl, dHl, g0, g2):
+        out = np.zeros(10)
+        args = [np.ascontiguousarray(a, dtype=float) for a in (h, dth, dh, Hl, dHl)]
+        self.lib.orc_source(which, *[_dp(a) for a in args], g0, g2, _dp(out))
+        return out
+
+    def divergences(self, which, h, dh):
+        out = np.zeros(4)
+        a = [np.ascontiguousarray(x, dtype=float) for x in (h, dh)]
+        self.lib.orc_divergences(which, _dp(a[0]), _dp(a[1]), _dp(out))
+        return out
+
+    def background(self, case):
+        return case.config(4).bg
+
+    def dmetric(self, bg, p):
+        g = np.zeros(16)
+        dg = np.zeros(64)
+        self.lib.orc_dmetric(ctypes.byref(bg), _dp(np.ascontiguousarray(p, dtype=float)), _dp(g), _dp(dg))
+        return g.reshape(4, 4), dg.reshape(4, 4, 4)
+
+    def background_state(self, bg, t, x):
+        h, Pi, dh, dtg = np.zeros(10), np.zeros(10), np.zeros(30), np.zeros(10)
+        self.lib.orc_background_state(ctypes.byref(bg), t, _dp(np.ascontiguousarray(x, dtype=float)), _dp(h),
+                                      _dp(Pi), _dp(dh), _dp(dtg))
+        return h, Pi, dh.reshape(3, 10), dtg
+
+    def gauge_source_grad(self, bg, p):
+        Hl, dHl = np.zeros(4), np.zeros(16)
+        self.lib.orc_gauge_source_grad(ctypes.byref(bg), _dp(np.ascontiguousarray(p, dtype=float)), _dp(Hl),
+                                       _dp(dHl))
+        return Hl, dHl.reshape(4, 4)
+
+    def algebraic_gauge_source(self, M, spin, vel, h, dth, dh):
+        Hl, dHl = np.zeros(4), np.zeros(16)
+        a = [np.ascontiguousarray(x, dtype=float) for x in (spin, vel, h, dth, dh)]
+        self.lib.orc_algebraic_gauge_source(M, *[_dp(x) for x in a], _dp(Hl), _dp(dHl))
+        return Hl, dHl.reshape(4, 4)
+
+
+class OracleProblem:
+    def __init__(self, orc, case, forest, q, margin_check=False):
+        self.orc, self.lib = orc, orc.lib
+        self.case, self.forest, self.q = case, forest, q
+        self._cfg = case.config(q)
+        self._mesh = forest.mesh()
+        err = ctypes.create_string_buffer(512)
+        self.h = self.lib.orc_create(ctypes.byref(self._cfg), ctypes.byref(self._mesh), int(margin_check), err, 512)
+        if not self.h:
+            raise RuntimeError(err.value.decode())
+        self.L = int(self.lib.orc_state_length(self.h))
+        self.LW = int(self.lib.orc_work_length(self.h))
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            self.lib.orc_destroy(self.h)
+            self.h = None
+
+    def statevector(self):
+        return np.zeros(self.L)
+
+    def initial_state(self, u, t):
+        self.lib.orc_initial_state(self.h, _dp(u), t)
+        return u
+
+    def prepare(self, u, t):
+        st = self.lib.orc_prepare(self.h, _dp(u), t)
+        assert st == 0, self.lib.orc_last_error(self.h)
+
+    def rhs(self, du, t, matter=None):
+        self.lib.orc_rhs(self.h, _dp(du), t, _dp(matter) if matter is not None else None)
+
+    def gh_rhs(self, du, u, t, matter=None):
+        self.prepare(u, t)
+        self.rhs(du, t, matter)
+
+    def work(self):
+        w = np.zeros(self.LW)
+        self.lib.orc_copy_work(self.h, _dp(w))
+        return w
+
+    def hsrc(self):
+        w = np.zeros(self.L)
+        self.lib.orc_copy_hsrc(self.h, _dp(w))
+        return w
+
+    def rk4_step(self, u, t, dt):
+        st = self.lib.orc_rk4_step(self.h, _dp(u), t, dt)
+        assert st == 0, self.lib.orc_last_error(self.h)
+
+    def max_speed(self, u, t):
+        lam = ctypes.c_double()
+        st = self.lib.orc_max_speed(self.h, _dp(u), t, ctypes.byref(lam))
+        return st, lam.value
+
+    def error_norm(self, u, t):
+        a, b = ctypes.c_double(), ctypes.c_double()
+        self.lib.orc_error_norm(self.h, _dp(u), t, ctypes.byref(a), ctypes.byref(b))
+        return a.value, b.value
+
+    def host_rhs_at(self, b, i, j, k, t):
+        out = np.zeros(20)
+        self.lib.orc_host_rhs_at(self.h, b, i, j, k, t, _dp(out))
+        return out
+
+    def rhs_scale(self, b, i, j, k):
+        return self.lib.orc_rhs_scale(self.h, b, i, j, k)
+
+    def stage_limit(self, u, t):
+        self.lib.orc_stage_limit(self.h, _dp(u), t)

@@ -1,0 +1,177 @@
+"""The CUDA path against the CPU oracle on identical inputs (the parity gate).
+
+Tolerances (the reference's own, test/evolution_tests.jl:141-179): the right-hand side
+within 1e-12 of rhs_scale per point; copies of the ghost fill bit for bit, prolongation
+bit for bit, Dirichlet ghosts within 1e-13 relative (two evaluations of the analytic
+metric); one RK4 step within 1e-12 absolute on states of order one.
+"""
+import math
+
+import numpy as np
+import pytest
+import torch
+
+from helpers import cases, rhs_error, rhs_scale, two_level_forest
+
+pytestmark = pytest.mark.gpu
+
+RHS_TOL = 1e-12
+
+
+def _to_gpu(a):
+    return torch.from_numpy(np.ascontiguousarray(a)).cuda()
+
+
+def _initial(tgh, P, O, case, forest, name, t):
+    u = O.initial_state(O.statevector(), t)
+    if name.startswith("perturbed"):
+        u = u + tgh.perturbation(forest, amplitude=1e-4)
+    elif name.startswith("kerr") or name.startswith("gauge"):
+        u = u + tgh.perturbation(forest, amplitude=1e-6, seed=11)
+    if name.endswith("pasted"):
+        O.stage_limit(u, t)
+    return u
+
+
+@pytest.mark.parametrize("row", range(14))
+def test_rhs_matches_oracle(tgh, oracle, row):
+    name, case, forest, q, t = cases(tgh)[row]
+    P = tgh.GHProblem(case, forest, q, margin_check=False)
+    O = oracle.problem(case, forest, q)
+    u = _initial(tgh, P, O, case, forest, name, t)
+    du_ref = np.zeros(O.L)
+    O.gh_rhs(du_ref, u, t)
+    ug = _to_gpu(u)
+    dug = torch.full_like(ug, float("nan"))
+    P.gh_rhs(dug, ug, t)
+    torch.cuda.synchronize()
+    assert torch.equal(ug, _to_gpu(u)), "u was written"
+    du = dug.cpu().numpy()
+    assert np.all(np.isfinite(du))
+    err = rhs_error(du, du_ref, rhs_scale(O.work(), forest, q), forest)
+    assert err < RHS_TOL, f"{name}: {err}"
+
+
+def test_matter_source_matches_oracle(tgh, oracle):
+    c = tgh.gauge_wave_case(eps_ko=0.5, gamma0=1.0, gamma2=-0.5)
+    f = tgh.gh_forest(c, 8, 2)
+    P = tgh.GHProblem(c, f, 4)
+    O = oracle.problem(c, f, 4)
+    u = O.initial_state(O.statevector(), 0.1)
+    rng = np.random.default_rng(3)
+    m = 1e-3 * rng.standard_normal(10 * (f.N + 1) ** 3 * f.nblocks)
+    du_ref = np.zeros(O.L)
+    O.gh_rhs(du_ref, u, 0.1, m)
+    du = torch.zeros(O.L, dtype=torch.float64, device="cuda")
+    P.gh_rhs(du, _to_gpu(u), 0.1, _to_gpu(m))
+    assert rhs_error(du.cpu().numpy(), du_ref, rhs_scale(O.work(), f, 4), f) < RHS_TOL
+    # and the matter term is live
+    du0 = torch.zeros_like(du)
+    P.gh_rhs(du0, _to_gpu(u), 0.1)
+    assert torch.max(torch.abs(du - du0)).item() > 1e-6
+
+
+@pytest.mark.parametrize("which", ["periodic", "dirichlet", "two_level"])
+def test_fill_matches_oracle(tgh, oracle, which):
+    if which == "periodic":
+        c = tgh.perturbed_minkowski_case()
+        f = tgh.gh_forest(c, 8, 2)
+    elif which == "dirichlet":
+        c = tgh.kerr_schild_case(M=1.0, a=0.7, halfwidth=2.0, r0=0.8, r1=1.3, gauge="algebraic")
+        f = tgh.gh_forest(c, 8, 2)
+    else:
+        c = tgh.gauge_wave_case(eps_ko=0.5, gamma0=1.0)
+        f = two_level_forest(tgh, c)
+    P = tgh.GHProblem(c, f, 4, margin_check=False)
+    O = oracle.problem(c, f, 4)
+    u = O.initial_state(O.statevector(), 0.2) + tgh.perturbation(f, amplitude=1e-5, seed=5)
+    O.prepare(u, 0.2)
+    P.prepare(_to_gpu(u), 0.2)
+    wg = P.copy_work().cpu().numpy()
+    wo = O.work()
+    if which == "dirichlet":
+        assert np.max(np.abs(wg - wo) / np.maximum(1.0, np.abs(wo))) < 1e-13
+    else:
+        assert np.array_equal(wg, wo)
+
+
+@pytest.mark.parametrize("row", [0, 2, 6, 7, 9, 11])
+def test_rk4_step_matches_oracle(tgh, oracle, row):
+    name, case, forest, q, t = cases(tgh)[row]
+    P = tgh.GHProblem(case, forest, q, margin_check=False)
+    O = oracle.problem(case, forest, q)
+    u = _initial(tgh, P, O, case, forest, name, t)
+    dt = 0.25 * forest.h0 / 2.0
+    ug = _to_gpu(u)
+    P.rk4_step(ug, t, dt)
+    uo = u.copy()
+    O.rk4_step(uo, t, dt)
+    assert np.max(np.abs(ug.cpu().numpy() - uo)) < 1e-12
+    if not name.endswith("pasted"):
+        ub = _to_gpu(u)
+        P.step_batched(ub, t, dt, 1)
+        # compare settled states (the batched form keeps each copy at its primary's value)
+        P.settle(ub, t + dt)
+        us = _to_gpu(uo)
+        P.settle(us, t + dt)
+        assert torch.max(torch.abs(ub - us)).item() < 1e-12
+
+
+def test_two_level_rk4_step_matches_oracle(tgh, oracle):
+    c = tgh.gauge_wave_case(eps_ko=0.5, gamma0=1.0, gamma2=-0.5)
+    f = two_level_forest(tgh, c)
+    P = tgh.GHProblem(c, f, 4)
+    O = oracle.problem(c, f, 4)
+    u = O.initial_state(O.statevector(), 0.0)
+    dt = 0.25 * f.h0 / 2 / 2.0
+    ug = _to_gpu(u)
+    P.rk4_step(ug, 0.0, dt)
+    uo = u.copy()
+    O.rk4_step(uo, 0.0, dt)
+    assert np.max(np.abs(ug.cpu().numpy() - uo)) < 1e-12
+
+
+def test_max_speed_and_error_norm_match_oracle(tgh, oracle):
+    c = tgh.kerr_schild_case(M=1.0, a=0.7, halfwidth=2.0, r0=0.8, r1=1.3, gauge="algebraic")
+    f = tgh.gh_forest(c, 8, 2)
+    P = tgh.GHProblem(c, f, 4, margin_check=False)
+    O = oracle.problem(c, f, 4)
+    u = O.initial_state(O.statevector(), 0.0)
+    ug = P.initial_state(P.statevector(), 0.0)
+    assert np.max(np.abs(ug.cpu().numpy() - u)) < 1e-13 * max(1.0, np.max(np.abs(u)))
+    st, lam_o = O.max_speed(u, 0.0)
+    assert st == 0
+    assert P.max_speed(ug, 0.0) == pytest.approx(lam_o, rel=1e-14)
+    pert = tgh.perturbation(f, amplitude=1e-6, seed=9)
+    l2o, lio = O.error_norm(u + pert, 0.0)
+    l2g, lig = P.error_norm(_to_gpu(u + pert), 0.0)
+    assert l2g == pytest.approx(l2o, rel=1e-10) and lig == pytest.approx(lio, rel=1e-10)
+    assert l2o > 0
+
+
+def test_flat_speed_is_sqrt3_and_nonfinite_refused(tgh):
+    c = tgh.minkowski_case(L=1.0)
+    f = tgh.gh_forest(c, 8, 2)
+    P = tgh.GHProblem(c, f, 4)
+    u = P.initial_state(P.statevector(), 0.0)
+    assert P.max_speed(u, 0.0) == pytest.approx(math.sqrt(3.0), rel=1e-15)
+    u[1234] = float("nan")
+    with pytest.raises(tgh._abi.TGHError) as e:
+        P.max_speed(u, 0.0)
+    assert e.value.code == tgh._abi.TGH_ERR_NONFINITE
+    u.zero_()
+    u[:] = float("nan")
+    with pytest.raises(tgh._abi.TGHError):
+        P.max_speed(u, 0.0)
+
+
+def test_hole_interior_is_masked_for_speed(tgh):
+    # a NaN inside r_1 is not a reason to refuse (src/evolution.jl:1531-1537)
+    c = tgh.kerr_schild_case(M=1.0, a=0.7, halfwidth=2.0, r0=0.8, r1=1.3, gauge="algebraic")
+    f = tgh.gh_forest(c, 8, 2)
+    P = tgh.GHProblem(c, f, 4, margin_check=False)
+    u = P.initial_state(P.statevector(), 0.0)
+    N1 = f.N + 1
+    # block 0 is [-2,0]^3; its corner point (N, N, N) is the origin
+    u[0 * 20 * N1 ** 3 + f.N + N1 * (f.N + N1 * f.N)] = float("nan")
+    assert math.isfinite(P.max_speed(u, 0.0))

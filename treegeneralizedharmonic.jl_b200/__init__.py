@@ -1,0 +1,27 @@
+"""B200-native generalized-harmonic time stepping (the hot path of TreeGeneralizedHarmonic.jl).
+
+The package loads as `tgh_b200` (its directory name is not a Python identifier):
+
+    import importlib.util, sys
+    spec = importlib.util.spec_from_file_location(
+        "tgh_b200", "<repo>/treegeneralizedharmonic.jl_b200/__init__.py",
+        submodule_search_locations=["<repo>/treegeneralizedharmonic.jl_b200"])
+
+Public surface, named after the reference's:
+  cases      minkowski_case, gauge_wave_case, shifted_minkowski_case, kerr_schild_case, ...
+  forests    gh_forest, hole_forest
+  problem    GHProblem with prepare, rhs, gh_rhs, settle, stage_limit, step_limit, max_speed,
+             initial_state, gh_dt, rk4_step, step_batched, gh_solve, error_norm
+"""
+from . import _abi
+from .cases import (Case, gauge_wave_case, horizon_min_radius, kerr_schild_case, minkowski_case,
+                    perturbed_minkowski_case, shifted_minkowski_case)
+from .forest import Forest, gh_forest, hole_forest
+from .initialdata import fourier_modes, perturbation
+from .problem import GHProblem, fp64_peak_tflops
+
+__all__ = ["Case", "Forest", "GHProblem", "gauge_wave_case", "gh_forest", "hole_forest", "kerr_schild_case",
+           "minkowski_case", "perturbed_minkowski_case", "shifted_minkowski_case", "horizon_min_radius",
+           "fourier_modes", "perturbation", "fp64_peak_tflops", "load_library"]
+
+load_library = _abi.load_library

@@ -1,0 +1,316 @@
+// Non-RHS device kernels of the stepping path: the ghost fill (scatter, same-level copies,
+// injection, the Dirichlet hook, tensor-product Lagrange prolongation), the RK4 stage
+// updates of the plain form, the characteristic speed, the error norm, the analytic
+// initial state, the :pasted overwrite and the sampled gauge source.
+#pragma once
+#include <cstdint>
+
+#include "physics.cuh"
+
+namespace tgh {
+
+// A run of points along x copied from a primary owner: the destination is a working array
+// (block, linear work index), the source an owned point (block, i, j, k) read from either the
+// state vector or the source block's working array; step is 1 (same level) or 2^d (injection
+// from a level d finer).
+struct CopyRun {
+  int dst_b, dst_w;
+  int src_b, si, sj, sk;
+  int len, step;
+};
+// One prolonged point: the destination, the coarse block, the coarse work index of the
+// stencil box's lower corner and a bit per axis saying whether the axis interpolates.
+struct ProlongPt {
+  int dst_b, dst_w;
+  int src_b, src_w;
+  int odd;
+};
+// One Dirichlet ghost point: the destination; the position is recomputed from the block.
+struct HookPt {
+  int b, w;
+};
+
+struct Geo {
+  int N1, Wd, G;
+  long S, Wv;  // points per block in state / work layout
+};
+
+// The position of point (i, j, k) of block b (i may lie in the ghost zone): blk holds per
+// block the domain's low corner, the spacing and the integer corner, 8 doubles; the point
+// is lo + (corner + i) h with the product and the sum each rounded.
+__device__ __forceinline__ void point_pos(const double* blk, int b, int i, int j, int k, double* x) {
+  const double* bl = blk + 8 * b;
+  x[0] = __dadd_rn(bl[0], __dmul_rn(bl[4] + (double)i, bl[3]));
+  x[1] = __dadd_rn(bl[1], __dmul_rn(bl[5] + (double)j, bl[3]));
+  x[2] = __dadd_rn(bl[2], __dmul_rn(bl[6] + (double)k, bl[3]));
+}
+
+// stage 0 of a fill: copies. from_work: read the source from the working array (batched
+// form, where the state lives in the working array), else from the state vector u.
+__global__ void fill_copy_kernel(const CopyRun* __restrict__ runs, int nruns, const double* __restrict__ u,
+                                 double* __restrict__ work, Geo g, int from_work) {
+  // one warp per run, lanes over the run's points, loop over variables
+  const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  if (warp >= nruns) return;
+  const CopyRun r = runs[warp];
+  for (int e = lane; e < r.len; e += 32) {
+    const double* src;
+    long sstride;
+    if (from_work) {
+      src = u + (long)r.src_b * NV * g.Wv + (r.si + e * r.step + g.G) +
+            (long)g.Wd * ((r.sj + g.G) + (long)g.Wd * (r.sk + g.G));
+      sstride = g.Wv;
+    } else {
+      src = u + (long)r.src_b * NV * g.S + (r.si + e * r.step) + (long)g.N1 * (r.sj + (long)g.N1 * r.sk);
+      sstride = g.S;
+    }
+    double* dst = work + (long)r.dst_b * NV * g.Wv + r.dst_w + e;
+#pragma unroll 4
+    for (int v = 0; v < NV; ++v) dst[v * g.Wv] = src[v * sstride];
+  }
+}
+
+// the Dirichlet hook: the analytic state (through the core rule) at each outer ghost point
+__global__ void fill_hook_kernel(const HookPt* __restrict__ pts, int n, const double* __restrict__ blk,
+                                 double* __restrict__ work, Geo g, const Case cs, double t) {
+  const int id = blockIdx.x * blockDim.x + threadIdx.x;
+  if (id >= n) return;
+  const HookPt p = pts[id];
+  const int i = p.w % g.Wd, j = (p.w / g.Wd) % g.Wd, k = p.w / (g.Wd * g.Wd);
+  double x[3];
+  point_pos(blk, p.b, i - g.G, j - g.G, k - g.G, x);
+  double v20[NV];
+  exact_state(cs, t, x, v20);
+  double* dst = work + (long)p.b * NV * g.Wv + p.w;
+#pragma unroll
+  for (int v = 0; v < NV; ++v) dst[v * g.Wv] = v20[v];
+}
+
+// tensor-product Lagrange prolongation of order P from the coarse block's filled working
+// array, summed with x innermost, then y, then z; products and sums rounded one by one
+__constant__ double c_wprol[10];
+
+template <int P>
+__global__ void fill_prolong_kernel(const ProlongPt* __restrict__ pts, int n, double* __restrict__ work, Geo g) {
+  const int id = blockIdx.x * blockDim.x + threadIdx.x;
+  if (id >= n * NV) return;
+  const int pi = id / NV, v = id % NV;
+  const ProlongPt p = pts[pi];
+  const int cx = (p.odd & 1) ? P : 1, cy = (p.odd & 2) ? P : 1, cz = (p.odd & 4) ? P : 1;
+  const double* src = work + (long)p.src_b * NV * g.Wv + (long)v * g.Wv + p.src_w;
+  const long sy = g.Wd, sz = (long)g.Wd * g.Wd;
+  double szv = 0.0;
+  for (int kz = 0; kz < cz; ++kz) {
+    const double wz = cz == 1 ? 1.0 : c_wprol[kz];
+    double syv = 0.0;
+    for (int ky = 0; ky < cy; ++ky) {
+      const double wy = cy == 1 ? 1.0 : c_wprol[ky];
+      double sxv = 0.0;
+      const double* row = src + kz * sz + ky * sy;
+      for (int kx = 0; kx < cx; ++kx) {
+        const double wx = cx == 1 ? 1.0 : c_wprol[kx];
+        const double term = __dmul_rn(wx, row[kx]);
+        sxv = kx == 0 ? term : __dadd_rn(sxv, term);
+      }
+      const double ty = __dmul_rn(wy, sxv);
+      syv = ky == 0 ? ty : __dadd_rn(syv, ty);
+    }
+    const double tz = __dmul_rn(wz, syv);
+    szv = kz == 0 ? tz : __dadd_rn(szv, tz);
+  }
+  work[(long)p.dst_b * NV * g.Wv + (long)v * g.Wv + p.dst_w] = szv;
+}
+
+// plain-form RK4 stage updates over the whole state vector (each one fused multiply-add):
+//  kind 0: acc = u + cb k, y = u + ca k   kind 1: acc = acc + cb k, y = u + ca k
+//  kind 2: u = acc + cb k
+__global__ void stage_update_kernel(int kind, long n, const double* __restrict__ k, const double* __restrict__ u0,
+                                    double* __restrict__ acc, double* __restrict__ y, double* __restrict__ uout,
+                                    double ca, double cb) {
+  for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) {
+    const double kv = k[i];
+    if (kind == 0) {
+      const double uv = u0[i];
+      acc[i] = fma(cb, kv, uv);
+      y[i] = fma(ca, kv, uv);
+    } else if (kind == 1) {
+      acc[i] = fma(cb, kv, acc[i]);
+      y[i] = fma(ca, kv, u0[i]);
+    } else {
+      uout[i] = fma(cb, kv, acc[i]);
+    }
+  }
+}
+
+__device__ __forceinline__ bool evolved(const Case& cs, double t, const double* x) {
+  return cs.interior == TGH_INT_NONE ? true : interior_radius(cs, t, x) >= cs.r1;
+}
+
+// The speed lambda = alpha sqrt(tr gamma^{ij}) + |beta| at every evolved owned point and the
+// count of non-finite evolved values; reduced per CTA into scratch[0] (max, as the ordered
+// bits of a non-negative double or a NaN) and scratch[1] (count).
+__global__ void speed_kernel(const double* __restrict__ u, const double* __restrict__ blk, Geo g, long npts,
+                             const Case cs, double t, unsigned long long* scratch) {
+  const long p = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  double lam = 0.0;
+  unsigned long long bad = 0;
+  if (p < npts) {
+    const int b = (int)(p / g.S);
+    const long ip = p - (long)b * g.S;
+    const int k = (int)(ip / ((long)g.N1 * g.N1)), j = (int)((ip / g.N1) % g.N1), i = (int)(ip % g.N1);
+    double x[3];
+    point_pos(blk, b, i, j, k, x);
+    if (evolved(cs, t, x)) {
+      const double* q = u + (long)b * NV * g.S + ip;
+      double hv[NC];
+      for (int v = 0; v < NV; ++v) {
+        const double a = q[v * g.S];
+        if (!isfinite(a)) ++bad;
+        if (v < NC) hv[v] = a;
+      }
+      Coef<double> C;
+      metric_quantities(hv, C);
+      lam = C.alpha * sqrt(C.gamu[0] + C.gamu[3] + C.gamu[5]) +
+            sqrt(C.beta[0] * C.beta[0] + C.beta[1] * C.beta[1] + C.beta[2] * C.beta[2]);
+    }
+  }
+  unsigned long long bits = isnan(lam) ? 0x7ff8000000000000ull : (unsigned long long)__double_as_longlong(lam);
+  for (int o = 16; o > 0; o >>= 1) {
+    unsigned long long ob = __shfl_down_sync(0xffffffffu, bits, o);
+    unsigned long long obad = __shfl_down_sync(0xffffffffu, bad, o);
+    bits = ob > bits ? ob : bits;
+    bad += obad;
+  }
+  if ((threadIdx.x & 31) == 0) {
+    if (bits) atomicMax(scratch, bits);
+    if (bad) atomicAdd(scratch + 1, bad);
+  }
+}
+
+// |u - u_exact| over the evolved primaries of the settled working array: per point the
+// squared magnitude weighted by h^3, the weight and the magnitude; per CTA partial sums in
+// a fixed order into part[3 * blockIdx.x + {0,1,2}] (sum e^2 h^3, sum h^3, max e)
+__global__ void error_kernel(const double* __restrict__ work, const double* __restrict__ blk,
+                             const uint8_t* __restrict__ primary, Geo g, long npts, const Case cs, double t,
+                             double* part) {
+  __shared__ double sh[3][128];
+  const long p = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  double s2 = 0.0, vol = 0.0, mx = 0.0;
+  if (p < npts && primary[p]) {
+    const int b = (int)(p / g.S);
+    const long ip = p - (long)b * g.S;
+    const int k = (int)(ip / ((long)g.N1 * g.N1)), j = (int)((ip / g.N1) % g.N1), i = (int)(ip % g.N1);
+    double x[3];
+    point_pos(blk, b, i, j, k, x);
+    if (evolved(cs, t, x)) {
+      double ex[NV];
+      exact_state(cs, t, x, ex);
+      const double* q = work + (long)b * NV * g.Wv + (i + g.G) + (long)g.Wd * ((j + g.G) + (long)g.Wd * (k + g.G));
+      double e2 = 0.0;
+      for (int v = 0; v < NV; ++v) {
+        const double d = q[v * g.Wv] - ex[v];
+        e2 = __dadd_rn(e2, __dmul_rn(d, d));
+      }
+      const double e = sqrt(e2);
+      const double h = blk[8 * b + 3];
+      const double w = h * h * h;
+      s2 = e * e * w;
+      vol = w;
+      mx = e;
+    }
+  }
+  sh[0][threadIdx.x] = s2;
+  sh[1][threadIdx.x] = vol;
+  sh[2][threadIdx.x] = mx;
+  __syncthreads();
+  for (int o = blockDim.x / 2; o > 0; o >>= 1) {
+    if (threadIdx.x < o) {
+      sh[0][threadIdx.x] += sh[0][threadIdx.x + o];
+      sh[1][threadIdx.x] += sh[1][threadIdx.x + o];
+      sh[2][threadIdx.x] = fmax(sh[2][threadIdx.x], sh[2][threadIdx.x + o]);
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    part[3 * blockIdx.x] = sh[0][0];
+    part[3 * blockIdx.x + 1] = sh[1][0];
+    part[3 * blockIdx.x + 2] = sh[2][0];
+  }
+}
+__global__ void error_final_kernel(const double* part, int n, double* out) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  double s2 = 0.0, vol = 0.0, mx = 0.0;
+  for (int i = 0; i < n; ++i) {
+    s2 += part[3 * i];
+    vol += part[3 * i + 1];
+    mx = fmax(mx, part[3 * i + 2]);
+  }
+  out[0] = vol == 0.0 ? 0.0 : sqrt(s2 / vol);
+  out[1] = mx;
+}
+
+// the case's state at every owned point (initial_state!); paste_only: only inside r_1 (the
+// :pasted limiter, gh_paste_kernel!)
+__global__ void exact_state_kernel(double* __restrict__ u, const double* __restrict__ blk, Geo g, long npts,
+                                   const Case cs, double t, int paste_only) {
+  const long p = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= npts) return;
+  const int b = (int)(p / g.S);
+  const long ip = p - (long)b * g.S;
+  const int k = (int)(ip / ((long)g.N1 * g.N1)), j = (int)((ip / g.N1) % g.N1), i = (int)(ip % g.N1);
+  double x[3];
+  point_pos(blk, b, i, j, k, x);
+  if (paste_only && interior_radius(cs, t, x) >= cs.r1) return;
+  double v20[NV];
+  exact_state(cs, t, x, v20);
+  double* q = u + (long)b * NV * g.S + ip;
+#pragma unroll
+  for (int v = 0; v < NV; ++v) q[v * g.S] = v20[v];
+}
+
+// the sampled gauge source at every owned point, through the core rule (src/gauge.jl:156-170)
+__global__ void sample_gauge_kernel(double* __restrict__ H, const double* __restrict__ blk, Geo g, long npts,
+                                    const Case cs, double t) {
+  const long p = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= npts) return;
+  const int b = (int)(p / g.S);
+  const long ip = p - (long)b * g.S;
+  const int k = (int)(ip / ((long)g.N1 * g.N1)), j = (int)((ip / g.N1) % g.N1), i = (int)(ip % g.N1);
+  double x[3], xc[3], v20[NV];
+  point_pos(blk, b, i, j, k, x);
+  core_position(cs, t, x, xc);
+  gauge_tuple(cs, t, xc, v20);
+  double* q = H + (long)b * NV * g.S + ip;
+  for (int v = 0; v < NV; ++v) q[v * g.S] = v20[v];
+}
+
+// owned values of the working array back to the state vector (the batched form's output)
+__global__ void gather_kernel(const double* __restrict__ work, double* __restrict__ u, Geo g, long npts) {
+  const long p = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= npts) return;
+  const int b = (int)(p / g.S);
+  const long ip = p - (long)b * g.S;
+  const int k = (int)(ip / ((long)g.N1 * g.N1)), j = (int)((ip / g.N1) % g.N1), i = (int)(ip % g.N1);
+  const double* q = work + (long)b * NV * g.Wv + (i + g.G) + (long)g.Wd * ((j + g.G) + (long)g.Wd * (k + g.G));
+  double* o = u + (long)b * NV * g.S + ip;
+#pragma unroll
+  for (int v = 0; v < NV; ++v) o[v * g.S] = q[v * g.Wv];
+}
+
+// sustained FP64 fused multiply-add throughput probe: 8 independent chains per thread
+__global__ void fp64_probe_kernel(double* out, int iters, double a, double b) {
+  double x0 = threadIdx.x * 1e-9, x1 = x0 + 1e-9, x2 = x0 + 2e-9, x3 = x0 + 3e-9;
+  double x4 = x0 + 4e-9, x5 = x0 + 5e-9, x6 = x0 + 6e-9, x7 = x0 + 7e-9;
+  for (int i = 0; i < iters; ++i) {
+#pragma unroll
+    for (int r = 0; r < 16; ++r) {
+      x0 = fma(x0, a, b); x1 = fma(x1, a, b); x2 = fma(x2, a, b); x3 = fma(x3, a, b);
+      x4 = fma(x4, a, b); x5 = fma(x5, a, b); x6 = fma(x6, a, b); x7 = fma(x7, a, b);
+    }
+  }
+  const double s = ((x0 + x1) + (x2 + x3)) + ((x4 + x5) + (x6 + x7));
+  if (s == 12345.0) out[0] = s;
+}
+
+}  // namespace tgh

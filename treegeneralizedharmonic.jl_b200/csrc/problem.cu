@@ -1,0 +1,703 @@
+// The C ABI of include/tgh.h: problem construction (GHProblem), the ghost-fill plan, the
+// verbs and the two RK4 forms. Host C++; all arithmetic runs in the kernels of
+// kernels.cuh and rhs.cuh.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdint>
+#include <cstring>
+#include <string>
+#include <unordered_map>
+#include <vector>
+
+#include "../../include/tgh.h"
+#include "kernels.cuh"
+#include "rhs_inst.cuh"
+
+using namespace tgh;
+
+struct GraphKey {
+  double t, dt;
+  int nsteps;
+};
+
+struct tgh_problem {
+  tgh_config cfg;
+  int q, G, N, N1, Wd, nb, maxlevel = 0;
+  double lo[3], h0;
+  int cells0[3], periodic[3];
+  std::vector<int> level, corner;
+  std::vector<std::unordered_map<int64_t, int>> lut;
+  Geo geo;
+  long S, Wv, npts;
+  Case cs;
+  bool diss = false, intr = false;
+  cudaStream_t stream = nullptr;
+  std::string err;
+  // device buffers
+  double* work = nullptr;     // the ghosted working array (also W0 of the batched form)
+  double* Hsrc = nullptr;
+  double* blk = nullptr;      // per block: domain lo (3), h, integer corner (3), pad
+  uint8_t* primary = nullptr; // per owned point: 1 where this block holds the primary copy
+  CopyRun* runs = nullptr;
+  int nruns = 0;
+  HookPt* hooks = nullptr;
+  int nhooks = 0;
+  std::vector<ProlongPt*> prol;  // per level 1..maxlevel
+  std::vector<int> nprol;
+  unsigned long long* scratch = nullptr;  // speed reduction: max bits, non-finite count
+  double* part = nullptr;                 // error-norm partials + result
+  int npart = 0;
+  // plain-form RK4 buffers (state layout)
+  double *k = nullptr, *acc = nullptr, *y = nullptr, *u0 = nullptr;
+  // batched-form buffers
+  double *W1 = nullptr, *W2 = nullptr, *bacc = nullptr;
+  cudaGraphExec_t gexec = nullptr;
+  GraphKey gkey{0, 0, 0};
+  const double* gu = nullptr;
+};
+
+#define CK(call)                                                         \
+  do {                                                                   \
+    cudaError_t e_ = (call);                                             \
+    if (e_ != cudaSuccess) {                                             \
+      p->err = std::string(#call) + ": " + cudaGetErrorString(e_);       \
+      return TGH_ERR_CUDA;                                               \
+    }                                                                    \
+  } while (0)
+
+static int fail(tgh_problem* p, int code, const std::string& msg) {
+  p->err = msg;
+  return code;
+}
+
+// ---- the forest: owners, positions ----
+static inline int64_t bkey(int64_t bx, int64_t by, int64_t bz) { return ((bx * 1048576) + by) * 1048576 + bz; }
+
+// The primary owner of lattice point n of level l: the finest leaf of level >= l holding the
+// point (closed blocks), and among a level's leaves the one with the point on its lower face.
+static bool find_owner(const tgh_problem* p, int l, const int64_t n[3], int& leaf, int loc[3], int& lev) {
+  for (int k = p->maxlevel; k >= l; --k) {
+    int64_t m[3], cand[3][2];
+    int nc[3];
+    for (int d = 0; d < 3; ++d) {
+      m[d] = n[d] << (k - l);
+      int64_t c = m[d] / p->N;
+      nc[d] = 0;
+      cand[d][nc[d]++] = c;
+      if (m[d] % p->N == 0) cand[d][nc[d]++] = c - 1;
+    }
+    for (int iz = 0; iz < nc[2]; ++iz)
+      for (int iy = 0; iy < nc[1]; ++iy)
+        for (int ix = 0; ix < nc[0]; ++ix) {
+          auto it = p->lut[k].find(bkey(cand[0][ix], cand[1][iy], cand[2][iz]));
+          if (it == p->lut[k].end()) continue;
+          leaf = it->second;
+          for (int d = 0; d < 3; ++d) loc[d] = (int)(m[d] - p->corner[3 * leaf + d]);
+          lev = k;
+          return true;
+        }
+  }
+  return false;
+}
+
+// a leaf of level exactly l whose closed box contains the (half-)integer position n/2 of
+// level l+1's point n
+static int coarse_cover(const tgh_problem* p, int l, const int64_t nf[3]) {
+  int64_t lo[3], hi[3];
+  for (int d = 0; d < 3; ++d) {
+    lo[d] = nf[d] >> 1;                     // floor(n/2)
+    hi[d] = (nf[d] & 1) ? lo[d] + 1 : lo[d];
+  }
+  for (int dz = -1; dz <= 0; ++dz)
+    for (int dy = -1; dy <= 0; ++dy)
+      for (int dx = -1; dx <= 0; ++dx) {
+        int64_t c[3] = {lo[0] / p->N + dx, lo[1] / p->N + dy, lo[2] / p->N + dz};
+        auto it = p->lut[l].find(bkey(c[0], c[1], c[2]));
+        if (it == p->lut[l].end()) continue;
+        const int b = it->second;
+        bool ok = true;
+        for (int d = 0; d < 3; ++d) {
+          const int64_t c0 = p->corner[3 * b + d];
+          if (lo[d] < c0 || hi[d] > c0 + p->N) ok = false;
+        }
+        if (ok) return b;
+      }
+  return -1;
+}
+
+static Case make_case(const tgh_config& c) {
+  Case k;
+  std::memset(&k, 0, sizeof(k));
+  k.bg = c.bg;
+  const double* u = c.bg.boost;
+  const double u2 = u[0] * u[0] + u[1] * u[1] + u[2] * u[2];
+  k.boosted = (c.bg.kind == TGH_BG_KERR_SCHILD && u2 > 0.0) ? 1 : 0;
+  const double gam = 1.0 / std::sqrt(1.0 - u2);
+  for (int i = 0; i < 4; ++i)
+    for (int j = 0; j < 4; ++j) k.L[i][j] = i == j ? 1.0 : 0.0;
+  if (k.boosted) {
+    k.L[0][0] = gam;
+    for (int i = 0; i < 3; ++i) {
+      k.L[0][i + 1] = k.L[i + 1][0] = gam * u[i];
+      for (int j = 0; j < 3; ++j) k.L[i + 1][j + 1] = (i == j ? 1.0 : 0.0) + (gam - 1.0) * u[i] * u[j] / u2;
+    }
+  }
+  k.gauge = c.gauge;
+  {
+    const double* v = c.ks_velocity;
+    const double* a = c.ks_spin;
+    const double v2 = v[0] * v[0] + v[1] * v[1] + v[2] * v[2];
+    const double g = 1.0 / std::sqrt(1.0 - v2);
+    const double va = v[0] * a[0] + v[1] * a[1] + v[2] * a[2];
+    k.ksM = c.ks_M;
+    k.ksS[0] = g * va;
+    for (int i = 0; i < 3; ++i) k.ksS[i + 1] = v2 == 0.0 ? a[i] : a[i] + ((g - 1.0) * va / v2) * v[i];
+    k.ksU[0] = g;
+    for (int i = 0; i < 3; ++i) k.ksU[i + 1] = g * v[i];
+  }
+  k.damping = c.damping;
+  k.g0 = c.gamma0;
+  k.dnear = c.damp_near;
+  k.dfar = c.damp_far;
+  k.dwidth = c.damp_width;
+  k.g2 = c.gamma2;
+  k.dissipation = c.dissipation;
+  k.eps = c.eps_ko;
+  k.eout = c.eps_out;
+  k.ein = c.eps_in;
+  k.er1 = c.eps_r1;
+  k.erh = c.eps_rh;
+  k.interior = c.interior;
+  for (int i = 0; i < 3; ++i) {
+    k.dc0[i] = c.damp_c0[i];
+    k.dv[i] = c.damp_v[i];
+    k.ec0[i] = c.eps_c0[i];
+    k.ev[i] = c.eps_v[i];
+    k.ic0[i] = c.int_c0[i];
+    k.iv[i] = c.int_v[i];
+  }
+  k.r0 = c.r0;
+  k.r1 = c.r1;
+  k.rho_max = c.rho_max;
+  k.w_ramp = c.w_ramp;
+  k.rho_ramp = c.rho_ramp;
+  return k;
+}
+
+static unsigned grid_for(long n, int threads) { return (unsigned)((n + threads - 1) / threads); }
+
+// The fill plan: for every point of every block's working array, where its value comes from.
+static int build_plan(tgh_problem* p) {
+  std::vector<CopyRun> runs;
+  std::vector<HookPt> hooks;
+  std::vector<std::vector<ProlongPt>> prol(p->maxlevel + 1);
+  std::vector<uint8_t> prim((size_t)p->npts, 0);
+  const int Wd = p->Wd, G = p->G, P = p->q + 2;
+  for (int b = 0; b < p->nb; ++b) {
+    const int l = p->level[b];
+    for (int k = 0; k < Wd; ++k)
+      for (int j = 0; j < Wd; ++j) {
+        CopyRun cur{};
+        bool open = false;
+        for (int i = 0; i < Wd; ++i) {
+          int64_t n[3] = {(int64_t)p->corner[3 * b] + i - G, (int64_t)p->corner[3 * b + 1] + j - G,
+                          (int64_t)p->corner[3 * b + 2] + k - G};
+          bool outside = false;
+          for (int d = 0; d < 3; ++d) {
+            const int64_t per = (int64_t)p->cells0[d] << l;
+            if (p->periodic[d]) {
+              n[d] %= per;
+              if (n[d] < 0) n[d] += per;
+            } else if (n[d] < 0 || n[d] > per) {
+              outside = true;
+            }
+          }
+          const int w = i + Wd * (j + Wd * k);
+          int leaf = -1, loc[3], lev = -1;
+          if (!outside && find_owner(p, l, n, leaf, loc, lev)) {
+            const int step = 1 << (lev - l);
+            const bool own = i >= G && i <= G + p->N && j >= G && j <= G + p->N && k >= G && k <= G + p->N;
+            if (own && leaf == b) {
+              prim[(size_t)b * p->S + (i - G) + (size_t)p->N1 * ((j - G) + (size_t)p->N1 * (k - G))] = 1;
+            }
+            if (open && cur.src_b == leaf && cur.step == step && cur.sj == loc[1] && cur.sk == loc[2] &&
+                cur.si + cur.len * step == loc[0] && cur.dst_w + cur.len == w) {
+              cur.len++;
+            } else {
+              if (open) runs.push_back(cur);
+              cur = CopyRun{b, w, leaf, loc[0], loc[1], loc[2], 1, step};
+              open = true;
+            }
+            continue;
+          }
+          if (open) {
+            runs.push_back(cur);
+            open = false;
+          }
+          if (outside) {
+            hooks.push_back(HookPt{b, w});
+            continue;
+          }
+          if (l == 0) return fail(p, TGH_ERR_ARG, "a lattice point is covered by no leaf of the forest");
+          const int c = coarse_cover(p, l - 1, n);
+          if (c < 0)
+            return fail(p, TGH_ERR_ARG,
+                        "a prolonged ghost point has no covering leaf one level coarser (the forest is not 2:1 balanced)");
+          int odd = 0;
+          int64_t base[3];
+          for (int d = 0; d < 3; ++d) {
+            if (n[d] & 1) {
+              odd |= 1 << d;
+              base[d] = (n[d] >> 1) - (P / 2 - 1);
+            } else {
+              base[d] = n[d] >> 1;
+            }
+            const int64_t rel = base[d] - p->corner[3 * c + d] + G;
+            const int64_t ext = (n[d] & 1) ? P : 1;
+            if (rel < 0 || rel + ext > Wd)
+              return fail(p, TGH_ERR_ARG, "a prolongation stencil leaves the coarse block's ghost zone");
+          }
+          const int sw = (int)((base[0] - p->corner[3 * c] + G) +
+                               Wd * ((base[1] - p->corner[3 * c + 1] + G) + (int64_t)Wd * (base[2] - p->corner[3 * c + 2] + G)));
+          prol[l].push_back(ProlongPt{b, w, c, sw, odd});
+        }
+        if (open) runs.push_back(cur);
+      }
+  }
+  p->nruns = (int)runs.size();
+  p->nhooks = (int)hooks.size();
+  CK(cudaMalloc(&p->runs, std::max<size_t>(1, runs.size()) * sizeof(CopyRun)));
+  CK(cudaMemcpy(p->runs, runs.data(), runs.size() * sizeof(CopyRun), cudaMemcpyHostToDevice));
+  CK(cudaMalloc(&p->hooks, std::max<size_t>(1, hooks.size()) * sizeof(HookPt)));
+  if (!hooks.empty()) CK(cudaMemcpy(p->hooks, hooks.data(), hooks.size() * sizeof(HookPt), cudaMemcpyHostToDevice));
+  p->prol.assign(p->maxlevel + 1, nullptr);
+  p->nprol.assign(p->maxlevel + 1, 0);
+  for (int l = 1; l <= p->maxlevel; ++l) {
+    p->nprol[l] = (int)prol[l].size();
+    CK(cudaMalloc(&p->prol[l], std::max<size_t>(1, prol[l].size()) * sizeof(ProlongPt)));
+    if (!prol[l].empty())
+      CK(cudaMemcpy(p->prol[l], prol[l].data(), prol[l].size() * sizeof(ProlongPt), cudaMemcpyHostToDevice));
+  }
+  CK(cudaMalloc(&p->primary, (size_t)p->npts));
+  CK(cudaMemcpy(p->primary, prim.data(), (size_t)p->npts, cudaMemcpyHostToDevice));
+  return TGH_OK;
+}
+
+// Lagrange weights of P points at the midpoint of the middle pair (exact rationals,
+// rounded once): numerators over 2^(2P-3) computed in integers.
+static void prolong_weights(int P, double* w) {
+  // w_k = prod_{m != k} (0 - x_m)/(x_k - x_m), x_m = m - (P/2 - 1) - 1/2, in doubled units
+  for (int k = 0; k < P; ++k) {
+    long double num = 1, den = 1;
+    int64_t inum = 1, iden = 1;
+    for (int m = 0; m < P; ++m) {
+      if (m == k) continue;
+      const int64_t xm = 2 * (m - (P / 2 - 1)) - 1, xk = 2 * (k - (P / 2 - 1)) - 1;
+      inum *= -xm;
+      iden *= (xk - xm);
+    }
+    (void)num;
+    (void)den;
+    w[k] = (double)inum / (double)iden;
+  }
+}
+
+// ---- the fill: stage 0 (copies, hooks), then prolongation level by level ----
+static int launch_fill(tgh_problem* p, const double* src, bool from_work, double* work, double t) {
+  const int T = 256;
+  if (p->nruns) {
+    fill_copy_kernel<<<grid_for((long)p->nruns * 32, T), T, 0, p->stream>>>(p->runs, p->nruns, src, work, p->geo,
+                                                                           from_work ? 1 : 0);
+    CK(cudaGetLastError());
+  }
+  if (p->nhooks) {
+    fill_hook_kernel<<<grid_for(p->nhooks, 128), 128, 0, p->stream>>>(p->hooks, p->nhooks, p->blk, work, p->geo,
+                                                                      p->cs, t);
+    CK(cudaGetLastError());
+  }
+  for (int l = 1; l <= p->maxlevel; ++l) {
+    if (!p->nprol[l]) continue;
+    const long n = (long)p->nprol[l] * NV;
+    switch (p->q + 2) {
+      case 4: fill_prolong_kernel<4><<<grid_for(n, T), T, 0, p->stream>>>(p->prol[l], p->nprol[l], work, p->geo); break;
+      case 6: fill_prolong_kernel<6><<<grid_for(n, T), T, 0, p->stream>>>(p->prol[l], p->nprol[l], work, p->geo); break;
+      case 8: fill_prolong_kernel<8><<<grid_for(n, T), T, 0, p->stream>>>(p->prol[l], p->nprol[l], work, p->geo); break;
+      default: fill_prolong_kernel<10><<<grid_for(n, T), T, 0, p->stream>>>(p->prol[l], p->nprol[l], work, p->geo); break;
+    }
+    CK(cudaGetLastError());
+  }
+  return TGH_OK;
+}
+
+static int launch_rhs(tgh_problem* p, const RhsArgs& a, int mode) {
+  cudaError_t e;
+  switch (p->q) {
+    case 2: e = launch_rhs_q2(p->diss, mode, p->intr, a.npts, p->stream, p->cs, a); break;
+    case 4: e = launch_rhs_q4(p->diss, mode, p->intr, a.npts, p->stream, p->cs, a); break;
+    case 6: e = launch_rhs_q6(p->diss, mode, p->intr, a.npts, p->stream, p->cs, a); break;
+    default: e = launch_rhs_q8(p->diss, mode, p->intr, a.npts, p->stream, p->cs, a); break;
+  }
+  CK(e);
+  return TGH_OK;
+}
+
+static RhsArgs base_args(tgh_problem* p, const double* work, double t) {
+  RhsArgs a;
+  std::memset(&a, 0, sizeof(a));
+  a.work = work;
+  a.Hsrc = p->Hsrc;
+  a.blk = p->blk;
+  a.N1 = p->N1;
+  a.Wd = p->Wd;
+  a.G = p->G;
+  a.npts = p->npts;
+  a.t = t;
+  return a;
+}
+
+static int stage_limit_impl(tgh_problem* p, double* u, double t) {
+  if (p->cfg.interior != TGH_INT_PASTED) return TGH_OK;
+  exact_state_kernel<<<grid_for(p->npts, 128), 128, 0, p->stream>>>(u, p->blk, p->geo, p->npts, p->cs, t, 1);
+  CK(cudaGetLastError());
+  return TGH_OK;
+}
+
+extern "C" {
+
+int tgh_problem_create(const tgh_config* cfg, const tgh_mesh* m, void* cuda_stream, int margin_check,
+                       tgh_problem** out) {
+  *out = nullptr;
+  tgh_problem* p = new tgh_problem();
+  *out = p;
+  p->cfg = *cfg;
+  p->stream = (cudaStream_t)cuda_stream;
+  const int q = cfg->q;
+  if (q < 2 || q > 8 || q % 2) return fail(p, TGH_ERR_ARG, "the finite-difference order must be even and in 2..8, got " + std::to_string(q));
+  if (m->N < 2 * (q / 2 + 1)) return fail(p, TGH_ERR_ARG, "the block edge N must be at least 2G");
+  if (m->nblocks < 1) return fail(p, TGH_ERR_ARG, "the forest has no leaves");
+  p->q = q;
+  p->G = q / 2 + 1;
+  p->N = m->N;
+  p->N1 = m->N + 1;
+  p->Wd = m->N + 2 * p->G + 1;
+  p->nb = m->nblocks;
+  p->h0 = m->h0;
+  for (int d = 0; d < 3; ++d) {
+    p->lo[d] = m->lo[d];
+    p->cells0[d] = m->cells0[d];
+    p->periodic[d] = m->periodic[d];
+    if (m->cells0[d] % m->N) return fail(p, TGH_ERR_ARG, "the domain is not a whole number of blocks");
+  }
+  p->level.assign(m->level, m->level + m->nblocks);
+  p->corner.assign(m->corner, m->corner + 3 * m->nblocks);
+  for (int b = 0; b < p->nb; ++b) {
+    if (p->level[b] < 0 || p->level[b] > 20) return fail(p, TGH_ERR_ARG, "block level out of range");
+    p->maxlevel = std::max(p->maxlevel, p->level[b]);
+    for (int d = 0; d < 3; ++d)
+      if (p->corner[3 * b + d] % p->N) return fail(p, TGH_ERR_ARG, "a block corner is not a multiple of N");
+  }
+  p->lut.resize(p->maxlevel + 1);
+  for (int b = 0; b < p->nb; ++b) {
+    auto key = bkey(p->corner[3 * b] / p->N, p->corner[3 * b + 1] / p->N, p->corner[3 * b + 2] / p->N);
+    if (!p->lut[p->level[b]].emplace(key, b).second) return fail(p, TGH_ERR_ARG, "two leaves share a corner and level");
+  }
+  p->S = (long)p->N1 * p->N1 * p->N1;
+  p->Wv = (long)p->Wd * p->Wd * p->Wd;
+  p->npts = p->S * p->nb;
+  p->geo = Geo{p->N1, p->Wd, p->G, p->S, p->Wv};
+  p->cs = make_case(*cfg);
+  p->diss = cfg->dissipation == TGH_DISS_CONSTANT ? cfg->eps_ko != 0.0 : !(cfg->eps_out == 0.0 && cfg->eps_in == 0.0);
+  p->intr = cfg->interior != TGH_INT_NONE;
+  if (p->intr) {
+    if (!(cfg->r0 > 0.0 && cfg->r1 > cfg->r0))
+      return fail(p, TGH_ERR_RADII, "the interior needs 0 < r_0 < r_1");
+    if (!(cfg->w_ramp > 0 && cfg->w_ramp <= 1 && cfg->rho_ramp > 0 && cfg->rho_ramp <= 1))
+      return fail(p, TGH_ERR_ARG, "the ramp fractions must lie in (0, 1]");
+    if (margin_check) {
+      // the layer must be resolved: r_1 - r_0 >= 2 (G + 1) h at the finest spacing present
+      const double hmin = std::ldexp(p->h0, -p->maxlevel);
+      if (cfg->r1 - cfg->r0 < 2.0 * (p->G + 1) * hmin)
+        return fail(p, TGH_ERR_RADII, "the damping layer is too thin: r_1 - r_0 < 2(G+1)h");
+      if (cfg->bg.kind == TGH_BG_KERR_SCHILD && cfg->r0 <= std::fabs(cfg->bg.a))
+        return fail(p, TGH_ERR_RADII, "the frozen core does not contain the chart's singular disk |x| <= |a|");
+    }
+  }
+  // per-block geometry
+  std::vector<double> blk(8 * (size_t)p->nb, 0.0);
+  for (int b = 0; b < p->nb; ++b) {
+    for (int d = 0; d < 3; ++d) {
+      blk[8 * b + d] = p->lo[d];
+      blk[8 * b + 4 + d] = (double)p->corner[3 * b + d];
+    }
+    blk[8 * b + 3] = std::ldexp(p->h0, -p->level[b]);
+  }
+  CK(cudaMalloc(&p->blk, blk.size() * sizeof(double)));
+  CK(cudaMemcpy(p->blk, blk.data(), blk.size() * sizeof(double), cudaMemcpyHostToDevice));
+  CK(cudaMalloc(&p->work, (size_t)p->Wv * NV * p->nb * sizeof(double)));
+  CK(cudaMemsetAsync(p->work, 0, (size_t)p->Wv * NV * p->nb * sizeof(double), p->stream));
+  CK(cudaMalloc(&p->scratch, 2 * sizeof(unsigned long long)));
+  p->npart = (int)grid_for(p->npts, 128);
+  CK(cudaMalloc(&p->part, (3 * (size_t)p->npart + 2) * sizeof(double)));
+  double wp[10] = {0};
+  prolong_weights(p->q + 2, wp);
+  CK(cudaMemcpyToSymbol(c_wprol, wp, sizeof(wp)));
+  int s = build_plan(p);
+  if (s) return s;
+  if (cfg->gauge == TGH_GAUGE_SAMPLED) {
+    CK(cudaMalloc(&p->Hsrc, (size_t)p->S * NV * p->nb * sizeof(double)));
+    sample_gauge_kernel<<<grid_for(p->npts, 64), 64, 0, p->stream>>>(p->Hsrc, p->blk, p->geo, p->npts, p->cs, 0.0);
+    CK(cudaGetLastError());
+  }
+  CK(cudaStreamSynchronize(p->stream));
+  return TGH_OK;
+}
+
+void tgh_problem_destroy(tgh_problem* p) {
+  if (!p) return;
+  if (p->gexec) cudaGraphExecDestroy(p->gexec);
+  void* bufs[] = {p->work, p->Hsrc, p->blk, p->primary, p->runs, p->hooks, p->scratch, p->part,
+                  p->k, p->acc, p->y, p->u0, p->W1, p->W2, p->bacc};
+  for (void* b : bufs)
+    if (b) cudaFree(b);
+  for (auto* pp : p->prol)
+    if (pp) cudaFree(pp);
+  delete p;
+}
+
+const char* tgh_last_error(const tgh_problem* p) { return p ? p->err.c_str() : "no problem"; }
+size_t tgh_state_length(const tgh_problem* p) { return (size_t)p->S * NV * p->nb; }
+size_t tgh_work_length(const tgh_problem* p) { return (size_t)p->Wv * NV * p->nb; }
+
+int tgh_copy_work(tgh_problem* p, double* dst) {
+  CK(cudaMemcpyAsync(dst, p->work, tgh_work_length(p) * sizeof(double), cudaMemcpyDeviceToDevice, p->stream));
+  CK(cudaStreamSynchronize(p->stream));
+  return TGH_OK;
+}
+
+int tgh_prepare(tgh_problem* p, const double* u, double t) { return launch_fill(p, u, false, p->work, t); }
+
+int tgh_rhs(tgh_problem* p, double* du, double t, const double* matter) {
+  RhsArgs a = base_args(p, p->work, t);
+  a.du = du;
+  a.matter = matter;
+  return launch_rhs(p, a, MODE_DU);
+}
+
+int tgh_gh_rhs(tgh_problem* p, double* du, const double* u, double t, const double* matter) {
+  int s = tgh_prepare(p, u, t);
+  return s ? s : tgh_rhs(p, du, t, matter);
+}
+
+int tgh_settle(tgh_problem* p, double* u, double t) {
+  int s = tgh_prepare(p, u, t);
+  if (s) return s;
+  gather_kernel<<<grid_for(p->npts, 256), 256, 0, p->stream>>>(p->work, u, p->geo, p->npts);
+  CK(cudaGetLastError());
+  return TGH_OK;
+}
+
+int tgh_stage_limit(tgh_problem* p, double* u, double t) { return stage_limit_impl(p, u, t); }
+int tgh_step_limit(tgh_problem* p, double* u, double t) { return stage_limit_impl(p, u, t); }
+
+int tgh_initial_state(tgh_problem* p, double* u, double t) {
+  exact_state_kernel<<<grid_for(p->npts, 128), 128, 0, p->stream>>>(u, p->blk, p->geo, p->npts, p->cs, t, 0);
+  CK(cudaGetLastError());
+  return stage_limit_impl(p, u, t);
+}
+
+int tgh_max_speed(tgh_problem* p, const double* u, double t, double* lambda) {
+  CK(cudaMemsetAsync(p->scratch, 0, 2 * sizeof(unsigned long long), p->stream));
+  speed_kernel<<<grid_for(p->npts, 128), 128, 0, p->stream>>>(u, p->blk, p->geo, p->npts, p->cs, t, p->scratch);
+  CK(cudaGetLastError());
+  unsigned long long h[2];
+  CK(cudaMemcpyAsync(h, p->scratch, sizeof(h), cudaMemcpyDeviceToHost, p->stream));
+  CK(cudaStreamSynchronize(p->stream));
+  if (h[1] > 0)
+    return fail(p, TGH_ERR_NONFINITE, "the state at t = " + std::to_string(t) + " is not finite where it is evolved: " +
+                                          std::to_string(h[1]) + " values at evolved points are NaN or Inf");
+  double lam;
+  std::memcpy(&lam, &h[0], sizeof(lam));
+  *lambda = lam;
+  if (!(std::isfinite(lam) && lam > 0))
+    return fail(p, TGH_ERR_SPEED, "the maximum characteristic speed over the evolved points came out as " +
+                                      std::to_string(lam) + ": there is no CFL-limited time step");
+  return TGH_OK;
+}
+
+int tgh_error_norm(tgh_problem* p, const double* u, double t, double* l2, double* linf) {
+  int s = tgh_prepare(p, u, t);
+  if (s) return s;
+  error_kernel<<<p->npart, 128, 0, p->stream>>>(p->work, p->blk, p->primary, p->geo, p->npts, p->cs, t, p->part);
+  CK(cudaGetLastError());
+  error_final_kernel<<<1, 32, 0, p->stream>>>(p->part, p->npart, p->part + 3 * (size_t)p->npart);
+  CK(cudaGetLastError());
+  double h[2];
+  CK(cudaMemcpyAsync(h, p->part + 3 * (size_t)p->npart, sizeof(h), cudaMemcpyDeviceToHost, p->stream));
+  CK(cudaStreamSynchronize(p->stream));
+  *l2 = h[0];
+  *linf = h[1];
+  return TGH_OK;
+}
+
+// plain form: per stage one fill, one right-hand-side launch, one stage update
+int tgh_rk4_step(tgh_problem* p, double* u, double t, double dt) {
+  const size_t L = tgh_state_length(p);
+  if (!p->k) {
+    CK(cudaMalloc(&p->k, L * sizeof(double)));
+    CK(cudaMalloc(&p->acc, L * sizeof(double)));
+    CK(cudaMalloc(&p->y, L * sizeof(double)));
+  }
+  const double b16 = dt / 6.0, b13 = dt / 3.0, a12 = 0.5 * dt;
+  const double tm = t + 0.5 * dt, te = t + dt;
+  const unsigned g = 148 * 8;
+  int s;
+  if ((s = tgh_gh_rhs(p, p->k, u, t, nullptr))) return s;
+  stage_update_kernel<<<g, 256, 0, p->stream>>>(0, (long)L, p->k, u, p->acc, p->y, nullptr, a12, b16);
+  CK(cudaGetLastError());
+  if ((s = stage_limit_impl(p, p->y, tm))) return s;
+  if ((s = tgh_gh_rhs(p, p->k, p->y, tm, nullptr))) return s;
+  stage_update_kernel<<<g, 256, 0, p->stream>>>(1, (long)L, p->k, u, p->acc, p->y, nullptr, a12, b13);
+  CK(cudaGetLastError());
+  if ((s = stage_limit_impl(p, p->y, tm))) return s;
+  if ((s = tgh_gh_rhs(p, p->k, p->y, tm, nullptr))) return s;
+  stage_update_kernel<<<g, 256, 0, p->stream>>>(1, (long)L, p->k, u, p->acc, p->y, nullptr, dt, b13);
+  CK(cudaGetLastError());
+  if ((s = stage_limit_impl(p, p->y, te))) return s;
+  if ((s = tgh_gh_rhs(p, p->k, p->y, te, nullptr))) return s;
+  stage_update_kernel<<<g, 256, 0, p->stream>>>(2, (long)L, p->k, nullptr, p->acc, nullptr, u, 0.0, b16);
+  CK(cudaGetLastError());
+  return stage_limit_impl(p, u, te);
+}
+
+// batched form, one step's launches on the stream (captured into a graph by the caller)
+static int batched_step(tgh_problem* p, double t, double dt) {
+  const double b16 = dt / 6.0, b13 = dt / 3.0, a12 = 0.5 * dt;
+  const double ts[4] = {t, t + 0.5 * dt, t + 0.5 * dt, t + dt};
+  const double ca[4] = {a12, a12, dt, 0.0}, cb[4] = {b16, b13, b13, b16};
+  double* rd[4] = {p->work, p->W1, p->W2, p->W1};
+  double* wr[4] = {p->W1, p->W2, p->W1, p->work};
+  int s;
+  for (int st = 0; st < 4; ++st) {
+    if ((s = launch_fill(p, rd[st], true, rd[st], ts[st]))) return s;
+    RhsArgs a = base_args(p, rd[st], ts[st]);
+    a.u0 = p->work;
+    a.acc = p->bacc;
+    a.next = wr[st];
+    a.ca = ca[st];
+    a.cb = cb[st];
+    a.stage = st + 1;
+    if ((s = launch_rhs(p, a, MODE_STAGE))) return s;
+  }
+  return TGH_OK;
+}
+
+int tgh_step_batched(tgh_problem* p, double* u, double t, double dt, int nsteps) {
+  if (nsteps < 1) return fail(p, TGH_ERR_ARG, "nsteps must be positive");
+  if (p->cfg.interior == TGH_INT_PASTED)
+    return fail(p, TGH_ERR_ARG, "the batched form has no :pasted limiter; use tgh_rk4_step");
+  const size_t Lw = tgh_work_length(p), L = tgh_state_length(p);
+  if (!p->W1) {
+    CK(cudaMalloc(&p->W1, Lw * sizeof(double)));
+    CK(cudaMalloc(&p->W2, Lw * sizeof(double)));
+    CK(cudaMalloc(&p->bacc, L * sizeof(double)));
+    CK(cudaMemsetAsync(p->W1, 0, Lw * sizeof(double), p->stream));
+    CK(cudaMemsetAsync(p->W2, 0, Lw * sizeof(double), p->stream));
+  }
+  // the state into W0's owned points (and ghosts), outside the graph
+  int s = launch_fill(p, u, false, p->work, t);
+  if (s) return s;
+  const bool reuse = p->gexec && p->gkey.t == t && p->gkey.dt == dt && p->gkey.nsteps == nsteps;
+  if (!reuse) {
+    if (p->gexec) {
+      cudaGraphExecDestroy(p->gexec);
+      p->gexec = nullptr;
+    }
+    cudaGraph_t graph;
+    CK(cudaStreamBeginCapture(p->stream, cudaStreamCaptureModeThreadLocal));
+    int st = TGH_OK;
+    for (int n = 0; n < nsteps && st == TGH_OK; ++n) st = batched_step(p, t + n * dt, dt);
+    cudaError_t ee = cudaStreamEndCapture(p->stream, &graph);
+    if (st) return st;
+    CK(ee);
+    CK(cudaGraphInstantiate(&p->gexec, graph, 0));
+    cudaGraphDestroy(graph);
+    p->gkey = GraphKey{t, dt, nsteps};
+  }
+  CK(cudaGraphLaunch(p->gexec, p->stream));
+  gather_kernel<<<grid_for(p->npts, 256), 256, 0, p->stream>>>(p->work, u, p->geo, p->npts);
+  CK(cudaGetLastError());
+  return TGH_OK;
+}
+
+// Benchmark aid: the average duration of the right-hand-side kernel alone, timed with CUDA
+// events on the problem's stream over nlaunch launches. mode 0: the plain form's kernel
+// (du); mode 1: the batched form's kernel with the stage-2 epilogue. u is filled first.
+int tgh_time_rhs(tgh_problem* p, const double* u, double t, int mode, int nlaunch, double* ms_per_launch) {
+  const size_t L = tgh_state_length(p), Lw = tgh_work_length(p);
+  if (!p->k) {
+    CK(cudaMalloc(&p->k, L * sizeof(double)));
+    CK(cudaMalloc(&p->acc, L * sizeof(double)));
+    CK(cudaMalloc(&p->y, L * sizeof(double)));
+  }
+  if (mode == 1 && !p->W1) {
+    CK(cudaMalloc(&p->W1, Lw * sizeof(double)));
+    CK(cudaMalloc(&p->W2, Lw * sizeof(double)));
+    CK(cudaMalloc(&p->bacc, L * sizeof(double)));
+    CK(cudaMemsetAsync(p->bacc, 0, L * sizeof(double), p->stream));
+  }
+  int s = tgh_prepare(p, u, t);
+  if (s) return s;
+  RhsArgs a = base_args(p, p->work, t);
+  a.du = p->k;
+  a.u0 = p->work;
+  a.acc = p->bacc;
+  a.next = p->W1;
+  a.ca = 1e-3;
+  a.cb = 1e-3;
+  a.stage = 2;
+  if ((s = launch_rhs(p, a, mode == 1 ? MODE_STAGE : MODE_DU))) return s;  // warm
+  cudaEvent_t e0, e1;
+  CK(cudaEventCreate(&e0));
+  CK(cudaEventCreate(&e1));
+  CK(cudaEventRecord(e0, p->stream));
+  for (int i = 0; i < nlaunch; ++i)
+    if ((s = launch_rhs(p, a, mode == 1 ? MODE_STAGE : MODE_DU))) return s;
+  CK(cudaEventRecord(e1, p->stream));
+  CK(cudaEventSynchronize(e1));
+  float ms = 0;
+  CK(cudaEventElapsedTime(&ms, e0, e1));
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  *ms_per_launch = ms / nlaunch;
+  return TGH_OK;
+}
+
+// sustained FP64 FMA rate of this GPU (2 flop per FMA), for the roofline denominator
+double tgh_fp64_probe(void* stream, int iters) {
+  double* d;
+  if (cudaMalloc(&d, sizeof(double)) != cudaSuccess) return -1;
+  int dev, nsm;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+  cudaStream_t s = (cudaStream_t)stream;
+  const int threads = 256, blocks = nsm * 8;
+  fp64_probe_kernel<<<blocks, threads, 0, s>>>(d, 10, 1.0000001, 1e-9);
+  cudaEvent_t e0, e1;
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  cudaEventRecord(e0, s);
+  fp64_probe_kernel<<<blocks, threads, 0, s>>>(d, iters, 1.0000001, 1e-9);
+  cudaEventRecord(e1, s);
+  cudaEventSynchronize(e1);
+  float ms = 0;
+  cudaEventElapsedTime(&ms, e0, e1);
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  cudaFree(d);
+  const double flops = 2.0 * 8 * 16 * (double)iters * threads * blocks;
+  return flops / (ms * 1e-3) / 1e12;
+}
+
+}  // extern "C"

@@ -1,0 +1,345 @@
+// The fused right-hand side of the generalized-harmonic system at one owned point per
+// thread, in the reference's streaming order (src/evolution.jl:258-388):
+//   1. h, Pi at the point; the 30 first derivatives d_i h; the coefficient set;
+//   2. d_t h = beta^i d_i h + (alpha/sqrt(gamma)) Pi + (eps/h) sum_d KO_d(h), stored at once;
+//   3. the gauge source, the reduced source with damping (+ matter);
+//   4. per component v (run-time loop): beta^i d_i Pi + (d_i beta^i) Pi + d_i A^{ij} d_j h
+//      + A^{ij} d_i d_j h + (eps/h) sum_d KO_d(Pi) + msrc_v, stored as it is finished.
+// The interior branches of gh_rhs_point! (src/evolution.jl:489-695) wrap it: the frozen
+// core is asked before any stencil is read.
+//
+// Two epilogues share the body:
+//   MODE_DU     write du in state layout (the plain form, rhs!)
+//   MODE_STAGE  the RK4 stage update in place of du: acc and the next stage's ghosted
+//               working array are written, u_n read (the batched form)
+#pragma once
+#include "algebra.cuh"
+
+namespace tgh {
+
+enum { MODE_DU = 0, MODE_STAGE = 1 };
+
+// finite-difference weights on unit spacing (exact rationals, correctly rounded once)
+template <int Q> struct W;
+template <> struct W<2> {
+  static constexpr int R = 1, RD = 2;
+  __device__ static constexpr double d1(int k) { return k == 1 ? 1.0 / 2.0 : 0.0; }  // antisymmetric, k > 0
+  __device__ static constexpr double d2(int k) { return k == 0 ? -2.0 : 1.0; }
+  __device__ static constexpr double ko(int k) { return k == 0 ? -6.0 / 16.0 : k == 1 ? 4.0 / 16.0 : -1.0 / 16.0; }
+};
+template <> struct W<4> {
+  static constexpr int R = 2, RD = 3;
+  __device__ static constexpr double d1(int k) { return k == 1 ? 2.0 / 3.0 : -1.0 / 12.0; }
+  __device__ static constexpr double d2(int k) { return k == 0 ? -5.0 / 2.0 : k == 1 ? 4.0 / 3.0 : -1.0 / 12.0; }
+  __device__ static constexpr double ko(int k) {
+    return k == 0 ? -20.0 / 64.0 : k == 1 ? 15.0 / 64.0 : k == 2 ? -6.0 / 64.0 : 1.0 / 64.0;
+  }
+};
+template <> struct W<6> {
+  static constexpr int R = 3, RD = 4;
+  __device__ static constexpr double d1(int k) { return k == 1 ? 3.0 / 4.0 : k == 2 ? -3.0 / 20.0 : 1.0 / 60.0; }
+  __device__ static constexpr double d2(int k) {
+    return k == 0 ? -49.0 / 18.0 : k == 1 ? 3.0 / 2.0 : k == 2 ? -3.0 / 20.0 : 1.0 / 90.0;
+  }
+  __device__ static constexpr double ko(int k) {
+    return k == 0 ? -70.0 / 256.0 : k == 1 ? 56.0 / 256.0 : k == 2 ? -28.0 / 256.0 : k == 3 ? 8.0 / 256.0 : -1.0 / 256.0;
+  }
+};
+template <> struct W<8> {
+  static constexpr int R = 4, RD = 5;
+  __device__ static constexpr double d1(int k) {
+    return k == 1 ? 4.0 / 5.0 : k == 2 ? -1.0 / 5.0 : k == 3 ? 4.0 / 105.0 : -1.0 / 280.0;
+  }
+  __device__ static constexpr double d2(int k) {
+    return k == 0 ? -205.0 / 72.0 : k == 1 ? 8.0 / 5.0 : k == 2 ? -1.0 / 5.0 : k == 3 ? 8.0 / 315.0 : -1.0 / 560.0;
+  }
+  __device__ static constexpr double ko(int k) {
+    return k == 0 ? -252.0 / 1024.0
+                  : k == 1 ? 210.0 / 1024.0
+                           : k == 2 ? -120.0 / 1024.0 : k == 3 ? 45.0 / 1024.0 : k == 4 ? -10.0 / 1024.0 : 1.0 / 1024.0;
+  }
+};
+
+template <class T> __device__ __forceinline__ T ld(const double* p) { return T(__ldg(p)); }
+
+// sum_k w_k u[k s] on the antisymmetric first-derivative stencil (center weight zero)
+template <int Q, class T> __device__ __forceinline__ T st_d1(const double* p, long s) {
+  T acc = T(0.0);
+#pragma unroll
+  for (int k = 1; k <= W<Q>::R; ++k) acc = fma(T(W<Q>::d1(k)), ld<T>(p + k * s) - ld<T>(p - k * s), acc);
+  return acc;
+}
+template <int Q, class T> __device__ __forceinline__ T st_d2(const double* p, long s, T c) {
+  T acc = T(W<Q>::d2(0)) * c;
+#pragma unroll
+  for (int k = 1; k <= W<Q>::R; ++k) acc = fma(T(W<Q>::d2(k)), ld<T>(p + k * s) + ld<T>(p - k * s), acc);
+  return acc;
+}
+template <int Q, class T> __device__ __forceinline__ T st_ko(const double* p, long s, T c) {
+  T acc = T(W<Q>::ko(0)) * c;
+#pragma unroll
+  for (int k = 1; k <= W<Q>::RD; ++k) acc = fma(T(W<Q>::ko(k)), ld<T>(p + k * s) + ld<T>(p - k * s), acc);
+  return acc;
+}
+// d_1 d_2 as the tensor product of two first-derivative stencils
+template <int Q, class T> __device__ __forceinline__ T st_mixed(const double* p, long s1, long s2) {
+  T acc = T(0.0);
+#pragma unroll
+  for (int a = 1; a <= W<Q>::R; ++a) {
+    T in = T(0.0);
+#pragma unroll
+    for (int e = 1; e <= W<Q>::R; ++e) {
+      const double* pp = p + a * s1;
+      const double* pm = p - a * s1;
+      T d = (ld<T>(pp + e * s2) - ld<T>(pp - e * s2)) - (ld<T>(pm + e * s2) - ld<T>(pm - e * s2));
+      in = fma(T(W<Q>::d1(e)), d, in);
+    }
+    acc = fma(T(W<Q>::d1(a)), in, acc);
+  }
+  return acc;
+}
+
+// one launch's geometry and buffers
+struct RhsArgs {
+  const double* work;     // ghosted working array, (W^3 x 20) per block
+  const double* Hsrc;     // sampled gauge source, (N1^3 x 20) per block, or null
+  const double* matter;   // (N1^3 x 10) per block, or null
+  const double* blk;      // per block: domain lo (3), h, integer corner (3), pad
+  double* du;             // MODE_DU: state layout
+  // MODE_STAGE
+  const double* u0;       // state at the start of the step (ghosted layout), null at stage 1
+  double* acc;            // accumulator (state layout)
+  double* next;           // the next stage's ghosted working array (owned points written)
+  double ca, cb;          // next = u0 + ca k ; acc = (stage 1 ? u0 : acc) + cb k ; final: next = acc + cb k
+  int stage;              // 1..4
+  int N1, Wd, G;
+  long npts;              // N1^3 * nblocks
+  double t;
+};
+
+template <int Q, bool DISS, class T, class Emit>
+__device__ __forceinline__ void rhs_core(const Case& cs, const RhsArgs& A, const double* wk, long sv, int b,
+                                         long ip, const double* x, double inv_h, Emit& out) {
+  const long s1 = 1, s2 = A.Wd, s3 = (long)A.Wd * A.Wd;
+  const T ih = T(inv_h), ih2 = T(inv_h * inv_h);
+  const T eh = T(DISS ? dissipation_rate(cs, A.t, x) * inv_h : 0.0);
+  const T g0 = T(damping_rate(cs, A.t, x));
+
+  // (1) state, first derivatives of h, coefficients
+  T hv[NC], dh0[NC], dh1[NC], dh2[NC];
+#pragma unroll
+  for (int v = 0; v < NC; ++v) {
+    const double* p = wk + v * sv;
+    hv[v] = ld<T>(p);
+    dh0[v] = ih * st_d1<Q, T>(p, s1);
+    dh1[v] = ih * st_d1<Q, T>(p, s2);
+    dh2[v] = ih * st_d1<Q, T>(p, s3);
+  }
+  Coef<T> C;
+  metric_quantities(hv, C);
+  const T a_div = C.alpha / C.sqrtg;
+  // (2) d_t h, stored at once
+  T dth[NC];
+#pragma unroll
+  for (int v = 0; v < NC; ++v) {
+    const double* p = wk + v * sv;
+    T s = C.beta[0] * dh0[v] + C.beta[1] * dh1[v] + C.beta[2] * dh2[v] + a_div * ld<T>(p + NC * sv);
+    if (DISS) s = fma(eh, st_ko<Q, T>(p, s1, hv[v]) + st_ko<Q, T>(p, s2, hv[v]) + st_ko<Q, T>(p, s3, hv[v]), s);
+    dth[v] = s;
+    out.put(v, (double)s);
+  }
+  // (3) the source
+  const T* dh[3] = {dh0, dh1, dh2};
+  const T* D[4] = {dth, dh0, dh1, dh2};
+  T msrc[NC];
+  if (cs.gauge == TGH_GAUGE_NONE) {
+    T Hl[4], dHl[4][4];
+    gh_source<T, false>(C, D, Hl, dHl, g0, T(cs.g2), msrc);
+  } else {
+    T Hl[4], dHl[4][4];
+    if (cs.gauge == TGH_GAUGE_SAMPLED) {
+      const long S = (long)A.N1 * A.N1 * A.N1;
+      const double* q = A.Hsrc + (long)b * NV * S + ip;
+#pragma unroll
+      for (int a = 0; a < 4; ++a) Hl[a] = ld<T>(q + a * S);
+#pragma unroll
+      for (int k = 0; k < 16; ++k) dHl[k % 4][k / 4] = ld<T>(q + (4 + k) * S);
+    } else {
+      ks_gauge_source<T>(cs, hv, D, Hl, dHl);
+    }
+    gh_source<T, true>(C, D, Hl, dHl, g0, T(cs.g2), msrc);
+  }
+  if (A.matter) {
+    const long S = (long)A.N1 * A.N1 * A.N1;
+    const double* q = A.matter + (long)b * 10 * S + ip;
+    T m[10], ms[NC];
+#pragma unroll
+    for (int k = 0; k < 10; ++k) m[k] = ld<T>(q + k * S);
+    matter_source(C, m, ms);
+#pragma unroll
+    for (int v = 0; v < NC; ++v) msrc[v] += ms[v];
+  }
+  // (4) the coefficients of the Pi components
+  T divb, divA[3];
+  metric_divergences(C, dh, divb, divA);
+  const T am = C.alpha * C.sqrtg;
+  T Axx = am * C.gamu[0], Axy = T(2.0) * am * C.gamu[1], Axz = T(2.0) * am * C.gamu[2];
+  T Ayy = am * C.gamu[3], Ayz = T(2.0) * am * C.gamu[4], Azz = am * C.gamu[5];
+  const T b0 = C.beta[0], b1 = C.beta[1], b2 = C.beta[2];
+#pragma unroll 1
+  for (int v = 0; v < NC; ++v) {
+    const double* ph = wk + v * sv;
+    const double* pp = ph + NC * sv;
+    const T hc = ld<T>(ph), pc = ld<T>(pp);
+    T s = b0 * (ih * st_d1<Q, T>(pp, s1));
+    s = fma(b1, ih * st_d1<Q, T>(pp, s2), s);
+    s = fma(b2, ih * st_d1<Q, T>(pp, s3), s);
+    s = fma(divb, pc, s);
+    s = fma(divA[0], ih * st_d1<Q, T>(ph, s1), s);
+    s = fma(divA[1], ih * st_d1<Q, T>(ph, s2), s);
+    s = fma(divA[2], ih * st_d1<Q, T>(ph, s3), s);
+    T p2 = Axx * st_d2<Q, T>(ph, s1, hc);
+    p2 = fma(Ayy, st_d2<Q, T>(ph, s2, hc), p2);
+    p2 = fma(Azz, st_d2<Q, T>(ph, s3, hc), p2);
+    p2 = fma(Axy, st_mixed<Q, T>(ph, s1, s2), p2);
+    p2 = fma(Axz, st_mixed<Q, T>(ph, s1, s3), p2);
+    p2 = fma(Ayz, st_mixed<Q, T>(ph, s2, s3), p2);
+    s = fma(ih2, p2, s);
+    if (DISS) s = fma(eh, st_ko<Q, T>(pp, s1, pc) + st_ko<Q, T>(pp, s2, pc) + st_ko<Q, T>(pp, s3, pc), s);
+    out.put(NC + v, (double)(s + msrc[v]));
+  }
+}
+
+// Where a finished component goes: straight to du (plain form), into the RK4 stage update
+// (batched form), or into a local vector the interior branches combine.
+struct EmitDu {
+  double* d;
+  long S;
+  __device__ __forceinline__ void put(int v, double val) { d[v * S] = val; }
+};
+struct EmitStage {
+  double* ac;
+  double* nx;
+  const double* u0;
+  long S, sv;
+  double ca, cb;
+  int stage;
+  __device__ __forceinline__ void put(int v, double kv) {
+    if (stage == 4) {
+      nx[v * sv] = fma(cb, kv, ac[v * S]);
+    } else {
+      const double un = u0[v * sv];
+      ac[v * S] = fma(cb, kv, stage == 1 ? un : ac[v * S]);
+      nx[v * sv] = fma(ca, kv, un);
+    }
+  }
+};
+struct EmitLocal {
+  double* o;
+  __device__ __forceinline__ void put(int v, double val) { o[v] = val; }
+};
+
+// the interior branches of gh_rhs_point! around F (src/evolution.jl:489-695)
+template <int Q, bool DISS, class Emit>
+__device__ __forceinline__ void rhs_interior(const Case& cs, const RhsArgs& A, const double* wk, long sv, int b,
+                                             long ip, const double* x, double inv_h, Emit& em) {
+  const double r = interior_radius(cs, A.t, x);
+  const bool frozen = cs.interior == TGH_INT_PASTED ? r < cs.r1 : r < cs.r0;
+  if (frozen) {
+    if (core_follows(cs)) {
+      const double rho = core_rate(cs), dl = layer_rate_step(cs);
+      double xc[3], hd[NC], Pd[NC];
+      core_position(cs, A.t, x, xc);
+      background_state(cs, A.t, xc, hd, Pd);
+      double dthd[NC], dtPd[NC];
+      const double sw = smoothstep(4.0 * r / cs.r0 - 1.0);
+      if (sw == 0.0) {
+        for (int n = 0; n < NC; ++n) dthd[n] = dtPd[n] = 0.0;
+      } else {
+        const double tp = A.t + dl, tm = A.t - dl;
+        double xp[3], xm[3], hp[NC], Pp[NC], hm[NC], Pm[NC];
+        core_position(cs, tp, x, xp);
+        core_position(cs, tm, x, xm);
+        background_state(cs, tp, xp, hp, Pp);
+        background_state(cs, tm, xm, hm, Pm);
+        const double f = sw / (tp - tm);
+        for (int n = 0; n < NC; ++n) {
+          dthd[n] = f * (hp[n] - hm[n]);
+          dtPd[n] = f * (Pp[n] - Pm[n]);
+        }
+      }
+      double hu[NC], rr[NC];
+      for (int v = 0; v < NC; ++v) hu[v] = wk[v * sv];
+      core_relaxation_rate(hu, hd, rho, dthd, rr);
+      for (int v = 0; v < NC; ++v) {
+        em.put(v, rr[v]);
+        em.put(NC + v, dtPd[v] - rho * (wk[(NC + v) * sv] - Pd[v]));
+      }
+    } else {
+      for (int v = 0; v < NV; ++v) em.put(v, 0.0);
+    }
+    return;
+  }
+  double F[NV];
+  EmitLocal el{F};
+  rhs_core<Q, DISS, double>(cs, A, wk, sv, b, ip, x, inv_h, el);
+  if (r >= cs.r1) {
+    for (int v = 0; v < NV; ++v) em.put(v, F[v]);
+    return;
+  }
+  double w, rho;
+  layer_profiles(cs, r, w, rho);
+  if (core_follows(cs)) {
+    const double dl = layer_rate_step(cs);
+    double hm[NC], Pm[NC], dthm[NC], Pp[NC], Pq[NC], hx[NC];
+    background_state(cs, A.t, x, hm, Pm, dthm);
+    const double tp = A.t + dl, tm = A.t - dl;
+    background_state(cs, tp, x, hx, Pp);
+    background_state(cs, tm, x, hx, Pq);
+    const double om = 1.0 - w;
+    for (int v = 0; v < NC; ++v) {
+      const double dtP = (Pp[v] - Pq[v]) / (tp - tm);
+      em.put(v, w * F[v] + om * dthm[v] - rho * (wk[v * sv] - hm[v]));
+      em.put(NC + v, w * F[NC + v] + om * dtP - rho * (wk[(NC + v) * sv] - Pm[v]));
+    }
+  } else {
+    double he[NC], Pe[NC];
+    background_state(cs, A.t, x, he, Pe);
+    for (int v = 0; v < NC; ++v) {
+      em.put(v, w * F[v] - rho * (wk[v * sv] - he[v]));
+      em.put(NC + v, w * F[NC + v] - rho * (wk[(NC + v) * sv] - Pe[v]));
+    }
+  }
+}
+
+template <int Q, bool DISS, int MODE, bool INT>
+__global__ void __launch_bounds__(128) rhs_kernel(const Case cs, const RhsArgs A) {
+  const long p = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= A.npts) return;
+  const int N1 = A.N1;
+  const long S = (long)N1 * N1 * N1;
+  const int b = (int)(p / S);
+  const long ip = p - (long)b * S;
+  const int k = (int)(ip / ((long)N1 * N1));
+  const int j = (int)((ip / N1) % N1);
+  const int i = (int)(ip % N1);
+  const double* bl = A.blk + 8 * b;
+  const double h = bl[3];
+  const double x[3] = {__dadd_rn(bl[0], __dmul_rn(bl[4] + (double)i, h)), __dadd_rn(bl[1], __dmul_rn(bl[5] + (double)j, h)),
+                       __dadd_rn(bl[2], __dmul_rn(bl[6] + (double)k, h))};
+  const long sv = (long)A.Wd * A.Wd * A.Wd;
+  const long wo = (long)b * NV * sv + (i + A.G) + (long)A.Wd * ((j + A.G) + (long)A.Wd * (k + A.G));
+  const double* wk = A.work + wo;
+  const double inv_h = 1.0 / h;
+  if (MODE == MODE_DU) {
+    EmitDu em{A.du + (long)b * NV * S + ip, S};
+    if (INT) rhs_interior<Q, DISS>(cs, A, wk, sv, b, ip, x, inv_h, em);
+    else rhs_core<Q, DISS, double>(cs, A, wk, sv, b, ip, x, inv_h, em);
+  } else {
+    EmitStage em{A.acc + (long)b * NV * S + ip, A.next + wo, A.u0 + wo, S, sv, A.ca, A.cb, A.stage};
+    if (INT) rhs_interior<Q, DISS>(cs, A, wk, sv, b, ip, x, inv_h, em);
+    else rhs_core<Q, DISS, double>(cs, A, wk, sv, b, ip, x, inv_h, em);
+  }
+}
+
+}  // namespace tgh

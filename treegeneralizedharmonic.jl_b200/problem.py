@@ -1,0 +1,156 @@
+"""GHProblem and the verbs of the reference's stepping path, on one GPU.
+
+Host-side mirror of src/evolution.jl:995-1560 and src/stepping.jl:91-239. Every verb is one
+call into libtgh_b200.so (include/tgh.h); the state vectors are torch float64 CUDA tensors
+owned by the caller. There is no CPU path: a missing library or a missing GPU raises.
+"""
+import ctypes
+
+import torch
+
+from . import _abi
+
+
+def _ptr(t):
+    if t is None:
+        return None
+    if not (t.is_cuda and t.dtype == torch.float64 and t.is_contiguous()):
+        raise TypeError("state vectors are contiguous float64 CUDA tensors")
+    return ctypes.c_void_p(t.data_ptr())
+
+
+class GHProblem:
+    """Everything one right-hand-side evaluation needs (GHProblem, src/evolution.jl:995-1149):
+    the forest's fill plan, the ghosted working array, the sampled gauge source and the case's
+    constants, on the current CUDA device and stream."""
+
+    def __init__(self, case, forest, q, margin_check=True, precision="fp64", stream=None):
+        if not torch.cuda.is_available():
+            raise RuntimeError("GHProblem runs on a CUDA device; none is available")
+        self.lib = _abi.load_library()
+        self.case, self.forest, self.q = case, forest, int(q)
+        self.stream = stream if stream is not None else torch.cuda.current_stream()
+        self._cfg = case.config(q, precision)
+        self._mesh = forest.mesh()
+        h = ctypes.c_void_p()
+        st = self.lib.tgh_problem_create(ctypes.byref(self._cfg), ctypes.byref(self._mesh),
+                                         ctypes.c_void_p(self.stream.cuda_stream), 1 if margin_check else 0,
+                                         ctypes.byref(h))
+        self._h = h
+        if st != _abi.TGH_OK:
+            msg = self.lib.tgh_last_error(h).decode() if h.value else "allocation failed"
+            self.close()
+            raise _abi.TGHError(st, msg)
+        self.state_length = int(self.lib.tgh_state_length(h))
+        self.work_length = int(self.lib.tgh_work_length(h))
+
+    # ---- lifetime ----
+    def close(self):
+        if getattr(self, "_h", None) is not None and self._h.value:
+            self.lib.tgh_problem_destroy(self._h)
+        self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _check(self, st):
+        if st != _abi.TGH_OK:
+            raise _abi.TGHError(st, self.lib.tgh_last_error(self._h).decode())
+
+    # ---- state vectors ----
+    def statevector(self):
+        return torch.zeros(self.state_length, dtype=torch.float64, device="cuda")
+
+    def evolved_sets(self):
+        """The field sets this package evolves, in segment order (src/stepping.jl:125)."""
+        return (self,)
+
+    # ---- the verbs ----
+    def prepare(self, u, t):
+        """prepare!(p, u, t): scatter u and fill the ghosts with the hook at t."""
+        self._check(self.lib.tgh_prepare(self._h, _ptr(u), float(t)))
+        return self
+
+    def rhs(self, du, t, matter=None):
+        """rhs!(du, p, t; matter): the right-hand side of the state prepare left."""
+        self._check(self.lib.tgh_rhs(self._h, _ptr(du), float(t), _ptr(matter)))
+
+    def gh_rhs(self, du, u, t, matter=None):
+        """gh_rhs!(du, u, p, t; matter) = prepare! then rhs!."""
+        self._check(self.lib.tgh_gh_rhs(self._h, _ptr(du), _ptr(u), float(t), _ptr(matter)))
+
+    def settle(self, u, t):
+        """settle!(p, u, t): u as the mesh sees it (fill, then gather)."""
+        self._check(self.lib.tgh_settle(self._h, _ptr(u), float(t)))
+        return u
+
+    def stage_limit(self, u, t):
+        self._check(self.lib.tgh_stage_limit(self._h, _ptr(u), float(t)))
+
+    def step_limit(self, u, t):
+        self._check(self.lib.tgh_step_limit(self._h, _ptr(u), float(t)))
+
+    def max_speed(self, u, t):
+        """max_speed(p, u, t): the checked maximum characteristic speed over evolved points."""
+        lam = ctypes.c_double()
+        self._check(self.lib.tgh_max_speed(self._h, _ptr(u), float(t), ctypes.byref(lam)))
+        return lam.value
+
+    def initial_state(self, u, t):
+        """initial_state!(u, p, t): the case's exact state, limited."""
+        self._check(self.lib.tgh_initial_state(self._h, _ptr(u), float(t)))
+        return u
+
+    def gh_dt(self, u, cfl=0.25, t=0.0):
+        """cfl * h_min / lambda_max (src/evolution.jl:1509-1519)."""
+        hmin = self.forest.h0 / 2 ** (self.forest.nlevels - 1)
+        return cfl * hmin / self.max_speed(u, t)
+
+    def error_norm(self, u, t):
+        """Masked volume-weighted (L2, Linf) of |u - u_exact| over evolved primaries."""
+        l2, li = ctypes.c_double(), ctypes.c_double()
+        self._check(self.lib.tgh_error_norm(self._h, _ptr(u), float(t), ctypes.byref(l2), ctypes.byref(li)))
+        return l2.value, li.value
+
+    def copy_work(self):
+        w = torch.empty(self.work_length, dtype=torch.float64, device="cuda")
+        self._check(self.lib.tgh_copy_work(self._h, _ptr(w)))
+        return w
+
+    # ---- time integration ----
+    def rk4_step(self, u, t, dt):
+        """One classical RK4 step, plain form (per stage: fill, RHS, stage update)."""
+        self._check(self.lib.tgh_rk4_step(self._h, _ptr(u), float(t), float(dt)))
+
+    def step_batched(self, u, t, dt, nsteps):
+        """nsteps RK4 steps, batched form: fused stage epilogue, one CUDA graph."""
+        self._check(self.lib.tgh_step_batched(self._h, _ptr(u), float(t), float(dt), int(nsteps)))
+
+    def time_rhs(self, u, t, mode=1, nlaunch=10):
+        """Average duration (ms) of the right-hand-side kernel alone, CUDA events on this
+        problem's stream; mode 1 is the batched form's kernel, 0 the plain form's."""
+        ms = ctypes.c_double()
+        self._check(self.lib.tgh_time_rhs(self._h, _ptr(u), float(t), int(mode), int(nlaunch), ctypes.byref(ms)))
+        return ms.value
+
+    def gh_solve(self, u, tspan, dt, batched=False):
+        """Integrate u from tspan[0] to tspan[1] with RK4 steps of at most dt, the last one
+        shortened to land on tspan[1] (gh_solve, src/stepping.jl:235-239)."""
+        t0, t1 = float(tspan[0]), float(tspan[1])
+        n = max(1, int(-(-(t1 - t0) // dt)))
+        dtu = (t1 - t0) / n
+        if batched:
+            self.step_batched(u, t0, dtu, n)
+        else:
+            for i in range(n):
+                self.rk4_step(u, t0 + i * dtu, dtu)
+        return u
+
+
+def fp64_peak_tflops(iters=4000):
+    """Sustained FP64 FMA throughput of the current GPU in TFLOP/s (2 flop per FMA)."""
+    lib = _abi.load_library()
+    return lib.tgh_fp64_probe(ctypes.c_void_p(torch.cuda.current_stream().cuda_stream), int(iters))
