@@ -104,7 +104,7 @@ class Clocks:
         sm = [float(r[1]) for r in rows if len(r) >= 9]
         mx = [float(r[2]) for r in rows if len(r) >= 9]
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        reasons = sorted({names[i - 5] for r in rows if len(r) >= 9 for i in range(5, 9) if "Active" in r[i]})
+        reasons = sorted({names[i - 5] for r in rows if len(r) >= 9 for i in range(5, 9) if r[i].strip() == "Active"})
         return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
                 "reasons": reasons, "samples": len(sm)}
 

@@ -14,7 +14,7 @@ namespace tgh {
 // msrc = -alpha sqrt(gamma) (S0 + Z) from the coefficients, D[c] = d_c g packed (c = t,x,y,z),
 // the lowered gauge source Hl and dHl[a][b] = d_a H_b.
 template <class T, bool HAS_H>
-__device__ __forceinline__ void gh_source(const Coef<T>& C, const T* const D[4], const T Hl[4],
+TGH_HD void gh_source(const Coef<T>& C, const T* const D[4], const T Hl[4],
                                           const T dHl[4][4], T g0, T g2, T* msrc) {
   const T* Gp = C.gu;
   T S[NC];
@@ -145,7 +145,7 @@ __device__ __forceinline__ void gh_source(const Coef<T>& C, const T* const D[4],
 
 // row a of d g^{ab} = -g^{ac} (d g_cd) g^{db}
 template <class T, int A>
-__device__ __forceinline__ void dgu_row(const T* Gp, const T* dg, T out[4]) {
+TGH_HD void dgu_row(const T* Gp, const T* dg, T out[4]) {
   T v[4];
 #pragma unroll
   for (int d = 0; d < 4; ++d) {
@@ -165,7 +165,7 @@ __device__ __forceinline__ void dgu_row(const T* Gp, const T* dg, T out[4]) {
 
 // d_i beta^i and d_i (alpha sqrt(gamma) gamma^{ij})
 template <class T>
-__device__ __forceinline__ void metric_divergences(const Coef<T>& C, const T* const dh[3], T& divb, T divA[3]) {
+TGH_HD void metric_divergences(const Coef<T>& C, const T* const dh[3], T& divb, T divA[3]) {
   const T* Gp = C.gu;
   const T igutt = T(1.0) / Gp[0];
   T r1[3][4], ri[3][4];
@@ -206,7 +206,7 @@ __device__ __forceinline__ void metric_divergences(const Coef<T>& C, const T* co
 
 // the stress-energy term alpha sqrt(gamma) (16 pi T_ab - 8 pi g_ab T); m = (rho, S_i, S_ij packed)
 template <class T>
-__device__ __forceinline__ void matter_source(const Coef<T>& C, const T* m, T* out) {
+TGH_HD void matter_source(const Coef<T>& C, const T* m, T* out) {
   const T c8 = T(8.0 * M_PI), c16 = T(16.0 * M_PI);
   const T* b = C.beta;
   const T rho = m[0];

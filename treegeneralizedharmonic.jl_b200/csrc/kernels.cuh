@@ -298,6 +298,12 @@ __global__ void gather_kernel(const double* __restrict__ work, double* __restric
   for (int v = 0; v < NV; ++v) o[v * g.S] = q[v * g.Wv];
 }
 
+// one point's analytic state (20) and gauge tuple (20), for diagnostics
+__global__ void point_physics_kernel(const Case cs, double t, const double* x, double* out) {
+  exact_state(cs, t, x, out);
+  gauge_tuple(cs, t, x, out + NV);
+}
+
 // sustained FP64 fused multiply-add throughput probe: 8 independent chains per thread
 __global__ void fp64_probe_kernel(double* out, int iters, double a, double b) {
   double x0 = threadIdx.x * 1e-9, x1 = x0 + 1e-9, x2 = x0 + 2e-9, x3 = x0 + 3e-9;

@@ -356,34 +356,34 @@ TGH_HD void gauge_tuple(const Case& c, double t, const double* x, double* out) {
   }
   D2 g2[4][4];
   metric(c, p, g2);
-  D1 g[4][4], dg[4][4][4];  // dg[c][a][b] = d_c g_ab
-  for (int a = 0; a < 4; ++a)
-    for (int b = 0; b < 4; ++b) {
-      g[a][b] = g2[a][b].v;
-      for (int k = 0; k < 4; ++k) dg[k][a][b] = g2[a][b].d[k];
-    }
-  // inverse by cofactors in D1 arithmetic
-  D1 cof[4][4];
-  for (int i = 0; i < 4; ++i)
-    for (int j = 0; j < 4; ++j) {
-      int r[3], cc[3], kr = 0, kc = 0;
-      for (int ii = 0; ii < 4; ++ii)
-        if (ii != i) r[kr++] = ii;
-      for (int jj = 0; jj < 4; ++jj)
-        if (jj != j) cc[kc++] = jj;
-      D1 mi = det3v(g[r[0]][cc[0]], g[r[0]][cc[1]], g[r[0]][cc[2]], g[r[1]][cc[0]], g[r[1]][cc[1]],
-                    g[r[1]][cc[2]], g[r[2]][cc[0]], g[r[2]][cc[1]], g[r[2]][cc[2]]);
-      cof[i][j] = ((i + j) % 2 == 0) ? mi : -mi;
-    }
-  D1 det = g[0][0] * cof[0][0] + g[0][1] * cof[0][1] + g[0][2] * cof[0][2] + g[0][3] * cof[0][3];
+  // the inverse metric with its first derivatives: cofactors of the symmetric matrix, each
+  // index a compile-time constant (fully unrolled)
+  D1 cof[NC];
+#pragma unroll
+  for (int n = 0; n < NC; ++n) {
+    const int i = prow(n), j = pcol(n);
+    const int r0 = i == 0 ? 1 : 0, r1 = i <= 1 ? 2 : 1, r2 = i <= 2 ? 3 : 2;
+    const int c0 = j == 0 ? 1 : 0, c1 = j <= 1 ? 2 : 1, c2 = j <= 2 ? 3 : 2;
+    D1 mi = det3v(g2[r0][c0].v, g2[r0][c1].v, g2[r0][c2].v, g2[r1][c0].v, g2[r1][c1].v, g2[r1][c2].v,
+                  g2[r2][c0].v, g2[r2][c1].v, g2[r2][c2].v);
+    cof[n] = ((i + j) % 2 == 0) ? mi : -mi;
+  }
+  const D1 det = g2[0][0].v * cof[pidx(0, 0)] + g2[0][1].v * cof[pidx(0, 1)] + g2[0][2].v * cof[pidx(0, 2)] +
+                 g2[0][3].v * cof[pidx(0, 3)];
+  const D1 idet = D1(1.0) / det;
+#pragma unroll
   for (int a = 0; a < 4; ++a) {
     D1 s = dconst(0.0);
+#pragma unroll
     for (int k = 0; k < 4; ++k)
+#pragma unroll
       for (int d = 0; d < 4; ++d) {
-        D1 G = 0.5 * (dg[k][a][d] + dg[d][a][k] - dg[a][k][d]);
-        s = s + (cof[d][k] / det) * G;
+        // Gamma_{a,kd} = (d_k g_ad + d_d g_ak - d_a g_kd) / 2, with d_k g_ab = g2[a][b].d[k]
+        const D1 low = 0.5 * (g2[a][d].d[k] + g2[a][k].d[d] - g2[k][d].d[a]);
+        s = s + (cof[pidx(d, k)] * idet) * low;
       }
     out[a] = -s.v;
+#pragma unroll
     for (int k = 0; k < 4; ++k) out[4 + k + 4 * a] = -s.d[k];
   }
 }
@@ -477,7 +477,7 @@ TGH_HD double core_rate(const Case& c) {
   return c.rho_max > k ? c.rho_max : k;
 }
 // cbrt(eps) r_0 with eps the double epsilon (src/interior.jl:545)
-TGH_HD double layer_rate_step(const Case& c) { return 6.055454452393343e-06 * c.r0; }
+TGH_HD double layer_rate_step(const Case& c) { return 6.0554544523933395e-06 * c.r0; }
 
 // the state the case puts at x (case_state_tuple): the background through the core rule
 TGH_HD void exact_state(const Case& c, double t, const double* x, double* out) {

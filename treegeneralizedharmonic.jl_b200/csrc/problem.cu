@@ -34,6 +34,7 @@ struct tgh_problem {
   Case cs;
   bool diss = false, intr = false;
   cudaStream_t stream = nullptr;
+  cudaStream_t cap = nullptr;  // the stream graphs are captured on
   std::string err;
   // device buffers
   double* work = nullptr;     // the ghosted working array (also W0 of the batched form)
@@ -457,6 +458,7 @@ int tgh_problem_create(const tgh_config* cfg, const tgh_mesh* m, void* cuda_stre
 void tgh_problem_destroy(tgh_problem* p) {
   if (!p) return;
   if (p->gexec) cudaGraphExecDestroy(p->gexec);
+  if (p->cap) cudaStreamDestroy(p->cap);
   void* bufs[] = {p->work, p->Hsrc, p->blk, p->primary, p->runs, p->hooks, p->scratch, p->part,
                   p->k, p->acc, p->y, p->u0, p->W1, p->W2, p->bacc};
   for (void* b : bufs)
@@ -614,11 +616,18 @@ int tgh_step_batched(tgh_problem* p, double* u, double t, double dt, int nsteps)
       cudaGraphExecDestroy(p->gexec);
       p->gexec = nullptr;
     }
+    // capture on the problem's own stream (the caller's may be the legacy default stream,
+    // which cannot be captured); the graph is then launched on the caller's stream
+    if (!p->cap) CK(cudaStreamCreateWithFlags(&p->cap, cudaStreamNonBlocking));
     cudaGraph_t graph;
-    CK(cudaStreamBeginCapture(p->stream, cudaStreamCaptureModeThreadLocal));
+    cudaStream_t user = p->stream;
+    p->stream = p->cap;
+    cudaError_t eb = cudaStreamBeginCapture(p->cap, cudaStreamCaptureModeThreadLocal);
     int st = TGH_OK;
-    for (int n = 0; n < nsteps && st == TGH_OK; ++n) st = batched_step(p, t + n * dt, dt);
-    cudaError_t ee = cudaStreamEndCapture(p->stream, &graph);
+    if (eb == cudaSuccess)
+      for (int n = 0; n < nsteps && st == TGH_OK; ++n) st = batched_step(p, t + n * dt, dt);
+    cudaError_t ee = eb == cudaSuccess ? cudaStreamEndCapture(p->cap, &graph) : eb;
+    p->stream = user;
     if (st) return st;
     CK(ee);
     CK(cudaGraphInstantiate(&p->gexec, graph, 0));
@@ -671,6 +680,26 @@ int tgh_time_rhs(tgh_problem* p, const double* u, double t, int mode, int nlaunc
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
   *ms_per_launch = ms / nlaunch;
+  return TGH_OK;
+}
+
+// Diagnostics: the sampled gauge source (device to device), and the analytic state and gauge
+// source of the problem's case at one point evaluated by a one-thread device kernel.
+int tgh_copy_hsrc(tgh_problem* p, double* dst) {
+  if (!p->Hsrc) return fail(p, TGH_ERR_ARG, "this problem has no sampled gauge source");
+  CK(cudaMemcpyAsync(dst, p->Hsrc, tgh_state_length(p) * sizeof(double), cudaMemcpyDeviceToDevice, p->stream));
+  CK(cudaStreamSynchronize(p->stream));
+  return TGH_OK;
+}
+int tgh_point_physics(tgh_problem* p, double t, const double* x_host, double* out40_host) {
+  double* d;
+  CK(cudaMalloc(&d, 43 * sizeof(double)));
+  CK(cudaMemcpy(d, x_host, 3 * sizeof(double), cudaMemcpyHostToDevice));
+  point_physics_kernel<<<1, 1, 0, p->stream>>>(p->cs, t, d, d + 3);
+  CK(cudaGetLastError());
+  CK(cudaStreamSynchronize(p->stream));
+  CK(cudaMemcpy(out40_host, d + 3, 40 * sizeof(double), cudaMemcpyDeviceToHost));
+  cudaFree(d);
   return TGH_OK;
 }
 
