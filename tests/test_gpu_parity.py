@@ -111,7 +111,10 @@ def test_rk4_step_matches_oracle(tgh, oracle, row):
     P.rk4_step(ug, t, dt)
     uo = u.copy()
     O.rk4_step(uo, t, dt)
-    tol = 1e-9 if name == "kerr_schild_moving" else 1e-12  # the target rate's difference quotient
+    # the moving core's target lies on the sphere r_0 = 0.8 just outside the a = 0.7 ring
+    # singularity, where the analytic state's roundoff (two correct evaluations differ by
+    # ~1e-13 relative) is amplified 1e5-fold by the target rate's centered time difference
+    tol = 1e-7 if name == "kerr_schild_moving" else 1e-12
     assert np.max(np.abs(ug.cpu().numpy() - uo)) < tol
     if not name.endswith("pasted"):
         ub = _to_gpu(u)

@@ -49,6 +49,7 @@ struct tgh_problem {
   std::vector<int> nprol;
   unsigned long long* scratch = nullptr;  // speed reduction: max bits, non-finite count
   double* part = nullptr;                 // error-norm partials + result
+  double* coef = nullptr;                 // per-point coefficients between the two RHS kernels
   int npart = 0;
   // plain-form RK4 buffers (state layout)
   double *k = nullptr, *acc = nullptr, *y = nullptr, *u0 = nullptr;
@@ -349,6 +350,7 @@ static RhsArgs base_args(tgh_problem* p, const double* work, double t) {
   std::memset(&a, 0, sizeof(a));
   a.work = work;
   a.Hsrc = p->Hsrc;
+  a.coef = p->coef;
   a.blk = p->blk;
   a.N1 = p->N1;
   a.Wd = p->Wd;
@@ -439,6 +441,7 @@ int tgh_problem_create(const tgh_config* cfg, const tgh_mesh* m, void* cuda_stre
   CK(cudaMalloc(&p->work, (size_t)p->Wv * NV * p->nb * sizeof(double)));
   CK(cudaMemsetAsync(p->work, 0, (size_t)p->Wv * NV * p->nb * sizeof(double), p->stream));
   CK(cudaMalloc(&p->scratch, 2 * sizeof(unsigned long long)));
+  CK(cudaMalloc(&p->coef, (size_t)NCOEF * p->npts * sizeof(double)));
   p->npart = (int)grid_for(p->npts, 128);
   CK(cudaMalloc(&p->part, (3 * (size_t)p->npart + 2) * sizeof(double)));
   double wp[10] = {0};
@@ -459,7 +462,7 @@ void tgh_problem_destroy(tgh_problem* p) {
   if (!p) return;
   if (p->gexec) cudaGraphExecDestroy(p->gexec);
   if (p->cap) cudaStreamDestroy(p->cap);
-  void* bufs[] = {p->work, p->Hsrc, p->blk, p->primary, p->runs, p->hooks, p->scratch, p->part,
+  void* bufs[] = {p->work, p->Hsrc, p->blk, p->primary, p->runs, p->hooks, p->scratch, p->part, p->coef,
                   p->k, p->acc, p->y, p->u0, p->W1, p->W2, p->bacc};
   for (void* b : bufs)
     if (b) cudaFree(b);

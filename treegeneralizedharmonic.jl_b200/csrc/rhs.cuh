@@ -99,15 +99,29 @@ template <int Q, class T> __device__ __forceinline__ T st_mixed(const double* p,
   return acc;
 }
 
+// Per-point coefficients the head kernel leaves for the Pi kernel (struct of arrays,
+// slot c of point p at coef[c * npts + p]).
+enum {
+  CF_B0 = 0, CF_B1, CF_B2,            // beta^i
+  CF_DIVB,                            // d_i beta^i
+  CF_DA0, CF_DA1, CF_DA2,             // d_i (alpha sqrt(gamma) gamma^{ij})
+  CF_AXX, CF_AXY, CF_AXZ, CF_AYY, CF_AYZ, CF_AZZ,  // alpha sqrt(gamma) gamma^{ij}, off-diagonals doubled
+  CF_EH,                              // eps_KO / h
+  CF_W,                               // the layer's w (1 outside; negative: the point is finished)
+  CF_M0,                              // 10 additive terms: msrc (+ the layer's relaxation)
+  NCOEF = CF_M0 + NC
+};
+
 // one launch's geometry and buffers
 struct RhsArgs {
   const double* work;     // ghosted working array, (W^3 x 20) per block
   const double* Hsrc;     // sampled gauge source, (N1^3 x 20) per block, or null
   const double* matter;   // (N1^3 x 10) per block, or null
   const double* blk;      // per block: domain lo (3), h, integer corner (3), pad
+  double* coef;           // NCOEF x npts scratch between the two kernels
   double* du;             // MODE_DU: state layout
   // MODE_STAGE
-  const double* u0;       // state at the start of the step (ghosted layout), null at stage 1
+  const double* u0;       // state at the start of the step (ghosted layout)
   double* acc;            // accumulator (state layout)
   double* next;           // the next stage's ghosted working array (owned points written)
   double ca, cb;          // next = u0 + ca k ; acc = (stage 1 ? u0 : acc) + cb k ; final: next = acc + cb k
@@ -117,15 +131,68 @@ struct RhsArgs {
   double t;
 };
 
-template <int Q, bool DISS, class T, class Emit>
-__device__ __forceinline__ void rhs_core(const Case& cs, const RhsArgs& A, const double* wk, long sv, int b,
-                                         long ip, const double* x, double inv_h, Emit& out) {
+// Where a finished component goes: straight to du (plain form) or into the RK4 stage
+// update (batched form).
+struct EmitDu {
+  double* d;
+  long S;
+  __device__ __forceinline__ void put(int v, double val) { d[v * S] = val; }
+};
+struct EmitStage {
+  double* ac;
+  double* nx;
+  const double* u0;
+  long S, sv;
+  double ca, cb;
+  int stage;
+  __device__ __forceinline__ void put(int v, double kv) {
+    if (stage == 4) {
+      nx[v * sv] = fma(cb, kv, ac[v * S]);
+    } else {
+      const double un = u0[v * sv];
+      ac[v * S] = fma(cb, kv, stage == 1 ? un : ac[v * S]);
+      nx[v * sv] = fma(ca, kv, un);
+    }
+  }
+};
+
+// the owned point p of a launch: block, index within the block, position, work offset
+struct PointIdx {
+  int b, i, j, k;
+  long ip, wo;
+  double x[3], h;
+};
+__device__ __forceinline__ PointIdx point_index(const RhsArgs& A, long p) {
+  PointIdx q;
+  const int N1 = A.N1;
+  const long S = (long)N1 * N1 * N1;
+  q.b = (int)(p / S);
+  q.ip = p - (long)q.b * S;
+  q.k = (int)(q.ip / ((long)N1 * N1));
+  q.j = (int)((q.ip / N1) % N1);
+  q.i = (int)(q.ip % N1);
+  const double* bl = A.blk + 8 * q.b;
+  q.h = bl[3];
+  q.x[0] = __dadd_rn(bl[0], __dmul_rn(bl[4] + (double)q.i, q.h));
+  q.x[1] = __dadd_rn(bl[1], __dmul_rn(bl[5] + (double)q.j, q.h));
+  q.x[2] = __dadd_rn(bl[2], __dmul_rn(bl[6] + (double)q.k, q.h));
+  const long sv = (long)A.Wd * A.Wd * A.Wd;
+  q.wo = (long)q.b * NV * sv + (q.i + A.G) + (long)A.Wd * ((q.j + A.G) + (long)A.Wd * (q.k + A.G));
+  return q;
+}
+
+// Steps 1-3 of the streaming order at one point (src/evolution.jl:258-297): the state, the
+// first derivatives of h, the coefficient set, d_t h (with the dissipation), the gauge
+// source, the reduced source with damping (+ matter), and the coefficients the Pi
+// components read (src/pointwise.jl:754-778).
+template <int Q, bool DISS, class T>
+__device__ __forceinline__ void rhs_head(const Case& cs, const RhsArgs& A, const double* wk, long sv, int b,
+                                         long ip, const double* x, double inv_h, T dth[NC], T msrc[NC],
+                                         T cf[CF_EH + 1]) {
   const long s1 = 1, s2 = A.Wd, s3 = (long)A.Wd * A.Wd;
-  const T ih = T(inv_h), ih2 = T(inv_h * inv_h);
+  const T ih = T(inv_h);
   const T eh = T(DISS ? dissipation_rate(cs, A.t, x) * inv_h : 0.0);
   const T g0 = T(damping_rate(cs, A.t, x));
-
-  // (1) state, first derivatives of h, coefficients
   T hv[NC], dh0[NC], dh1[NC], dh2[NC];
 #pragma unroll
   for (int v = 0; v < NC; ++v) {
@@ -138,20 +205,15 @@ __device__ __forceinline__ void rhs_core(const Case& cs, const RhsArgs& A, const
   Coef<T> C;
   metric_quantities(hv, C);
   const T a_div = C.alpha / C.sqrtg;
-  // (2) d_t h, stored at once
-  T dth[NC];
 #pragma unroll
   for (int v = 0; v < NC; ++v) {
     const double* p = wk + v * sv;
     T s = C.beta[0] * dh0[v] + C.beta[1] * dh1[v] + C.beta[2] * dh2[v] + a_div * ld<T>(p + NC * sv);
     if (DISS) s = fma(eh, st_ko<Q, T>(p, s1, hv[v]) + st_ko<Q, T>(p, s2, hv[v]) + st_ko<Q, T>(p, s3, hv[v]), s);
     dth[v] = s;
-    out.put(v, (double)s);
   }
-  // (3) the source
   const T* dh[3] = {dh0, dh1, dh2};
   const T* D[4] = {dth, dh0, dh1, dh2};
-  T msrc[NC];
   if (cs.gauge == TGH_GAUGE_NONE) {
     T Hl[4], dHl[4][4];
     gh_source<T, false>(C, D, Hl, dHl, g0, T(cs.g2), msrc);
@@ -179,13 +241,152 @@ __device__ __forceinline__ void rhs_core(const Case& cs, const RhsArgs& A, const
 #pragma unroll
     for (int v = 0; v < NC; ++v) msrc[v] += ms[v];
   }
-  // (4) the coefficients of the Pi components
   T divb, divA[3];
   metric_divergences(C, dh, divb, divA);
   const T am = C.alpha * C.sqrtg;
-  T Axx = am * C.gamu[0], Axy = T(2.0) * am * C.gamu[1], Axz = T(2.0) * am * C.gamu[2];
-  T Ayy = am * C.gamu[3], Ayz = T(2.0) * am * C.gamu[4], Azz = am * C.gamu[5];
-  const T b0 = C.beta[0], b1 = C.beta[1], b2 = C.beta[2];
+  cf[CF_B0] = C.beta[0];
+  cf[CF_B1] = C.beta[1];
+  cf[CF_B2] = C.beta[2];
+  cf[CF_DIVB] = divb;
+  cf[CF_DA0] = divA[0];
+  cf[CF_DA1] = divA[1];
+  cf[CF_DA2] = divA[2];
+  cf[CF_AXX] = am * C.gamu[0];
+  cf[CF_AXY] = T(2.0) * am * C.gamu[1];
+  cf[CF_AXZ] = T(2.0) * am * C.gamu[2];
+  cf[CF_AYY] = am * C.gamu[3];
+  cf[CF_AYZ] = T(2.0) * am * C.gamu[4];
+  cf[CF_AZZ] = am * C.gamu[5];
+  cf[CF_EH] = eh;
+}
+
+// The head kernel: d_t h at every owned point (emitted), the coefficients and additive
+// source of the Pi components (stored for the Pi kernel), and - with an interior - the
+// branches of gh_rhs_point! (src/evolution.jl:489-695): a frozen core is finished here and
+// never reaches a stencil; a layer point combines w F - rho (u - u_exact) (+ the moving
+// target's rate), the Pi half as w * (stencil part) + coef[CF_M0 + v].
+template <int Q, bool DISS, int MODE, bool INT>
+__global__ void __launch_bounds__(128) rhs_head_kernel(const Case cs, const RhsArgs A) {
+  const long p = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= A.npts) return;
+  const PointIdx q = point_index(A, p);
+  const long S = (long)A.N1 * A.N1 * A.N1;
+  const long sv = (long)A.Wd * A.Wd * A.Wd;
+  const double* wk = A.work + q.wo;
+  const double inv_h = 1.0 / q.h;
+  double* cfo = A.coef + p;
+  EmitDu ed{A.du + (long)q.b * NV * S + q.ip, S};
+  EmitStage es{A.acc + (long)q.b * NV * S + q.ip, A.next + q.wo, A.u0 + q.wo, S, sv, A.ca, A.cb, A.stage};
+  auto put = [&](int v, double val) {
+    if (MODE == MODE_DU) ed.put(v, val);
+    else es.put(v, val);
+  };
+  double w = 1.0, rho = 0.0, r = 0.0;
+  if (INT) {
+    r = interior_radius(cs, A.t, q.x);
+    const bool frozen = cs.interior == TGH_INT_PASTED ? r < cs.r1 : r < cs.r0;
+    if (frozen) {
+      if (core_follows(cs)) {
+        const double rc = core_rate(cs), dl = layer_rate_step(cs);
+        double xc[3], hd[NC], Pd[NC];
+        core_position(cs, A.t, q.x, xc);
+        background_state(cs, A.t, xc, hd, Pd);
+        double dthd[NC], dtPd[NC];
+        const double sw = smoothstep(4.0 * r / cs.r0 - 1.0);
+        if (sw == 0.0) {
+          for (int n = 0; n < NC; ++n) dthd[n] = dtPd[n] = 0.0;
+        } else {
+          const double tp = A.t + dl, tm = A.t - dl;
+          double xp[3], xm[3], hp[NC], Pp[NC], hm[NC], Pm[NC];
+          core_position(cs, tp, q.x, xp);
+          core_position(cs, tm, q.x, xm);
+          background_state(cs, tp, xp, hp, Pp);
+          background_state(cs, tm, xm, hm, Pm);
+          const double f = sw / (tp - tm);
+          for (int n = 0; n < NC; ++n) {
+            dthd[n] = f * (hp[n] - hm[n]);
+            dtPd[n] = f * (Pp[n] - Pm[n]);
+          }
+        }
+        double hu[NC], rr[NC];
+        for (int v = 0; v < NC; ++v) hu[v] = wk[v * sv];
+        core_relaxation_rate(hu, hd, rc, dthd, rr);
+        for (int v = 0; v < NC; ++v) {
+          put(v, rr[v]);
+          put(NC + v, dtPd[v] - rc * (wk[(NC + v) * sv] - Pd[v]));
+        }
+      } else {
+        for (int v = 0; v < NV; ++v) put(v, 0.0);
+      }
+      cfo[CF_W * A.npts] = -1.0;
+      return;
+    }
+    if (r < cs.r1) layer_profiles(cs, r, w, rho);
+  }
+  double dth[NC], msrc[NC], cf[CF_EH + 1];
+  rhs_head<Q, DISS, double>(cs, A, wk, sv, q.b, q.ip, q.x, inv_h, dth, msrc, cf);
+#pragma unroll
+  for (int c = 0; c <= CF_EH; ++c) cfo[c * A.npts] = cf[c];
+  if (!INT || r >= cs.r1) {
+#pragma unroll
+    for (int v = 0; v < NC; ++v) {
+      put(v, dth[v]);
+      cfo[(CF_M0 + v) * A.npts] = msrc[v];
+    }
+    cfo[CF_W * A.npts] = 1.0;
+    return;
+  }
+  // the layer r_0 <= r < r_1
+  if (core_follows(cs)) {
+    const double dl = layer_rate_step(cs);
+    double hm[NC], Pm[NC], dthm[NC], Pp[NC], Pq[NC], hx[NC];
+    background_state(cs, A.t, q.x, hm, Pm, dthm);
+    const double tp = A.t + dl, tm = A.t - dl;
+    background_state(cs, tp, q.x, hx, Pp);
+    background_state(cs, tm, q.x, hx, Pq);
+    const double om = 1.0 - w;
+    for (int v = 0; v < NC; ++v) {
+      const double dtP = (Pp[v] - Pq[v]) / (tp - tm);
+      put(v, w * dth[v] + om * dthm[v] - rho * (wk[v * sv] - hm[v]));
+      cfo[(CF_M0 + v) * A.npts] = w * msrc[v] + om * dtP - rho * (wk[(NC + v) * sv] - Pm[v]);
+    }
+  } else {
+    double he[NC], Pe[NC];
+    background_state(cs, A.t, q.x, he, Pe);
+    for (int v = 0; v < NC; ++v) {
+      put(v, w * dth[v] - rho * (wk[v * sv] - he[v]));
+      cfo[(CF_M0 + v) * A.npts] = w * msrc[v] - rho * (wk[(NC + v) * sv] - Pe[v]);
+    }
+  }
+  cfo[CF_W * A.npts] = w;
+}
+
+// Step 4 (src/evolution.jl:324-354): per component v the stencils of h_v and Pi_v
+// contracted with the head's coefficients, formed, consumed and dropped:
+//   beta^i d_i Pi + (d_i beta^i) Pi + d_i A^{ij} d_j h + A^{ij} d_i d_j h + (eps/h) KO(Pi)
+// then w * that + coef[CF_M0 + v]. Few registers, so many warps hide the load latency.
+template <int Q, bool DISS, int MODE, class T>
+__global__ void __launch_bounds__(128, 4) rhs_pi_kernel(const Case cs, const RhsArgs A) {
+  const long p = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= A.npts) return;
+  const double* cfi = A.coef + p;
+  const double w = cfi[CF_W * A.npts];
+  if (w < 0.0) return;
+  const PointIdx q = point_index(A, p);
+  const long S = (long)A.N1 * A.N1 * A.N1;
+  const long sv = (long)A.Wd * A.Wd * A.Wd;
+  const long s1 = 1, s2 = A.Wd, s3 = (long)A.Wd * A.Wd;
+  const double* wk = A.work + q.wo;
+  const double inv_h = 1.0 / q.h;
+  const T ih = T(inv_h), ih2 = T(inv_h * inv_h);
+  const T b0 = T(cfi[CF_B0 * A.npts]), b1 = T(cfi[CF_B1 * A.npts]), b2 = T(cfi[CF_B2 * A.npts]);
+  const T divb = T(cfi[CF_DIVB * A.npts]);
+  const T da0 = T(cfi[CF_DA0 * A.npts]), da1 = T(cfi[CF_DA1 * A.npts]), da2 = T(cfi[CF_DA2 * A.npts]);
+  const T Axx = T(cfi[CF_AXX * A.npts]), Axy = T(cfi[CF_AXY * A.npts]), Axz = T(cfi[CF_AXZ * A.npts]);
+  const T Ayy = T(cfi[CF_AYY * A.npts]), Ayz = T(cfi[CF_AYZ * A.npts]), Azz = T(cfi[CF_AZZ * A.npts]);
+  const T eh = T(cfi[CF_EH * A.npts]);
+  EmitDu ed{A.du + (long)q.b * NV * S + q.ip, S};
+  EmitStage es{A.acc + (long)q.b * NV * S + q.ip, A.next + q.wo, A.u0 + q.wo, S, sv, A.ca, A.cb, A.stage};
 #pragma unroll 1
   for (int v = 0; v < NC; ++v) {
     const double* ph = wk + v * sv;
@@ -195,9 +396,9 @@ __device__ __forceinline__ void rhs_core(const Case& cs, const RhsArgs& A, const
     s = fma(b1, ih * st_d1<Q, T>(pp, s2), s);
     s = fma(b2, ih * st_d1<Q, T>(pp, s3), s);
     s = fma(divb, pc, s);
-    s = fma(divA[0], ih * st_d1<Q, T>(ph, s1), s);
-    s = fma(divA[1], ih * st_d1<Q, T>(ph, s2), s);
-    s = fma(divA[2], ih * st_d1<Q, T>(ph, s3), s);
+    s = fma(da0, ih * st_d1<Q, T>(ph, s1), s);
+    s = fma(da1, ih * st_d1<Q, T>(ph, s2), s);
+    s = fma(da2, ih * st_d1<Q, T>(ph, s3), s);
     T p2 = Axx * st_d2<Q, T>(ph, s1, hc);
     p2 = fma(Ayy, st_d2<Q, T>(ph, s2, hc), p2);
     p2 = fma(Azz, st_d2<Q, T>(ph, s3, hc), p2);
@@ -206,139 +407,10 @@ __device__ __forceinline__ void rhs_core(const Case& cs, const RhsArgs& A, const
     p2 = fma(Ayz, st_mixed<Q, T>(ph, s2, s3), p2);
     s = fma(ih2, p2, s);
     if (DISS) s = fma(eh, st_ko<Q, T>(pp, s1, pc) + st_ko<Q, T>(pp, s2, pc) + st_ko<Q, T>(pp, s3, pc), s);
-    out.put(NC + v, (double)(s + msrc[v]));
-  }
-}
-
-// Where a finished component goes: straight to du (plain form), into the RK4 stage update
-// (batched form), or into a local vector the interior branches combine.
-struct EmitDu {
-  double* d;
-  long S;
-  __device__ __forceinline__ void put(int v, double val) { d[v * S] = val; }
-};
-struct EmitStage {
-  double* ac;
-  double* nx;
-  const double* u0;
-  long S, sv;
-  double ca, cb;
-  int stage;
-  __device__ __forceinline__ void put(int v, double kv) {
-    if (stage == 4) {
-      nx[v * sv] = fma(cb, kv, ac[v * S]);
-    } else {
-      const double un = u0[v * sv];
-      ac[v * S] = fma(cb, kv, stage == 1 ? un : ac[v * S]);
-      nx[v * sv] = fma(ca, kv, un);
-    }
-  }
-};
-struct EmitLocal {
-  double* o;
-  __device__ __forceinline__ void put(int v, double val) { o[v] = val; }
-};
-
-// the interior branches of gh_rhs_point! around F (src/evolution.jl:489-695)
-template <int Q, bool DISS, class Emit>
-__device__ __forceinline__ void rhs_interior(const Case& cs, const RhsArgs& A, const double* wk, long sv, int b,
-                                             long ip, const double* x, double inv_h, Emit& em) {
-  const double r = interior_radius(cs, A.t, x);
-  const bool frozen = cs.interior == TGH_INT_PASTED ? r < cs.r1 : r < cs.r0;
-  if (frozen) {
-    if (core_follows(cs)) {
-      const double rho = core_rate(cs), dl = layer_rate_step(cs);
-      double xc[3], hd[NC], Pd[NC];
-      core_position(cs, A.t, x, xc);
-      background_state(cs, A.t, xc, hd, Pd);
-      double dthd[NC], dtPd[NC];
-      const double sw = smoothstep(4.0 * r / cs.r0 - 1.0);
-      if (sw == 0.0) {
-        for (int n = 0; n < NC; ++n) dthd[n] = dtPd[n] = 0.0;
-      } else {
-        const double tp = A.t + dl, tm = A.t - dl;
-        double xp[3], xm[3], hp[NC], Pp[NC], hm[NC], Pm[NC];
-        core_position(cs, tp, x, xp);
-        core_position(cs, tm, x, xm);
-        background_state(cs, tp, xp, hp, Pp);
-        background_state(cs, tm, xm, hm, Pm);
-        const double f = sw / (tp - tm);
-        for (int n = 0; n < NC; ++n) {
-          dthd[n] = f * (hp[n] - hm[n]);
-          dtPd[n] = f * (Pp[n] - Pm[n]);
-        }
-      }
-      double hu[NC], rr[NC];
-      for (int v = 0; v < NC; ++v) hu[v] = wk[v * sv];
-      core_relaxation_rate(hu, hd, rho, dthd, rr);
-      for (int v = 0; v < NC; ++v) {
-        em.put(v, rr[v]);
-        em.put(NC + v, dtPd[v] - rho * (wk[(NC + v) * sv] - Pd[v]));
-      }
-    } else {
-      for (int v = 0; v < NV; ++v) em.put(v, 0.0);
-    }
-    return;
-  }
-  double F[NV];
-  EmitLocal el{F};
-  rhs_core<Q, DISS, double>(cs, A, wk, sv, b, ip, x, inv_h, el);
-  if (r >= cs.r1) {
-    for (int v = 0; v < NV; ++v) em.put(v, F[v]);
-    return;
-  }
-  double w, rho;
-  layer_profiles(cs, r, w, rho);
-  if (core_follows(cs)) {
-    const double dl = layer_rate_step(cs);
-    double hm[NC], Pm[NC], dthm[NC], Pp[NC], Pq[NC], hx[NC];
-    background_state(cs, A.t, x, hm, Pm, dthm);
-    const double tp = A.t + dl, tm = A.t - dl;
-    background_state(cs, tp, x, hx, Pp);
-    background_state(cs, tm, x, hx, Pq);
-    const double om = 1.0 - w;
-    for (int v = 0; v < NC; ++v) {
-      const double dtP = (Pp[v] - Pq[v]) / (tp - tm);
-      em.put(v, w * F[v] + om * dthm[v] - rho * (wk[v * sv] - hm[v]));
-      em.put(NC + v, w * F[NC + v] + om * dtP - rho * (wk[(NC + v) * sv] - Pm[v]));
-    }
-  } else {
-    double he[NC], Pe[NC];
-    background_state(cs, A.t, x, he, Pe);
-    for (int v = 0; v < NC; ++v) {
-      em.put(v, w * F[v] - rho * (wk[v * sv] - he[v]));
-      em.put(NC + v, w * F[NC + v] - rho * (wk[(NC + v) * sv] - Pe[v]));
-    }
-  }
-}
-
-template <int Q, bool DISS, int MODE, bool INT>
-__global__ void __launch_bounds__(128) rhs_kernel(const Case cs, const RhsArgs A) {
-  const long p = (long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (p >= A.npts) return;
-  const int N1 = A.N1;
-  const long S = (long)N1 * N1 * N1;
-  const int b = (int)(p / S);
-  const long ip = p - (long)b * S;
-  const int k = (int)(ip / ((long)N1 * N1));
-  const int j = (int)((ip / N1) % N1);
-  const int i = (int)(ip % N1);
-  const double* bl = A.blk + 8 * b;
-  const double h = bl[3];
-  const double x[3] = {__dadd_rn(bl[0], __dmul_rn(bl[4] + (double)i, h)), __dadd_rn(bl[1], __dmul_rn(bl[5] + (double)j, h)),
-                       __dadd_rn(bl[2], __dmul_rn(bl[6] + (double)k, h))};
-  const long sv = (long)A.Wd * A.Wd * A.Wd;
-  const long wo = (long)b * NV * sv + (i + A.G) + (long)A.Wd * ((j + A.G) + (long)A.Wd * (k + A.G));
-  const double* wk = A.work + wo;
-  const double inv_h = 1.0 / h;
-  if (MODE == MODE_DU) {
-    EmitDu em{A.du + (long)b * NV * S + ip, S};
-    if (INT) rhs_interior<Q, DISS>(cs, A, wk, sv, b, ip, x, inv_h, em);
-    else rhs_core<Q, DISS, double>(cs, A, wk, sv, b, ip, x, inv_h, em);
-  } else {
-    EmitStage em{A.acc + (long)b * NV * S + ip, A.next + wo, A.u0 + wo, S, sv, A.ca, A.cb, A.stage};
-    if (INT) rhs_interior<Q, DISS>(cs, A, wk, sv, b, ip, x, inv_h, em);
-    else rhs_core<Q, DISS, double>(cs, A, wk, sv, b, ip, x, inv_h, em);
+    const double m = cfi[(CF_M0 + v) * A.npts];
+    const double val = w == 1.0 ? (double)s + m : fma(w, (double)s, m);
+    if (MODE == MODE_DU) ed.put(NC + v, val);
+    else es.put(NC + v, val);
   }
 }
 
