@@ -165,6 +165,20 @@ int tgh_step_batched(tgh_problem* p, double* u, double t, double dt, int nsteps)
  * masked, volume-weighted L2 and max of |u - u_exact| over the evolved primaries */
 int tgh_error_norm(tgh_problem* p, const double* u, double t, double* l2, double* linf);
 
+/* --- allocation-free speed (no counterpart in the reference) ---
+ * tgh_max_speed without a problem handle, for callers that cannot allocate device memory
+ * (their device memory belongs to another allocator or pool, or allocation is forbidden in
+ * the loop that asks for the time step). It allocates nothing: its scratch is one fixed
+ * device array in the library, which holds the block table of at most
+ * TGH_NOALLOC_MAX_BLOCKS blocks; larger meshes are refused with TGH_ERR_ARG. u is a device
+ * state vector of mesh's layout; the result and the checks are those of tgh_max_speed. The
+ * first call on a device looks up the array's address (make it before any stream capture);
+ * every call shares the array, so calls that overlap on the GPU race. errbuf (nullable)
+ * receives the message of a failure. */
+#define TGH_NOALLOC_MAX_BLOCKS 8192
+int tgh_max_speed_noalloc(const tgh_config* cfg, const tgh_mesh* mesh, const double* u, double t,
+                          void* cuda_stream, double* lambda, char* errbuf, int errlen);
+
 #ifdef __cplusplus
 }
 #endif

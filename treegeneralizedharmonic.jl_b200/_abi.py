@@ -70,6 +70,8 @@ SIGNATURES = {
     "tgh_rk4_step": (ctypes.c_int, [_VP, _VP, _D, _D]),
     "tgh_step_batched": (ctypes.c_int, [_VP, _VP, _D, _D, ctypes.c_int]),
     "tgh_error_norm": (ctypes.c_int, [_VP, _VP, _D, ctypes.POINTER(_D), ctypes.POINTER(_D)]),
+    "tgh_max_speed_noalloc": (ctypes.c_int, [ctypes.POINTER(Config), ctypes.POINTER(Mesh), _VP, _D, _VP,
+                                             ctypes.POINTER(_D), ctypes.c_char_p, ctypes.c_int]),
 }
 EXTRA_SIGNATURES = {
     "tgh_fp64_probe": (ctypes.c_double, [_VP, ctypes.c_int]),
