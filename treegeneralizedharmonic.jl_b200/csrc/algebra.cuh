@@ -12,45 +12,78 @@
 namespace tgh {
 
 // msrc = -alpha sqrt(gamma) (S0 + Z) from the coefficients, D[c] = d_c g packed (c = t,x,y,z),
-// the lowered gauge source Hl and dHl[a][b] = d_a H_b.
+// the lowered gauge source Hl and dHs = d_a H_b + d_b H_a packed.
+//
+// The terms are formed in the order that keeps the fewest values live at one point (one
+// thread holds them all in registers): first everything that reads D besides the
+// Christoffels - the contracted Christoffel Gamma^c = g^{cx} (g^{ab} d_a g_xb - g^{ab} d_x g_ab / 2),
+// the term Gamma^c d_c g_ab, and C2 + C2^T built one row of g^{-1} (d_a g) at a time - then
+// the 40 Christoffels Gamma^a_bc, after which D is dead, then Gamma.Gamma, the gauge terms
+// and the damping. Same terms as the reference's spelling, summed in another order.
 template <class T, bool HAS_H>
-TGH_HD void gh_source(const Coef<T>& C, const T* const D[4], const T Hl[4],
-                                          const T dHl[4][4], T g0, T g2, T* msrc) {
+TGH_HD void gh_source(const Coef<T>& C, const T* const D[4], const T Hl[4], const T dHs[NC], T g0, T g2,
+                      T* msrc) {
   const T* Gp = C.gu;
+  // (1) Gamma^c
+  T Gup[4];
+  {
+    T V[4];
+#pragma unroll
+    for (int x = 0; x < 4; ++x) {
+      T s = T(0.0), tr = T(0.0);
+#pragma unroll
+      for (int a = 0; a < 4; ++a)
+#pragma unroll
+        for (int b = 0; b < 4; ++b) s = fma(Gp[pidx(a, b)], D[a][pidx(x, b)], s);
+#pragma unroll
+      for (int n = 0; n < NC; ++n) tr = fma(prow(n) == pcol(n) ? Gp[n] : T(2.0) * Gp[n], D[x][n], tr);
+      V[x] = fma(T(-0.5), tr, s);
+    }
+#pragma unroll
+    for (int c = 0; c < 4; ++c) {
+      T s = Gp[pidx(c, 0)] * V[0];
+#pragma unroll
+      for (int x = 1; x < 4; ++x) s = fma(Gp[pidx(c, x)], V[x], s);
+      Gup[c] = s;
+    }
+  }
+  // (2) S = -(d_a H_b + d_b H_a) - Gamma^c d_c g_ab
   T S[NC];
 #pragma unroll
-  for (int n = 0; n < NC; ++n) S[n] = T(0.0);
-  // (1) C2 + C2^T, one first index a at a time: E = G d_a g, Cuu = E G, C2[a][b] = Cuu_{mn} d_m g_{nb}
+  for (int n = 0; n < NC; ++n) {
+    T t5 = Gup[0] * D[0][n];
+#pragma unroll
+    for (int c = 1; c < 4; ++c) t5 = fma(Gup[c], D[c][n], t5);
+    S[n] = HAS_H ? -(dHs[n] + t5) : -t5;
+  }
+  // (3) C2 + C2^T with C2[a][b] = Cuu_{mn} d_m g_nb, Cuu = g^{-1} (d_a g) g^{-1} (symmetric):
+  //     row m of E = g^{-1} d_a g, then Cuu_{mn} for n >= m, consumed at once
 #pragma unroll
   for (int a = 0; a < 4; ++a) {
-    T E[4][4];
-#pragma unroll
-    for (int r = 0; r < 4; ++r)
-#pragma unroll
-      for (int c = 0; c < 4; ++c) {
-        T s = Gp[pidx(r, 0)] * D[a][pidx(0, c)];
-#pragma unroll
-        for (int x = 1; x < 4; ++x) s = fma(Gp[pidx(r, x)], D[a][pidx(x, c)], s);
-        E[r][c] = s;
-      }
-    T Cuu[NC];
-#pragma unroll
-    for (int n = 0; n < NC; ++n) {
-      const int i = prow(n), j = pcol(n);
-      T s = E[i][0] * Gp[pidx(0, j)];
-#pragma unroll
-      for (int y = 1; y < 4; ++y) s = fma(E[i][y], Gp[pidx(y, j)], s);
-      Cuu[n] = s;
-    }
     T C2[4];
 #pragma unroll
-    for (int b = 0; b < 4; ++b) {
-      T s = T(0.0);
+    for (int b = 0; b < 4; ++b) C2[b] = T(0.0);
 #pragma unroll
-      for (int m = 0; m < 4; ++m)
+    for (int m = 0; m < 4; ++m) {
+      T E[4];
 #pragma unroll
-        for (int nn = 0; nn < 4; ++nn) s = fma(Cuu[pidx(m, nn)], D[m][pidx(nn, b)], s);
-      C2[b] = s;
+      for (int c = 0; c < 4; ++c) {
+        T s = Gp[pidx(m, 0)] * D[a][pidx(0, c)];
+#pragma unroll
+        for (int x = 1; x < 4; ++x) s = fma(Gp[pidx(m, x)], D[a][pidx(x, c)], s);
+        E[c] = s;
+      }
+#pragma unroll
+      for (int n = m; n < 4; ++n) {
+        T cu = E[0] * Gp[pidx(0, n)];
+#pragma unroll
+        for (int y = 1; y < 4; ++y) cu = fma(E[y], Gp[pidx(y, n)], cu);
+#pragma unroll
+        for (int b = 0; b < 4; ++b) {
+          C2[b] = fma(cu, D[m][pidx(n, b)], C2[b]);
+          if (n != m) C2[b] = fma(cu, D[n][pidx(m, b)], C2[b]);
+        }
+      }
     }
 #pragma unroll
     for (int n = 0; n < NC; ++n) {
@@ -59,7 +92,7 @@ TGH_HD void gh_source(const Coef<T>& C, const T* const D[4], const T Hl[4],
       if (j == a) S[n] += C2[i];
     }
   }
-  // (2) Christoffels Gamma^a_bc = g^{ax} (d_b g_xc + d_c g_xb - d_x g_bc)/2, packed over (bc)
+  // (4) Christoffels Gamma^a_bc = g^{ax} (d_b g_xc + d_c g_xb - d_x g_bc)/2, packed over (bc)
   T G[4][NC];
 #pragma unroll
   for (int n = 0; n < NC; ++n) {
@@ -75,14 +108,7 @@ TGH_HD void gh_source(const Coef<T>& C, const T* const D[4], const T Hl[4],
       G[a][n] = s;
     }
   }
-  T Gup[4];
-#pragma unroll
-  for (int c = 0; c < 4; ++c) {
-    T s = T(0.0);
-#pragma unroll
-    for (int n = 0; n < NC; ++n) s = fma(prow(n) == pcol(n) ? Gp[n] : T(2.0) * Gp[n], G[c][n], s);
-    Gup[c] = s;
-  }
+  // (5) -2 Gamma^x_ya Gamma^y_xb and + 2 Gamma^c_ab H_c
 #pragma unroll
   for (int n = 0; n < NC; ++n) {
     const int a = prow(n), b = pcol(n);
@@ -91,19 +117,16 @@ TGH_HD void gh_source(const Coef<T>& C, const T* const D[4], const T Hl[4],
     for (int x = 0; x < 4; ++x)
 #pragma unroll
       for (int y = 0; y < 4; ++y) t2 = fma(G[x][pidx(y, a)], G[y][pidx(x, b)], t2);
-    T t5 = Gup[0] * D[0][n];
-#pragma unroll
-    for (int c = 1; c < 4; ++c) t5 = fma(Gup[c], D[c][n], t5);
-    T s = S[n] - T(2.0) * t2 - t5;
+    T s = fma(T(-2.0), t2, S[n]);
     if (HAS_H) {
       T t4 = G[0][n] * Hl[0];
 #pragma unroll
       for (int c = 1; c < 4; ++c) t4 = fma(G[c][n], Hl[c], t4);
-      s = s - (dHl[a][b] + dHl[b][a]) + T(2.0) * t4;
+      s = fma(T(2.0), t4, s);
     }
     S[n] = s;
   }
-  // (3) Gundlach-Pretorius damping with t_a = -alpha delta_a^t
+  // (6) Gundlach-Pretorius damping with t_a = -alpha delta_a^t
   if (g0 != T(0.0)) {
     T Cup[4], Cl[4];
 #pragma unroll

@@ -181,19 +181,15 @@ __device__ __forceinline__ PointIdx point_index(const RhsArgs& A, long p) {
   return q;
 }
 
-// Steps 1-3 of the streaming order at one point (src/evolution.jl:258-297): the state, the
-// first derivatives of h, the coefficient set, d_t h (with the dissipation), the gauge
-// source, the reduced source with damping (+ matter), and the coefficients the Pi
-// components read (src/pointwise.jl:754-778).
+// Steps 1-2 of the streaming order at one point (src/evolution.jl:258-285): the state, the
+// 30 first derivatives of h, the coefficient set and d_t h (with the dissipation).
 template <int Q, bool DISS, class T>
-__device__ __forceinline__ void rhs_head(const Case& cs, const RhsArgs& A, const double* wk, long sv, int b,
-                                         long ip, const double* x, double inv_h, T dth[NC], T msrc[NC],
-                                         T cf[CF_EH + 1]) {
+__device__ __forceinline__ void rhs_dt(const Case& cs, const RhsArgs& A, const double* wk, long sv,
+                                       const double* x, double inv_h, T hv[NC], T dh0[NC], T dh1[NC],
+                                       T dh2[NC], Coef<T>& C, T dth[NC], T& eh) {
   const long s1 = 1, s2 = A.Wd, s3 = (long)A.Wd * A.Wd;
   const T ih = T(inv_h);
-  const T eh = T(DISS ? dissipation_rate(cs, A.t, x) * inv_h : 0.0);
-  const T g0 = T(damping_rate(cs, A.t, x));
-  T hv[NC], dh0[NC], dh1[NC], dh2[NC];
+  eh = T(DISS ? dissipation_rate(cs, A.t, x) * inv_h : 0.0);
 #pragma unroll
   for (int v = 0; v < NC; ++v) {
     const double* p = wk + v * sv;
@@ -201,63 +197,87 @@ __device__ __forceinline__ void rhs_head(const Case& cs, const RhsArgs& A, const
     dh0[v] = ih * st_d1<Q, T>(p, s1);
     dh1[v] = ih * st_d1<Q, T>(p, s2);
     dh2[v] = ih * st_d1<Q, T>(p, s3);
+    // the dissipation stencils read the same rows: sum them here, scale them below
+    if (DISS) dth[v] = st_ko<Q, T>(p, s1, hv[v]) + st_ko<Q, T>(p, s2, hv[v]) + st_ko<Q, T>(p, s3, hv[v]);
   }
-  Coef<T> C;
   metric_quantities(hv, C);
   const T a_div = C.alpha / C.sqrtg;
 #pragma unroll
   for (int v = 0; v < NC; ++v) {
     const double* p = wk + v * sv;
     T s = C.beta[0] * dh0[v] + C.beta[1] * dh1[v] + C.beta[2] * dh2[v] + a_div * ld<T>(p + NC * sv);
-    if (DISS) s = fma(eh, st_ko<Q, T>(p, s1, hv[v]) + st_ko<Q, T>(p, s2, hv[v]) + st_ko<Q, T>(p, s3, hv[v]), s);
+    if (DISS) s = fma(eh, dth[v], s);
     dth[v] = s;
   }
-  const T* dh[3] = {dh0, dh1, dh2};
-  const T* D[4] = {dth, dh0, dh1, dh2};
-  if (cs.gauge == TGH_GAUGE_NONE) {
-    T Hl[4], dHl[4][4];
-    gh_source<T, false>(C, D, Hl, dHl, g0, T(cs.g2), msrc);
-  } else {
-    T Hl[4], dHl[4][4];
-    if (cs.gauge == TGH_GAUGE_SAMPLED) {
-      const long S = (long)A.N1 * A.N1 * A.N1;
-      const double* q = A.Hsrc + (long)b * NV * S + ip;
-#pragma unroll
-      for (int a = 0; a < 4; ++a) Hl[a] = ld<T>(q + a * S);
-#pragma unroll
-      for (int k = 0; k < 16; ++k) dHl[k % 4][k / 4] = ld<T>(q + (4 + k) * S);
-    } else {
-      ks_gauge_source<T>(cs, hv, D, Hl, dHl);
-    }
-    gh_source<T, true>(C, D, Hl, dHl, g0, T(cs.g2), msrc);
-  }
-  if (A.matter) {
-    const long S = (long)A.N1 * A.N1 * A.N1;
-    const double* q = A.matter + (long)b * 10 * S + ip;
-    T m[10], ms[NC];
-#pragma unroll
-    for (int k = 0; k < 10; ++k) m[k] = ld<T>(q + k * S);
-    matter_source(C, m, ms);
-#pragma unroll
-    for (int v = 0; v < NC; ++v) msrc[v] += ms[v];
-  }
+}
+
+// The coefficients the Pi components read (src/pointwise.jl:754-778), stored at once so
+// that the shift, the spatial inverse metric and the divergences are dead before the source.
+template <class T>
+__device__ __forceinline__ void store_pi_coefficients(const Coef<T>& C, const T* const dh[3], T eh, double* cfo,
+                                                      long npts) {
   T divb, divA[3];
   metric_divergences(C, dh, divb, divA);
   const T am = C.alpha * C.sqrtg;
-  cf[CF_B0] = C.beta[0];
-  cf[CF_B1] = C.beta[1];
-  cf[CF_B2] = C.beta[2];
-  cf[CF_DIVB] = divb;
-  cf[CF_DA0] = divA[0];
-  cf[CF_DA1] = divA[1];
-  cf[CF_DA2] = divA[2];
-  cf[CF_AXX] = am * C.gamu[0];
-  cf[CF_AXY] = T(2.0) * am * C.gamu[1];
-  cf[CF_AXZ] = T(2.0) * am * C.gamu[2];
-  cf[CF_AYY] = am * C.gamu[3];
-  cf[CF_AYZ] = T(2.0) * am * C.gamu[4];
-  cf[CF_AZZ] = am * C.gamu[5];
-  cf[CF_EH] = eh;
+  cfo[CF_B0 * npts] = C.beta[0];
+  cfo[CF_B1 * npts] = C.beta[1];
+  cfo[CF_B2 * npts] = C.beta[2];
+  cfo[CF_DIVB * npts] = divb;
+  cfo[CF_DA0 * npts] = divA[0];
+  cfo[CF_DA1 * npts] = divA[1];
+  cfo[CF_DA2 * npts] = divA[2];
+  cfo[CF_AXX * npts] = am * C.gamu[0];
+  cfo[CF_AXY * npts] = T(2.0) * am * C.gamu[1];
+  cfo[CF_AXZ * npts] = T(2.0) * am * C.gamu[2];
+  cfo[CF_AYY * npts] = am * C.gamu[3];
+  cfo[CF_AYZ * npts] = T(2.0) * am * C.gamu[4];
+  cfo[CF_AZZ * npts] = am * C.gamu[5];
+  cfo[CF_EH * npts] = eh;
+}
+
+// The matter term (src/pointwise.jl:667-698) of the point, parked in the additive slots of
+// the Pi coefficients until the source is added to it.
+template <class T>
+__device__ __forceinline__ void store_matter(const Coef<T>& C, const RhsArgs& A, int b, long ip, double* cfo) {
+  const long S = (long)A.N1 * A.N1 * A.N1;
+  const double* q = A.matter + (long)b * 10 * S + ip;
+  T m[10], ms[NC];
+#pragma unroll
+  for (int k = 0; k < 10; ++k) m[k] = ld<T>(q + k * S);
+  matter_source(C, m, ms);
+#pragma unroll
+  for (int v = 0; v < NC; ++v) cfo[(CF_M0 + v) * A.npts] = ms[v];
+}
+
+// Step 3 (src/evolution.jl:286-297): the gauge source (sampled, closed-form Kerr-Schild or
+// none) and the reduced source with damping, from D[c] = d_c h (c = t, x, y, z).
+template <class T>
+__device__ __forceinline__ void rhs_source(const Case& cs, const RhsArgs& A, int b, long ip, const double* x,
+                                           const T hv[NC], const Coef<T>& C, const T* const D[4], T msrc[NC]) {
+  const T g0 = T(damping_rate(cs, A.t, x));
+  if (cs.gauge == TGH_GAUGE_NONE) {
+    gh_source<T, false>(C, D, nullptr, nullptr, g0, T(cs.g2), msrc);
+    return;
+  }
+  T Hl[4], dHs[NC];
+  if (cs.gauge == TGH_GAUGE_SAMPLED) {
+    // rows: H_a (4), then d_c H_a at 4 + c + 4 a
+    const long S = (long)A.N1 * A.N1 * A.N1;
+    const double* q = A.Hsrc + (long)b * NV * S + ip;
+#pragma unroll
+    for (int a = 0; a < 4; ++a) Hl[a] = ld<T>(q + a * S);
+#pragma unroll
+    for (int n = 0; n < NC; ++n) {
+      const int a = prow(n), c = pcol(n);
+      dHs[n] = ld<T>(q + (4 + a + 4 * c) * S) + ld<T>(q + (4 + c + 4 * a) * S);
+    }
+  } else {
+    T dHl[4][4];
+    ks_gauge_source<T>(cs, hv, D, Hl, dHl);
+#pragma unroll
+    for (int n = 0; n < NC; ++n) dHs[n] = dHl[prow(n)][pcol(n)] + dHl[pcol(n)][prow(n)];
+  }
+  gh_source<T, true>(C, D, Hl, dHs, g0, T(cs.g2), msrc);
 }
 
 // The head kernel: d_t h at every owned point (emitted), the coefficients and additive
@@ -323,40 +343,59 @@ __global__ void __launch_bounds__(128) rhs_head_kernel(const Case cs, const RhsA
     }
     if (r < cs.r1) layer_profiles(cs, r, w, rho);
   }
-  double dth[NC], msrc[NC], cf[CF_EH + 1];
-  rhs_head<Q, DISS, double>(cs, A, wk, sv, q.b, q.ip, q.x, inv_h, dth, msrc, cf);
+  // d_t h first, emitted at once (in the layer r_0 <= r < r_1 combined with the target)
+  double hv[NC], dh0[NC], dh1[NC], dh2[NC], dth[NC], eh;
+  Coef<double> C;
+  rhs_dt<Q, DISS, double>(cs, A, wk, sv, q.x, inv_h, hv, dh0, dh1, dh2, C, dth, eh);
+  const bool layer = INT && r < cs.r1;
+  const bool follows = INT && core_follows(cs);
+  if (!layer) {
 #pragma unroll
-  for (int c = 0; c <= CF_EH; ++c) cfo[c * A.npts] = cf[c];
-  if (!INT || r >= cs.r1) {
+    for (int v = 0; v < NC; ++v) put(v, dth[v]);
+  } else if (follows) {
+    double hm[NC], Pm[NC], dthm[NC];
+    background_state(cs, A.t, q.x, hm, Pm, dthm);
+    const double om = 1.0 - w;
+    for (int v = 0; v < NC; ++v) put(v, w * dth[v] + om * dthm[v] - rho * (wk[v * sv] - hm[v]));
+  } else {
+    double he[NC], Pe[NC];
+    background_state(cs, A.t, q.x, he, Pe);
+    for (int v = 0; v < NC; ++v) put(v, w * dth[v] - rho * (wk[v * sv] - he[v]));
+  }
+  // the Pi coefficients (and the matter term), then the source
+  const double* dh[3] = {dh0, dh1, dh2};
+  store_pi_coefficients(C, dh, eh, cfo, A.npts);
+  if (A.matter) store_matter(C, A, q.b, q.ip, cfo);
+  double msrc[NC];
+  const double* D[4] = {dth, dh0, dh1, dh2};
+  rhs_source(cs, A, q.b, q.ip, q.x, hv, C, D, msrc);
+  if (A.matter) {
 #pragma unroll
-    for (int v = 0; v < NC; ++v) {
-      put(v, dth[v]);
-      cfo[(CF_M0 + v) * A.npts] = msrc[v];
-    }
+    for (int v = 0; v < NC; ++v) msrc[v] += cfo[(CF_M0 + v) * A.npts];
+  }
+  if (!layer) {
+#pragma unroll
+    for (int v = 0; v < NC; ++v) cfo[(CF_M0 + v) * A.npts] = msrc[v];
     cfo[CF_W * A.npts] = 1.0;
     return;
   }
-  // the layer r_0 <= r < r_1
-  if (core_follows(cs)) {
+  // the layer's Pi half: w msrc - rho (Pi - Pi_target) (+ (1 - w) d_t Pi_target, moving core)
+  if (follows) {
     const double dl = layer_rate_step(cs);
-    double hm[NC], Pm[NC], dthm[NC], Pp[NC], Pq[NC], hx[NC];
-    background_state(cs, A.t, q.x, hm, Pm, dthm);
+    double hx[NC], Pm[NC], Pp[NC], Pq[NC];
+    background_state(cs, A.t, q.x, hx, Pm);
     const double tp = A.t + dl, tm = A.t - dl;
     background_state(cs, tp, q.x, hx, Pp);
     background_state(cs, tm, q.x, hx, Pq);
     const double om = 1.0 - w;
     for (int v = 0; v < NC; ++v) {
       const double dtP = (Pp[v] - Pq[v]) / (tp - tm);
-      put(v, w * dth[v] + om * dthm[v] - rho * (wk[v * sv] - hm[v]));
       cfo[(CF_M0 + v) * A.npts] = w * msrc[v] + om * dtP - rho * (wk[(NC + v) * sv] - Pm[v]);
     }
   } else {
     double he[NC], Pe[NC];
     background_state(cs, A.t, q.x, he, Pe);
-    for (int v = 0; v < NC; ++v) {
-      put(v, w * dth[v] - rho * (wk[v * sv] - he[v]));
-      cfo[(CF_M0 + v) * A.npts] = w * msrc[v] - rho * (wk[(NC + v) * sv] - Pe[v]);
-    }
+    for (int v = 0; v < NC; ++v) cfo[(CF_M0 + v) * A.npts] = w * msrc[v] - rho * (wk[(NC + v) * sv] - Pe[v]);
   }
   cfo[CF_W * A.npts] = w;
 }
