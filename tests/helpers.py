@@ -39,6 +39,9 @@ def rhs_error(du_gpu, du_ref, scale, forest):
     return float(np.max(np.max(np.abs(a - b), axis=1) / scale))
 
 
+N_ROWS = 19
+
+
 def cases(tgh):
     """(name, case, forest, q, t) rows the GPU parity tests run on."""
     rows = []
@@ -61,6 +64,15 @@ def cases(tgh):
     c = tgh.kerr_schild_case(M=1.0, a=0.7, halfwidth=2.0, r0=0.8, r1=1.3, gauge="algebraic",
                              eps_ko={"eps_out": 0.5, "eps_in": 2.0, "r_1": 1.3, "r_h": 1.7, "c0": (0, 0, 0)})
     rows.append(("kerr_schild_horizon_dissipation", c, tgh.gh_forest(c, 8, 2), 4, 0.0))
+    # blocks of N = 32, the size the kernels are also compiled for with fixed strides
+    for q in (2, 4, 6, 8):
+        c = tgh.gauge_wave_case(eps_ko=0.5, gamma0=1.0, gamma2=-0.5)
+        rows.append((f"gauge_wave_q{q}_n32", c, tgh.gh_forest(c, 32, 2), q, 0.25))
+    c = tgh.kerr_schild_case(M=1.0, a=0.7, halfwidth=4.0, r0=0.8, r1=1.3, gauge="sampled")
+    rows.append(("kerr_schild_damped_n32", c, tgh.gh_forest(c, 32, 2), 4, 0.0))
+    c = tgh.kerr_schild_case(M=1.0, a=0.7, halfwidth=4.0, r0=0.8, r1=1.3, gauge="algebraic")
+    rows.append(("kerr_schild_algebraic_n32", c, tgh.gh_forest(c, 32, 2), 4, 0.0))
+    assert len(rows) == N_ROWS
     return rows
 
 

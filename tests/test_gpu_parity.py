@@ -11,7 +11,7 @@ import numpy as np
 import pytest
 import torch
 
-from helpers import cases, rhs_error, rhs_scale, two_level_forest
+from helpers import N_ROWS, cases, rhs_error, rhs_scale, two_level_forest
 
 pytestmark = pytest.mark.gpu
 
@@ -33,7 +33,7 @@ def _initial(tgh, P, O, case, forest, name, t):
     return u
 
 
-@pytest.mark.parametrize("row", range(13))
+@pytest.mark.parametrize("row", range(N_ROWS))
 def test_rhs_matches_oracle(tgh, oracle, row):
     name, case, forest, q, t = cases(tgh)[row]
     P = tgh.GHProblem(case, forest, q, margin_check=False)
@@ -100,7 +100,7 @@ def test_fill_matches_oracle(tgh, oracle, which):
         assert np.array_equal(wg, wo)
 
 
-@pytest.mark.parametrize("row", [0, 2, 6, 7, 9, 11])
+@pytest.mark.parametrize("row", [0, 2, 6, 7, 9, 11, 14, 17, 18])
 def test_rk4_step_matches_oracle(tgh, oracle, row):
     name, case, forest, q, t = cases(tgh)[row]
     P = tgh.GHProblem(case, forest, q, margin_check=False)

@@ -181,6 +181,18 @@ __device__ __forceinline__ PointIdx point_index(const RhsArgs& A, long p) {
   return q;
 }
 
+// The launch's geometry with the block size fixed at compile time when N1S > 0 (the usual
+// N = 32 blocks): every stencil offset is then an immediate of its load instruction.
+template <int Q, int N1S> __device__ __forceinline__ RhsArgs fixed_geometry(const RhsArgs& A) {
+  RhsArgs B = A;
+  if (N1S > 0) {
+    B.N1 = N1S;
+    B.G = Q / 2 + 1;
+    B.Wd = N1S + 2 * (Q / 2 + 1);
+  }
+  return B;
+}
+
 // Steps 1-2 of the streaming order at one point (src/evolution.jl:258-285): the state, the
 // 30 first derivatives of h, the coefficient set and d_t h (with the dissipation).
 template <int Q, bool DISS, class T>
@@ -285,8 +297,9 @@ __device__ __forceinline__ void rhs_source(const Case& cs, const RhsArgs& A, int
 // branches of gh_rhs_point! (src/evolution.jl:489-695): a frozen core is finished here and
 // never reaches a stencil; a layer point combines w F - rho (u - u_exact) (+ the moving
 // target's rate), the Pi half as w * (stencil part) + coef[CF_M0 + v].
-template <int Q, bool DISS, int MODE, bool INT>
-__global__ void __launch_bounds__(128) rhs_head_kernel(const Case cs, const RhsArgs A) {
+template <int Q, bool DISS, int MODE, bool INT, int N1S>
+__global__ void __launch_bounds__(128) rhs_head_kernel(const Case cs, const RhsArgs A0) {
+  const RhsArgs A = fixed_geometry<Q, N1S>(A0);
   const long p = (long)blockIdx.x * blockDim.x + threadIdx.x;
   if (p >= A.npts) return;
   const PointIdx q = point_index(A, p);
@@ -404,8 +417,9 @@ __global__ void __launch_bounds__(128) rhs_head_kernel(const Case cs, const RhsA
 // contracted with the head's coefficients, formed, consumed and dropped:
 //   beta^i d_i Pi + (d_i beta^i) Pi + d_i A^{ij} d_j h + A^{ij} d_i d_j h + (eps/h) KO(Pi)
 // then w * that + coef[CF_M0 + v]. Few registers, so many warps hide the load latency.
-template <int Q, bool DISS, int MODE, class T>
-__global__ void __launch_bounds__(128, 4) rhs_pi_kernel(const Case cs, const RhsArgs A) {
+template <int Q, bool DISS, int MODE, class T, int N1S>
+__global__ void __launch_bounds__(128, 4) rhs_pi_kernel(const Case cs, const RhsArgs A0) {
+  const RhsArgs A = fixed_geometry<Q, N1S>(A0);
   const long p = (long)blockIdx.x * blockDim.x + threadIdx.x;
   if (p >= A.npts) return;
   const double* cfi = A.coef + p;
