@@ -10,13 +10,17 @@
 namespace tgh {
 
 // A run of points along x copied from a primary owner: the destination is a working array
-// (block, linear work index), the source an owned point (block, i, j, k) read from either the
-// state vector or the source block's working array; step is 1 (same level) or 2^d (injection
-// from a level d finer).
+// (block, linear work index), the source an owned point (block, i, j, k) of the state vector;
+// step is 1 (same level) or 2^d (injection from a level d finer).
 struct CopyRun {
   int dst_b, dst_w;
   int src_b, si, sj, sk;
   int len, step;
+};
+// One copied point of the batched form's fill: destination block and work index, source
+// (primary) block and work index.
+struct __align__(16) CopyPt {
+  int dst_b, dst_w, src_b, src_w;
 };
 // One prolonged point: the destination, the coarse block, the coarse work index of the
 // stencil box's lower corner and a bit per axis saying whether the axis interpolates.
@@ -45,30 +49,37 @@ __device__ __forceinline__ void point_pos(const double* blk, int b, int i, int j
   x[2] = __dadd_rn(bl[2], __dmul_rn(bl[6] + (double)k, bl[3]));
 }
 
-// stage 0 of a fill: copies. from_work: read the source from the working array (batched
-// form, where the state lives in the working array), else from the state vector u.
+// stage 0 of the plain form's fill: the scatter of the state vector u into the working
+// array and the copies into ghost points, one warp per run of points along x
 __global__ void fill_copy_kernel(const CopyRun* __restrict__ runs, int nruns, const double* __restrict__ u,
-                                 double* __restrict__ work, Geo g, int from_work) {
-  // one warp per run, lanes over the run's points, loop over variables
+                                 double* __restrict__ work, Geo g) {
   const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int lane = threadIdx.x & 31;
   if (warp >= nruns) return;
   const CopyRun r = runs[warp];
   for (int e = lane; e < r.len; e += 32) {
-    const double* src;
-    long sstride;
-    if (from_work) {
-      src = u + (long)r.src_b * NV * g.Wv + (r.si + e * r.step + g.G) +
-            (long)g.Wd * ((r.sj + g.G) + (long)g.Wd * (r.sk + g.G));
-      sstride = g.Wv;
-    } else {
-      src = u + (long)r.src_b * NV * g.S + (r.si + e * r.step) + (long)g.N1 * (r.sj + (long)g.N1 * r.sk);
-      sstride = g.S;
-    }
+    const double* src = u + (long)r.src_b * NV * g.S + (r.si + e * r.step) + (long)g.N1 * (r.sj + (long)g.N1 * r.sk);
     double* dst = work + (long)r.dst_b * NV * g.Wv + r.dst_w + e;
 #pragma unroll 4
-    for (int v = 0; v < NV; ++v) dst[v * g.Wv] = src[v * sstride];
+    for (int v = 0; v < NV; ++v) dst[v * g.Wv] = src[v * g.S];
   }
+}
+
+// The copies of the batched form's fill, one thread per point: every ghost point with a
+// primary owner, and every owned point held by a block that is not its primary, from the
+// primary's working array (whose owned points the stage update has just written). A
+// primary's own points are not listed: they already hold their value.
+__global__ void fill_points_kernel(const CopyPt* __restrict__ pts, long n, double* __restrict__ work, Geo g) {
+  const long id = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (id >= n) return;
+  const CopyPt c = pts[id];
+  const double* src = work + (long)c.src_b * NV * g.Wv + c.src_w;
+  double* dst = work + (long)c.dst_b * NV * g.Wv + c.dst_w;
+  double v[NV];
+#pragma unroll
+  for (int k = 0; k < NV; ++k) v[k] = src[k * g.Wv];
+#pragma unroll
+  for (int k = 0; k < NV; ++k) dst[k * g.Wv] = v[k];
 }
 
 // the Dirichlet hook: the analytic state (through the core rule) at each outer ghost point

@@ -43,6 +43,8 @@ struct tgh_problem {
   uint8_t* primary = nullptr; // per owned point: 1 where this block holds the primary copy
   CopyRun* runs = nullptr;
   int nruns = 0;
+  CopyPt* gpts = nullptr;  // the batched form's copies (no primary self-copies)
+  long ngpts = 0;
   HookPt* hooks = nullptr;
   int nhooks = 0;
   std::vector<ProlongPt*> prol;  // per level 1..maxlevel
@@ -193,6 +195,7 @@ static unsigned grid_for(long n, int threads) { return (unsigned)((n + threads -
 // The fill plan: for every point of every block's working array, where its value comes from.
 static int build_plan(tgh_problem* p) {
   std::vector<CopyRun> runs;
+  std::vector<CopyPt> gpts;
   std::vector<HookPt> hooks;
   std::vector<std::vector<ProlongPt>> prol(p->maxlevel + 1);
   std::vector<uint8_t> prim((size_t)p->npts, 0);
@@ -223,6 +226,8 @@ static int build_plan(tgh_problem* p) {
             const bool own = i >= G && i <= G + p->N && j >= G && j <= G + p->N && k >= G && k <= G + p->N;
             if (own && leaf == b) {
               prim[(size_t)b * p->S + (i - G) + (size_t)p->N1 * ((j - G) + (size_t)p->N1 * (k - G))] = 1;
+            } else {
+              gpts.push_back(CopyPt{b, w, leaf, (loc[0] + G) + Wd * ((loc[1] + G) + Wd * (loc[2] + G))});
             }
             if (open && cur.src_b == leaf && cur.step == step && cur.sj == loc[1] && cur.sk == loc[2] &&
                 cur.si + cur.len * step == loc[0] && cur.dst_w + cur.len == w) {
@@ -269,7 +274,10 @@ static int build_plan(tgh_problem* p) {
       }
   }
   p->nruns = (int)runs.size();
+  p->ngpts = (long)gpts.size();
   p->nhooks = (int)hooks.size();
+  CK(cudaMalloc(&p->gpts, std::max<size_t>(1, gpts.size()) * sizeof(CopyPt)));
+  if (!gpts.empty()) CK(cudaMemcpy(p->gpts, gpts.data(), gpts.size() * sizeof(CopyPt), cudaMemcpyHostToDevice));
   CK(cudaMalloc(&p->runs, std::max<size_t>(1, runs.size()) * sizeof(CopyRun)));
   CK(cudaMemcpy(p->runs, runs.data(), runs.size() * sizeof(CopyRun), cudaMemcpyHostToDevice));
   CK(cudaMalloc(&p->hooks, std::max<size_t>(1, hooks.size()) * sizeof(HookPt)));
@@ -309,9 +317,13 @@ static void prolong_weights(int P, double* w) {
 // ---- the fill: stage 0 (copies, hooks), then prolongation level by level ----
 static int launch_fill(tgh_problem* p, const double* src, bool from_work, double* work, double t) {
   const int T = 256;
-  if (p->nruns) {
-    fill_copy_kernel<<<grid_for((long)p->nruns * 32, T), T, 0, p->stream>>>(p->runs, p->nruns, src, work, p->geo,
-                                                                           from_work ? 1 : 0);
+  if (from_work) {
+    if (p->ngpts) {
+      fill_points_kernel<<<grid_for(p->ngpts, T), T, 0, p->stream>>>(p->gpts, p->ngpts, work, p->geo);
+      CK(cudaGetLastError());
+    }
+  } else if (p->nruns) {
+    fill_copy_kernel<<<grid_for((long)p->nruns * 32, T), T, 0, p->stream>>>(p->runs, p->nruns, src, work, p->geo);
     CK(cudaGetLastError());
   }
   if (p->nhooks) {
@@ -462,7 +474,7 @@ void tgh_problem_destroy(tgh_problem* p) {
   if (!p) return;
   if (p->gexec) cudaGraphExecDestroy(p->gexec);
   if (p->cap) cudaStreamDestroy(p->cap);
-  void* bufs[] = {p->work, p->Hsrc, p->blk, p->primary, p->runs, p->hooks, p->scratch, p->part, p->coef,
+  void* bufs[] = {p->work, p->Hsrc, p->blk, p->primary, p->runs, p->gpts, p->hooks, p->scratch, p->part, p->coef,
                   p->k, p->acc, p->y, p->u0, p->W1, p->W2, p->bacc};
   for (void* b : bufs)
     if (b) cudaFree(b);
