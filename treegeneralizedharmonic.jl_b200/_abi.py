@@ -78,6 +78,7 @@ EXTRA_SIGNATURES = {
     "tgh_time_rhs": (ctypes.c_int, [_VP, _VP, _D, ctypes.c_int, ctypes.c_int, ctypes.POINTER(_D)]),
     "tgh_copy_hsrc": (ctypes.c_int, [_VP, _VP]),
     "tgh_point_physics": (ctypes.c_int, [_VP, _D, ctypes.POINTER(_D), ctypes.POINTER(_D)]),
+    "tgh_last_launch_count": (ctypes.c_int, [_VP, ctypes.POINTER(ctypes.c_long)]),
 }
 
 _lib = None

@@ -59,6 +59,8 @@ struct tgh_problem {
   double *W1 = nullptr, *W2 = nullptr, *bacc = nullptr;
   cudaGraphExec_t gexec = nullptr;
   GraphKey gkey{0, 0, 0};
+  long graph_kernels = 0;  // kernel nodes of the captured graph
+  long last_launches = 0;  // kernels the last tgh_step_batched call ran
   const double* gu = nullptr;
 };
 
@@ -343,6 +345,15 @@ static int launch_fill(tgh_problem* p, const double* src, bool from_work, double
     CK(cudaGetLastError());
   }
   return TGH_OK;
+}
+
+// the kernel launches of one launch_fill call
+static long fill_launches(const tgh_problem* p, bool from_work) {
+  long n = from_work ? (p->ngpts ? 1 : 0) : (p->nruns ? 1 : 0);
+  if (p->nhooks) ++n;
+  for (int l = 1; l <= p->maxlevel; ++l)
+    if (p->nprol[l]) ++n;
+  return n;
 }
 
 static int launch_rhs(tgh_problem* p, const RhsArgs& a, int mode) {
@@ -645,6 +656,16 @@ int tgh_step_batched(tgh_problem* p, double* u, double t, double dt, int nsteps)
     p->stream = user;
     if (st) return st;
     CK(ee);
+    size_t nn = 0;
+    CK(cudaGraphGetNodes(graph, nullptr, &nn));
+    std::vector<cudaGraphNode_t> nodes(nn);
+    if (nn) CK(cudaGraphGetNodes(graph, nodes.data(), &nn));
+    p->graph_kernels = 0;
+    for (size_t i = 0; i < nn; ++i) {
+      cudaGraphNodeType ty;
+      CK(cudaGraphNodeGetType(nodes[i], &ty));
+      if (ty == cudaGraphNodeTypeKernel) ++p->graph_kernels;
+    }
     CK(cudaGraphInstantiate(&p->gexec, graph, 0));
     cudaGraphDestroy(graph);
     p->gkey = GraphKey{t, dt, nsteps};
@@ -652,6 +673,7 @@ int tgh_step_batched(tgh_problem* p, double* u, double t, double dt, int nsteps)
   CK(cudaGraphLaunch(p->gexec, p->stream));
   gather_kernel<<<grid_for(p->npts, 256), 256, 0, p->stream>>>(p->work, u, p->geo, p->npts);
   CK(cudaGetLastError());
+  p->last_launches = fill_launches(p, false) + p->graph_kernels + 1;
   return TGH_OK;
 }
 
@@ -695,6 +717,13 @@ int tgh_time_rhs(tgh_problem* p, const double* u, double t, int mode, int nlaunc
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
   *ms_per_launch = ms / nlaunch;
+  return TGH_OK;
+}
+
+// Benchmark aid: how many kernels the last tgh_step_batched call launched (the fill of u,
+// the captured graph's kernel nodes, the gather).
+int tgh_last_launch_count(tgh_problem* p, long* n) {
+  *n = p->last_launches;
   return TGH_OK;
 }
 

@@ -136,6 +136,13 @@ class GHProblem:
         self._check(self.lib.tgh_time_rhs(self._h, _ptr(u), float(t), int(mode), int(nlaunch), ctypes.byref(ms)))
         return ms.value
 
+    def last_launch_count(self):
+        """Kernels the last step_batched call launched: the fill of u, the captured graph's
+        kernel nodes and the gather."""
+        n = ctypes.c_long()
+        self._check(self.lib.tgh_last_launch_count(self._h, ctypes.byref(n)))
+        return n.value
+
     def gh_solve(self, u, tspan, dt, batched=False):
         """Integrate u from tspan[0] to tspan[1] with RK4 steps of at most dt, the last one
         shortened to land on tspan[1] (gh_solve, src/stepping.jl:235-239)."""
