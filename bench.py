@@ -5,7 +5,7 @@ One "step" is one classical RK4 step (four right-hand sides with Kreiss-Oliger d
 the ghost fill before each, the stage arithmetic) over the whole mesh of the workload. A
 point is an owned point counted N^3 per block, as the reference counts it.
 
-    python bench.py [--gpus N] [--steps K] [--warmup W] [--workload kerr_schild_static|fourier]
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--workload kerr_schild_static|fourier|hierarchy]
     python bench.py --impl reference ...   # the CPU restatement of the reference's path
 
 Workloads (seeded synthetic inputs, fully specified by their parameters):
@@ -14,6 +14,10 @@ Workloads (seeded synthetic inputs, fully specified by their parameters):
                       sampled gauge source, Gaussian damping, eps_KO = 1/2, q = 4, dt = h/(4 lambda)
   fourier             Minkowski + 8 Fourier modes (amplitude 1e-4) per component on the periodic
                       [-1,1]^3, 8 blocks of 32^3, q = 4, eps_KO = 1/2, gamma0 = 1, dt = h/4
+  hierarchy           the hole of kerr_schild_static boosted to v = 0.1 along x, on [-40,40]^3
+                      refined around its path in 5 levels to 2472 blocks of 32^3 (finest h =
+                      5/256), algebraic Kerr-Schild gauge source, moving :damped core; ~117 GB
+                      on the device, so the plain-form and host-buffer legs are left out
 """
 import argparse
 import ctypes
@@ -33,8 +37,9 @@ PKG = ROOT / "treegeneralizedharmonic.jl_b200"
 
 # Algorithmic FP64 operations of one right-hand-side point at q = 4 (adds + multiplies +
 # divides + square roots; an FMA is two), fixed by running the oracle's point right-hand side
-# with an op-counting scalar (orc_count_flops): no gauge source / sampled gauge source.
-FLOP_PER_POINT_RHS = {"none": 7909, "sampled": 7975}
+# with an op-counting scalar (orc_count_flops) at the centre of the first block of each
+# workload: no gauge source (fourier), sampled (kerr_schild_static), algebraic (hierarchy).
+FLOP_PER_POINT_RHS = {"none": 7909, "sampled": 7957, "algebraic": 8283}
 # RK4 stage arithmetic per point-update: 20 variables x (4 + 4 + 4 + 2) flops
 FLOP_PER_POINT_STAGES = 280
 
@@ -66,7 +71,28 @@ def workload(tgh, name):
         cfg = {"workload": "fourier_minkowski", "domain": "[-1,1]^3 periodic", "blocks": 8, "block": "32^3",
                "h": 1 / 32, "q": 4, "modes": 8, "amplitude": 1e-4, "eps_ko": 0.5, "gamma0": 1.0, "cfl": 0.25}
         return case, forest, case, forest, cfg, "none", True
+    if name == "hierarchy":
+        radii = [30.0, 16.0, 8.0, 4.5, 2.6]
+        case = tgh.kerr_schild_case(M=1.0, a=0.7, v=0.1, halfwidth=40.0, r0=0.8, r1=1.3, rho_max=4.0,
+                                    variant="damped", gauge="algebraic", eps_ko=0.5)
+        # the shells follow the centre over the 200-step run (t_end ~ 0.6, so 0.07 along x)
+        forest = tgh.hole_forest(case, 32, 4, radii, path=((0.0, 0.0, 0.0), (0.07, 0.0, 0.0)))
+        sample = tgh.kerr_schild_case(M=1.0, a=0.7, v=0.1, halfwidth=4.0, r0=0.8, r1=1.3, rho_max=4.0,
+                                      variant="damped", gauge="algebraic", eps_ko=0.5)
+        sample_forest = tgh.gh_forest(sample, 32, 2)
+        counts = [int(c) for c in __import__("numpy").bincount(forest.level)]
+        cfg = {"workload": "kerr_schild_hierarchy", "M": 1.0, "a": 0.7, "velocity": [0.1, 0.0, 0.0],
+               "domain": "[-40,40]^3", "blocks": forest.nblocks, "blocks_per_level": counts, "block": "32^3",
+               "h_min": forest.h0 / 2 ** int(forest.level.max()), "refinement_radii": radii, "q": 4,
+               "boundary": "dirichlet", "interior": "damped moving core r0=0.8 r1=1.3",
+               "gauge_source": "algebraic", "eps_ko": 0.5, "cfl": 0.25}
+        return case, forest, sample, sample_forest, cfg, "algebraic", False
     raise SystemExit(f"unknown workload {name}")
+
+
+def h_min(forest):
+    """The finest spacing of a forest: the time step is set by it (one dt for every level)."""
+    return forest.h0 / 2 ** int(forest.level.max())
 
 
 def initial(tgh, P, forest, perturbed):
@@ -109,9 +135,9 @@ class Clocks:
                 "reasons": reasons, "samples": len(sm)}
 
 
-def cpu_baseline(tgh, sample_case, sample_forest, perturbed, steps=1):
+def cpu_baseline(tgh, sample_case, sample_forest, perturbed, seconds=10.0, max_steps=40):
     """The oracle's RK4 step (the C++ restatement of the reference's CPU path) on a bounded
-    sample of the workload, with every host thread."""
+    sample of the workload, with every host thread: steps until about `seconds` of work."""
     sys.path.insert(0, str(ROOT / "tests"))
     import oracle_binding  # noqa: E402  (test infrastructure, loaded for the baseline only)
     orc = oracle_binding.Oracle.load()
@@ -121,11 +147,13 @@ def cpu_baseline(tgh, sample_case, sample_forest, perturbed, steps=1):
     if perturbed:
         u = u + tgh.perturbation(sample_forest, amplitude=1e-4)
     st, lam = O.max_speed(u, 0.0)
-    dt = 0.25 * sample_forest.h0 / lam
+    dt = 0.25 * h_min(sample_forest) / lam
     O.rk4_step(u, 0.0, dt)  # warm
     t0 = time.perf_counter()
-    for n in range(steps):
-        O.rk4_step(u, (n + 1) * dt, dt)
+    steps = 0
+    while steps < max_steps and (steps == 0 or time.perf_counter() - t0 < seconds):
+        O.rk4_step(u, (steps + 1) * dt, dt)
+        steps += 1
     el = time.perf_counter() - t0
     pts = sample_forest.points() * steps
     return {"value": pts / el, "unit": "point-updates/s", "cores": int(orc.lib.orc_get_threads()), "kind": "port",
@@ -148,7 +176,7 @@ def run_reference(args):
     if perturbed:
         u = u + tgh.perturbation(sforest, amplitude=1e-4)
     _, lam = O.max_speed(u, 0.0)
-    dt = 0.25 * sforest.h0 / lam
+    dt = 0.25 * h_min(sforest) / lam
     for n in range(args.warmup):
         O.rk4_step(u, n * dt, dt)
     t0 = time.perf_counter()
@@ -170,13 +198,40 @@ def run_reference(args):
     return 0
 
 
+def end_to_end(P, u0, dt, K, world, pts, stream, dist):
+    """The metric through the public API with host buffers: per step the state is copied in
+    from pinned host memory, stepped, and copied back, all inside the timed region."""
+    import torch
+    uh = u0.cpu().pin_memory()
+    res_h = torch.empty_like(uh).pin_memory()
+    P.step_batched(u0.clone(), 0.0, dt, 1)  # graph for one step
+    torch.cuda.synchronize()
+    ud = torch.empty_like(u0)
+    e2, e3 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e2.record(stream)
+    for _ in range(K):
+        ud.copy_(uh, non_blocking=True)
+        P.step_batched(ud, 0.0, dt, 1)
+        res_h.copy_(ud, non_blocking=True)
+    e3.record(stream)
+    torch.cuda.synchronize()
+    e2e_ms = e2.elapsed_time(e3)
+    if world > 1:
+        t = torch.tensor([e2e_ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_ms = float(t.item())
+    nbytes = uh.numel() * 8
+    return {"value": world * pts * K / (e2e_ms * 1e-3), "unit": "point-updates/s",
+            "h2d_bytes_per_step": nbytes, "d2h_bytes_per_step": nbytes}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=30)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="kerr_schild_static", choices=["kerr_schild_static", "fourier"])
+    ap.add_argument("--workload", default="kerr_schild_static", choices=["kerr_schild_static", "fourier", "hierarchy"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--rhs-only", action="store_true",
                     help="time only the right-hand side (head + Pi kernels, stage epilogue) on the workload: "
@@ -206,16 +261,18 @@ def main():
         P.close()
         return 0
     lam = P.max_speed(u0, 0.0)
-    dt = 0.25 * forest.h0 / lam
+    dt = 0.25 * h_min(forest) / lam
     K, W = args.steps, max(3, args.warmup)
 
-    # warm-up: W untimed K-step runs on copies (the first captures the graph)
-    for _ in range(W):
-        w = u0.clone()
-        P.step_batched(w, 0.0, dt, K)
-    torch.cuda.synchronize()
-
+    big = args.workload == "hierarchy"
+    # warm-up: at least W untimed steps, as K-step runs of the graph the timed run replays
+    # (the first run captures it), on one copy of the initial state
     u = u0.clone()
+    for _ in range(-(-W // K)):
+        u.copy_(u0)
+        P.step_batched(u, 0.0, dt, K)
+    torch.cuda.synchronize()
+    u.copy_(u0)
     clocks = Clocks(local)
     time.sleep(0.3)
     if world > 1:
@@ -240,6 +297,29 @@ def main():
     pts = forest.points()
     value = world * pts * K / (ms * 1e-3)
 
+    # the plain per-stage form on the same workload (fill of u, RHS into du, stage update; each
+    # launch issued from the host), for the batched form's speed-up
+    plain = {"skipped": "its three state-sized buffers do not fit beside the batched form's"}
+    if not big:
+        up = u0.clone()
+        P.rk4_step(up, 0.0, dt)
+        torch.cuda.synchronize()
+        Kp = max(3, K // 3)
+        e4, e5 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e4.record(stream)
+        for n in range(Kp):
+            P.rk4_step(up, n * dt, dt)
+        e5.record(stream)
+        torch.cuda.synchronize()
+        plain_ms = e4.elapsed_time(e5) / Kp
+        if world > 1:
+            t = torch.tensor([plain_ms], device="cuda")
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            plain_ms = float(t.item())
+        del up
+        plain = {"value": world * pts / (plain_ms * 1e-3), "unit": "point-updates/s", "ms_per_step": plain_ms,
+                 "steps": Kp, "form": "per stage: fill of u, RHS into du, stage update (host-issued launches)"}
+
     # the dominant kernel alone: the right-hand side with the fused RK4 epilogue
     rhs_ms = P.time_rhs(u0, 0.0, mode=1, nlaunch=max(4, K))
     n1pts = (forest.N + 1) ** 3 * forest.nblocks
@@ -256,25 +336,10 @@ def main():
 
     # end to end through the public API with host buffers: per step the state is copied in
     # from pinned host memory and the result copied back
-    uh = u0.cpu().pin_memory()
-    res_h = torch.empty_like(uh).pin_memory()
-    P.step_batched(u0.clone(), 0.0, dt, 1)  # graph for one step
-    torch.cuda.synchronize()
-    ud = torch.empty_like(u0)
-    e2, e3 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    e2.record(stream)
-    for _ in range(K):
-        ud.copy_(uh, non_blocking=True)
-        P.step_batched(ud, 0.0, dt, 1)
-        res_h.copy_(ud, non_blocking=True)
-    e3.record(stream)
-    torch.cuda.synchronize()
-    e2e_ms = e2.elapsed_time(e3)
-    if world > 1:
-        t = torch.tensor([e2e_ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_ms = float(t.item())
-    nbytes = uh.numel() * 8
+    if big:
+        e2e = {"skipped": "two pinned host copies of the 14 GB state", "unit": "point-updates/s"}
+    else:
+        e2e = end_to_end(P, u0, dt, K, world, pts, stream, dist)
 
     out = {"metric": "RK4 point-updates/s", "value": value, "unit": "point-updates/s", "n_gpus": world,
            "steps": K, "warmup": W, "ms_per_step": ms / K, "higher_is_better": True, "scaling": "weak",
@@ -288,8 +353,8 @@ def main():
                         "flop_per_point": FLOP_PER_POINT_RHS[gauge], "points_per_launch": n1pts,
                         "ms_per_launch": rhs_ms,
                         "peak_source": "measured FP64 FMA probe on this GPU (MEASURED_PEAKS.json has no FP64)"},
-           "e2e": {"value": world * pts * K / (e2e_ms * 1e-3), "unit": "point-updates/s",
-                   "h2d_bytes_per_step": nbytes, "d2h_bytes_per_step": nbytes},
+           "e2e": e2e,
+           "plain_form": plain,
            "gpu_launches": launches, "clocks": ck}
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         out["cpu_baseline"] = cpu_baseline(tgh, scase, sforest, perturbed)

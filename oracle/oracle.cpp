@@ -240,11 +240,7 @@ static void gauge_at_point(const Problem& P, int b, const int I[3], const T* h, 
     for (int a = 0; a < 4; ++a) Hl[a] = T(P.Hsrc[o + a * P.npt_state()]);
     for (int k = 0; k < 16; ++k) dHl[k % 4][k / 4] = T(P.Hsrc[o + (4 + k) * P.npt_state()]);
   } else {
-    if constexpr (std::is_same<T, double>::value) {
-      algebraic_gauge_source(P.ks, h, dth, dh, Hl, dHl);
-    } else {
-      throw std::runtime_error("op counting covers the none and sampled gauge sources");
-    }
+    algebraic_gauge_source<T>(P.ks, h, dth, dh, Hl, dHl);
   }
 }
 
@@ -910,6 +906,7 @@ static inline Cnt operator*(Cnt a, Cnt b) {
 static inline Cnt operator/(Cnt a, Cnt b) { ++Cnt::ndiv; return Cnt(a.v / b.v); }
 static inline bool operator!=(Cnt a, Cnt b) { return a.v != b.v; }
 static inline Cnt sqrt(Cnt a) { ++Cnt::nsqrt; return Cnt(std::sqrt(a.v)); }
+static inline double dval(Cnt a) { return a.v; }
 }  // namespace orc
 
 extern "C" {

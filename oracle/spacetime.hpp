@@ -269,44 +269,49 @@ static inline KSSource make_ks_source(double M, const double spin[3], const doub
   for (int i = 0; i < 3; ++i) k.u[i + 1] = gam * vel[i];
   return k;
 }
-// src/gauge.jl:302-326 (+ _algebraic_dH :330-336); dHl[c][a] = d_c H_a
-static inline void algebraic_gauge_source(const KSSource& src, const double* h, const double* dth,
-                                          const double* const dh[3], double Hl[4], double dHl[4][4]) {
-  double hm[4][4];
+// the value of a scalar for the branch conditions (an op-counting scalar overloads it)
+static inline double dval(double x) { return x; }
+
+// src/gauge.jl:302-326 (+ _algebraic_dH :330-336); dHl[c][a] = d_c H_a. Templated on the
+// scalar so the op-counting instantiation sees its arithmetic.
+template <class T>
+static inline void algebraic_gauge_source(const KSSource& src, const T* h, const T* dth, const T* const dh[3],
+                                          T Hl[4], T dHl[4][4]) {
+  using std::sqrt;
+  T hm[4][4];
   sym4(h, hm);
-  double w[4];
+  T w[4];
   for (int a = 0; a < 4; ++a) {
-    double s = hm[a][0] * src.u[0];
-    for (int b = 1; b < 4; ++b) s = s + hm[a][b] * src.u[b];
+    T s = hm[a][0] * T(src.u[0]);
+    for (int b = 1; b < 4; ++b) s = s + hm[a][b] * T(src.u[b]);
     w[a] = s;
   }
-  double K = src.u[0] * w[0];
-  for (int a = 1; a < 4; ++a) K = K + src.u[a] * w[a];
-  double sw = src.S[0] * w[0];
-  for (int a = 1; a < 4; ++a) sw = sw + src.S[a] * w[a];
-  double rad = src.M * src.M - sw * sw;
-  double root = rad > 0 ? std::sqrt(rad > 0 ? rad : 0.0) : 0.0;
-  double D = src.M + root;
+  T K = T(src.u[0]) * w[0];
+  for (int a = 1; a < 4; ++a) K = K + T(src.u[a]) * w[a];
+  T sw = T(src.S[0]) * w[0];
+  for (int a = 1; a < 4; ++a) sw = sw + T(src.S[a]) * w[a];
+  T rad = T(src.M) * T(src.M) - sw * sw;
+  T root = dval(rad) > 0 ? sqrt(rad) : T(0.0);
+  T D = T(src.M) + root;
   for (int a = 0; a < 4; ++a) Hl[a] = (-K / D) * w[a];
-  const double* Dp[4] = {dth, dh[0], dh[1], dh[2]};
-  double dw[4][4];
+  const T* Dp[4] = {dth, dh[0], dh[1], dh[2]};
+  T dw[4][4];
   for (int c = 0; c < 4; ++c) {
-    double dm[4][4];
+    T dm[4][4];
     sym4(Dp[c], dm);
     for (int a = 0; a < 4; ++a) {
-      double s = dm[a][0] * src.u[0];
-      for (int b = 1; b < 4; ++b) s = s + dm[a][b] * src.u[b];
+      T s = dm[a][0] * T(src.u[0]);
+      for (int b = 1; b < 4; ++b) s = s + dm[a][b] * T(src.u[b]);
       dw[c][a] = s;
     }
   }
   for (int c = 0; c < 4; ++c) {
-    double dK = src.u[0] * dw[c][0];
-    for (int a = 1; a < 4; ++a) dK = dK + src.u[a] * dw[c][a];
-    double Sdw = src.S[0] * dw[c][0];
-    for (int a = 1; a < 4; ++a) Sdw = Sdw + src.S[a] * dw[c][a];
-    double dD = root > 0 ? -sw * Sdw / root : 0.0;
-    for (int a = 0; a < 4; ++a)
-      dHl[c][a] = -(dK * w[a] + K * dw[c][a]) / D + K * w[a] * dD / (D * D);
+    T dK = T(src.u[0]) * dw[c][0];
+    for (int a = 1; a < 4; ++a) dK = dK + T(src.u[a]) * dw[c][a];
+    T Sdw = T(src.S[0]) * dw[c][0];
+    for (int a = 1; a < 4; ++a) Sdw = Sdw + T(src.S[a]) * dw[c][a];
+    T dD = dval(root) > 0 ? -sw * Sdw / root : T(0.0);
+    for (int a = 0; a < 4; ++a) dHl[c][a] = -(dK * w[a] + K * dw[c][a]) / D + K * w[a] * dD / (D * D);
   }
 }
 

@@ -39,7 +39,7 @@ def rhs_error(du_gpu, du_ref, scale, forest):
     return float(np.max(np.max(np.abs(a - b), axis=1) / scale))
 
 
-N_ROWS = 19
+N_ROWS = 20
 
 
 def cases(tgh):
@@ -72,6 +72,12 @@ def cases(tgh):
     rows.append(("kerr_schild_damped_n32", c, tgh.gh_forest(c, 32, 2), 4, 0.0))
     c = tgh.kerr_schild_case(M=1.0, a=0.7, halfwidth=4.0, r0=0.8, r1=1.3, gauge="algebraic")
     rows.append(("kerr_schild_algebraic_n32", c, tgh.gh_forest(c, 32, 2), 4, 0.0))
+    # a moving boosted hole on a four-level hierarchy of 8^3 blocks (levels 1-3 populated,
+    # prolongation at two interfaces): the hierarchy workload's physics at a size the
+    # oracle steps in seconds
+    c = tgh.kerr_schild_case(M=1.0, a=0.7, v=0.1, halfwidth=4.0, r0=0.8, r1=1.3, gauge="algebraic")
+    f = tgh.hole_forest(c, 8, 2, [3.0, 1.8, 1.4], path=((0.0, 0.0, 0.0), (0.05, 0.0, 0.0)))
+    rows.append(("kerr_schild_hierarchy_moving", c, f, 4, 0.3))
     assert len(rows) == N_ROWS
     return rows
 

@@ -572,8 +572,8 @@ int tgh_error_norm(tgh_problem* p, const double* u, double t, double* l2, double
 // plain form: per stage one fill, one right-hand-side launch, one stage update
 int tgh_rk4_step(tgh_problem* p, double* u, double t, double dt) {
   const size_t L = tgh_state_length(p);
-  if (!p->k) {
-    CK(cudaMalloc(&p->k, L * sizeof(double)));
+  if (!p->k) CK(cudaMalloc(&p->k, L * sizeof(double)));
+  if (!p->acc) {
     CK(cudaMalloc(&p->acc, L * sizeof(double)));
     CK(cudaMalloc(&p->y, L * sizeof(double)));
   }
@@ -682,11 +682,7 @@ int tgh_step_batched(tgh_problem* p, double* u, double t, double dt, int nsteps)
 // (du); mode 1: the batched form's kernel with the stage-2 epilogue. u is filled first.
 int tgh_time_rhs(tgh_problem* p, const double* u, double t, int mode, int nlaunch, double* ms_per_launch) {
   const size_t L = tgh_state_length(p), Lw = tgh_work_length(p);
-  if (!p->k) {
-    CK(cudaMalloc(&p->k, L * sizeof(double)));
-    CK(cudaMalloc(&p->acc, L * sizeof(double)));
-    CK(cudaMalloc(&p->y, L * sizeof(double)));
-  }
+  if (mode == 0 && !p->k) CK(cudaMalloc(&p->k, L * sizeof(double)));
   if (mode == 1 && !p->W1) {
     CK(cudaMalloc(&p->W1, Lw * sizeof(double)));
     CK(cudaMalloc(&p->W2, Lw * sizeof(double)));

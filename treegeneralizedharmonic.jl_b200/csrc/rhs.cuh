@@ -109,7 +109,8 @@ enum {
   CF_EH,                              // eps_KO / h
   CF_W,                               // the layer's w (1 outside; negative: the point is finished)
   CF_M0,                              // 10 additive terms: msrc (+ the layer's relaxation)
-  NCOEF = CF_M0 + NC
+  CF_DTH0 = CF_M0 + NC,               // batched form: the 10 d_t h values, updated by the Pi kernel
+  NCOEF = CF_DTH0 + NC
 };
 
 // one launch's geometry and buffers
@@ -151,6 +152,17 @@ struct EmitStage {
     } else {
       const double un = u0[v * sv];
       ac[v * S] = fma(cb, kv, stage == 1 ? un : ac[v * S]);
+      nx[v * sv] = fma(ca, kv, un);
+    }
+  }
+  // the same update in two halves, so that its loads can be issued before k is known
+  __device__ __forceinline__ double pre_u(int v) const { return stage == 4 ? 0.0 : u0[v * sv]; }
+  __device__ __forceinline__ double pre_a(int v) const { return stage == 1 ? 0.0 : ac[v * S]; }
+  __device__ __forceinline__ void fin(int v, double kv, double un, double a) {
+    if (stage == 4) {
+      nx[v * sv] = fma(cb, kv, a);
+    } else {
+      ac[v * S] = fma(cb, kv, stage == 1 ? un : a);
       nx[v * sv] = fma(ca, kv, un);
     }
   }
@@ -292,8 +304,9 @@ __device__ __forceinline__ void rhs_source(const Case& cs, const RhsArgs& A, int
   gh_source<T, true>(C, D, Hl, dHs, g0, T(cs.g2), msrc);
 }
 
-// The head kernel: d_t h at every owned point (emitted), the coefficients and additive
-// source of the Pi components (stored for the Pi kernel), and - with an interior - the
+// The head kernel: d_t h at every owned point (emitted in the plain form; in the batched
+// form left in the coefficients for the Pi kernel's stage update), the coefficients and
+// additive source of the Pi components (stored for the Pi kernel), and - with an interior - the
 // branches of gh_rhs_point! (src/evolution.jl:489-695): a frozen core is finished here and
 // never reaches a stencil; a layer point combines w F - rho (u - u_exact) (+ the moving
 // target's rate), the Pi half as w * (stencil part) + coef[CF_M0 + v].
@@ -313,6 +326,12 @@ __global__ void __launch_bounds__(128) rhs_head_kernel(const Case cs, const RhsA
   auto put = [&](int v, double val) {
     if (MODE == MODE_DU) ed.put(v, val);
     else es.put(v, val);
+  };
+  // d_t h of an evolved point: stored at once in the plain form; in the batched form parked in
+  // the coefficients, and the Pi kernel (more warps to cover the loads) does its stage update
+  auto put_dth = [&](int v, double val) {
+    if (MODE == MODE_DU) ed.put(v, val);
+    else cfo[(CF_DTH0 + v) * A.npts] = val;
   };
   double w = 1.0, rho = 0.0, r = 0.0;
   if (INT) {
@@ -364,16 +383,16 @@ __global__ void __launch_bounds__(128) rhs_head_kernel(const Case cs, const RhsA
   const bool follows = INT && core_follows(cs);
   if (!layer) {
 #pragma unroll
-    for (int v = 0; v < NC; ++v) put(v, dth[v]);
+    for (int v = 0; v < NC; ++v) put_dth(v, dth[v]);
   } else if (follows) {
     double hm[NC], Pm[NC], dthm[NC];
     background_state(cs, A.t, q.x, hm, Pm, dthm);
     const double om = 1.0 - w;
-    for (int v = 0; v < NC; ++v) put(v, w * dth[v] + om * dthm[v] - rho * (wk[v * sv] - hm[v]));
+    for (int v = 0; v < NC; ++v) put_dth(v, w * dth[v] + om * dthm[v] - rho * (wk[v * sv] - hm[v]));
   } else {
     double he[NC], Pe[NC];
     background_state(cs, A.t, q.x, he, Pe);
-    for (int v = 0; v < NC; ++v) put(v, w * dth[v] - rho * (wk[v * sv] - he[v]));
+    for (int v = 0; v < NC; ++v) put_dth(v, w * dth[v] - rho * (wk[v * sv] - he[v]));
   }
   // the Pi coefficients (and the matter term), then the source
   const double* dh[3] = {dh0, dh1, dh2};
@@ -442,6 +461,16 @@ __global__ void __launch_bounds__(128, 4) rhs_pi_kernel(const Case cs, const Rhs
   EmitStage es{A.acc + (long)q.b * NV * S + q.ip, A.next + q.wo, A.u0 + q.wo, S, sv, A.ca, A.cb, A.stage};
 #pragma unroll 1
   for (int v = 0; v < NC; ++v) {
+    // the epilogue's loads first: they are in flight while the stencils are formed
+    const double m = cfi[(CF_M0 + v) * A.npts];
+    double kh = 0.0, uh = 0.0, up = 0.0, ah = 0.0, ap = 0.0;
+    if (MODE == MODE_STAGE) {
+      kh = cfi[(CF_DTH0 + v) * A.npts];
+      uh = es.pre_u(v);
+      up = es.pre_u(NC + v);
+      ah = es.pre_a(v);
+      ap = es.pre_a(NC + v);
+    }
     const double* ph = wk + v * sv;
     const double* pp = ph + NC * sv;
     const T hc = ld<T>(ph), pc = ld<T>(pp);
@@ -460,10 +489,13 @@ __global__ void __launch_bounds__(128, 4) rhs_pi_kernel(const Case cs, const Rhs
     p2 = fma(Ayz, st_mixed<Q, T>(ph, s2, s3), p2);
     s = fma(ih2, p2, s);
     if (DISS) s = fma(eh, st_ko<Q, T>(pp, s1, pc) + st_ko<Q, T>(pp, s2, pc) + st_ko<Q, T>(pp, s3, pc), s);
-    const double m = cfi[(CF_M0 + v) * A.npts];
     const double val = w == 1.0 ? (double)s + m : fma(w, (double)s, m);
-    if (MODE == MODE_DU) ed.put(NC + v, val);
-    else es.put(NC + v, val);
+    if (MODE == MODE_DU) {
+      ed.put(NC + v, val);
+    } else {
+      es.fin(v, kh, uh, ah);
+      es.fin(NC + v, val, up, ap);
+    }
   }
 }
 
