@@ -356,15 +356,20 @@ static long fill_launches(const tgh_problem* p, bool from_work) {
   return n;
 }
 
-static int launch_rhs(tgh_problem* p, const RhsArgs& a, int mode) {
-  cudaError_t e;
+static cudaError_t launch_part(tgh_problem* p, int part, int mode, cudaStream_t s, const RhsArgs& a) {
   switch (p->q) {
-    case 2: e = launch_rhs_q2(p->diss, mode, p->intr, a.npts, p->stream, p->cs, a); break;
-    case 4: e = launch_rhs_q4(p->diss, mode, p->intr, a.npts, p->stream, p->cs, a); break;
-    case 6: e = launch_rhs_q6(p->diss, mode, p->intr, a.npts, p->stream, p->cs, a); break;
-    default: e = launch_rhs_q8(p->diss, mode, p->intr, a.npts, p->stream, p->cs, a); break;
+    case 2: return launch_rhs_q2(part, p->diss, mode, p->intr, s, p->cs, a);
+    case 4: return launch_rhs_q4(part, p->diss, mode, p->intr, s, p->cs, a);
+    case 6: return launch_rhs_q6(part, p->diss, mode, p->intr, s, p->cs, a);
+    default: return launch_rhs_q8(part, p->diss, mode, p->intr, s, p->cs, a);
   }
-  CK(e);
+}
+
+// One right-hand side: the head kernel, then the Pi kernel, over all blocks on the problem's
+// stream.
+static int launch_rhs(tgh_problem* p, const RhsArgs& a, int mode) {
+  CK(launch_part(p, 0, mode, p->stream, a));
+  CK(launch_part(p, 1, mode, p->stream, a));
   return TGH_OK;
 }
 
@@ -379,6 +384,8 @@ static RhsArgs base_args(tgh_problem* p, const double* work, double t) {
   a.Wd = p->Wd;
   a.G = p->G;
   a.npts = p->npts;
+  a.p0 = 0;
+  a.p1 = p->npts;
   a.t = t;
   return a;
 }

@@ -129,6 +129,7 @@ struct RhsArgs {
   int stage;              // 1..4
   int N1, Wd, G;
   long npts;              // N1^3 * nblocks
+  long p0, p1;            // the points [p0, p1) this launch covers (whole blocks)
   double t;
 };
 
@@ -313,8 +314,8 @@ __device__ __forceinline__ void rhs_source(const Case& cs, const RhsArgs& A, int
 template <int Q, bool DISS, int MODE, bool INT, int N1S>
 __global__ void __launch_bounds__(128) rhs_head_kernel(const Case cs, const RhsArgs A0) {
   const RhsArgs A = fixed_geometry<Q, N1S>(A0);
-  const long p = (long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (p >= A.npts) return;
+  const long p = A.p0 + (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= A.p1) return;
   const PointIdx q = point_index(A, p);
   const long S = (long)A.N1 * A.N1 * A.N1;
   const long sv = (long)A.Wd * A.Wd * A.Wd;
@@ -439,8 +440,8 @@ __global__ void __launch_bounds__(128) rhs_head_kernel(const Case cs, const RhsA
 template <int Q, bool DISS, int MODE, class T, int N1S>
 __global__ void __launch_bounds__(128, 4) rhs_pi_kernel(const Case cs, const RhsArgs A0) {
   const RhsArgs A = fixed_geometry<Q, N1S>(A0);
-  const long p = (long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (p >= A.npts) return;
+  const long p = A.p0 + (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= A.p1) return;
   const double* cfi = A.coef + p;
   const double w = cfi[CF_W * A.npts];
   if (w < 0.0) return;

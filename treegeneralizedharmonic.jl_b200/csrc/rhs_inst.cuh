@@ -6,36 +6,38 @@
 #include "rhs.cuh"
 
 namespace tgh {
-cudaError_t launch_rhs_q2(bool diss, int mode, bool intr, long npts, cudaStream_t s, const Case& cs, const RhsArgs& a);
-cudaError_t launch_rhs_q4(bool diss, int mode, bool intr, long npts, cudaStream_t s, const Case& cs, const RhsArgs& a);
-cudaError_t launch_rhs_q6(bool diss, int mode, bool intr, long npts, cudaStream_t s, const Case& cs, const RhsArgs& a);
-cudaError_t launch_rhs_q8(bool diss, int mode, bool intr, long npts, cudaStream_t s, const Case& cs, const RhsArgs& a);
+// part 0: the head kernel, part 1: the Pi kernel, over the points [a.p0, a.p1)
+cudaError_t launch_rhs_q2(int part, bool diss, int mode, bool intr, cudaStream_t s, const Case& cs, const RhsArgs& a);
+cudaError_t launch_rhs_q4(int part, bool diss, int mode, bool intr, cudaStream_t s, const Case& cs, const RhsArgs& a);
+cudaError_t launch_rhs_q6(int part, bool diss, int mode, bool intr, cudaStream_t s, const Case& cs, const RhsArgs& a);
+cudaError_t launch_rhs_q8(int part, bool diss, int mode, bool intr, cudaStream_t s, const Case& cs, const RhsArgs& a);
 
 template <int Q, bool DISS, int MODE, int N1S>
-cudaError_t launch_rhs_n(bool intr, long npts, cudaStream_t s, const Case& cs, const RhsArgs& a) {
+cudaError_t launch_rhs_n(int part, bool intr, cudaStream_t s, const Case& cs, const RhsArgs& a) {
   const int T = 128;
-  const unsigned nb = (unsigned)((npts + T - 1) / T);
-  if (intr) rhs_head_kernel<Q, DISS, MODE, true, N1S><<<nb, T, 0, s>>>(cs, a);
-  else rhs_head_kernel<Q, DISS, MODE, false, N1S><<<nb, T, 0, s>>>(cs, a);
-  cudaError_t e = cudaGetLastError();
-  if (e != cudaSuccess) return e;
-  rhs_pi_kernel<Q, DISS, MODE, double, N1S><<<nb, T, 0, s>>>(cs, a);
+  const unsigned nb = (unsigned)((a.p1 - a.p0 + T - 1) / T);
+  if (part == 0) {
+    if (intr) rhs_head_kernel<Q, DISS, MODE, true, N1S><<<nb, T, 0, s>>>(cs, a);
+    else rhs_head_kernel<Q, DISS, MODE, false, N1S><<<nb, T, 0, s>>>(cs, a);
+  } else {
+    rhs_pi_kernel<Q, DISS, MODE, double, N1S><<<nb, T, 0, s>>>(cs, a);
+  }
   return cudaGetLastError();
 }
 
 // blocks of N = 32 cells run the kernels compiled for that size, others the general ones
 template <int Q, bool DISS, int MODE>
-cudaError_t launch_rhs_t(bool intr, long npts, cudaStream_t s, const Case& cs, const RhsArgs& a) {
-  if (a.N1 == 33) return launch_rhs_n<Q, DISS, MODE, 33>(intr, npts, s, cs, a);
-  return launch_rhs_n<Q, DISS, MODE, 0>(intr, npts, s, cs, a);
+cudaError_t launch_rhs_t(int part, bool intr, cudaStream_t s, const Case& cs, const RhsArgs& a) {
+  if (a.N1 == 33) return launch_rhs_n<Q, DISS, MODE, 33>(part, intr, s, cs, a);
+  return launch_rhs_n<Q, DISS, MODE, 0>(part, intr, s, cs, a);
 }
 
-#define TGH_DEFINE_RHS_LAUNCH(QQ)                                                                     \
-  cudaError_t launch_rhs_q##QQ(bool diss, int mode, bool intr, long npts, cudaStream_t s, const Case& cs, \
-                               const RhsArgs& a) {                                                   \
-    if (diss) return mode == MODE_DU ? launch_rhs_t<QQ, true, MODE_DU>(intr, npts, s, cs, a)          \
-                                     : launch_rhs_t<QQ, true, MODE_STAGE>(intr, npts, s, cs, a);      \
-    return mode == MODE_DU ? launch_rhs_t<QQ, false, MODE_DU>(intr, npts, s, cs, a)                   \
-                           : launch_rhs_t<QQ, false, MODE_STAGE>(intr, npts, s, cs, a);               \
+#define TGH_DEFINE_RHS_LAUNCH(QQ)                                                                        \
+  cudaError_t launch_rhs_q##QQ(int part, bool diss, int mode, bool intr, cudaStream_t s, const Case& cs, \
+                               const RhsArgs& a) {                                                      \
+    if (diss) return mode == MODE_DU ? launch_rhs_t<QQ, true, MODE_DU>(part, intr, s, cs, a)             \
+                                     : launch_rhs_t<QQ, true, MODE_STAGE>(part, intr, s, cs, a);         \
+    return mode == MODE_DU ? launch_rhs_t<QQ, false, MODE_DU>(part, intr, s, cs, a)                      \
+                           : launch_rhs_t<QQ, false, MODE_STAGE>(part, intr, s, cs, a);                  \
   }
 }  // namespace tgh
