@@ -134,7 +134,8 @@ void tgh_problem_destroy(tgh_problem* p);
 const char* tgh_last_error(const tgh_problem* p);
 /* doubles in one state vector: (N+1)^3 * 20 * nblocks */
 size_t tgh_state_length(const tgh_problem* p);
-/* doubles in the ghosted working array: (N+2G+1)^3 * 20 * nblocks */
+/* doubles in the ghosted working array: (N+2G+1)^3 * 20 * blocks held (a rank of a sharded
+ * problem holds its own leaves and its halo) */
 size_t tgh_work_length(const tgh_problem* p);
 /* copy the working array (device to device) for inspection */
 int tgh_copy_work(tgh_problem* p, double* dst);
@@ -178,6 +179,44 @@ int tgh_error_norm(tgh_problem* p, const double* u, double t, double* l2, double
 #define TGH_NOALLOC_MAX_BLOCKS 8192
 int tgh_max_speed_noalloc(const tgh_config* cfg, const tgh_mesh* mesh, const double* u, double t,
                           void* cuda_stream, double* lambda, char* errbuf, int errlen);
+
+/* --- one rank per GPU (TreeAMR's distribution of a forest's blocks over the ranks of a
+ * communicator, src/distributed.jl:1-22; the forest itself is on every rank) ---
+ * tgh_partition: the owner rank of every leaf: per refinement level, the level's leaves in
+ * Morton order of their block coordinates cut into nranks runs of nearly equal length. Host
+ * only.
+ * tgh_problem_create_shard: the problem of `rank`'s leaves (owner[b] == rank) over the whole
+ * forest `mesh`; its state vectors hold its own leaves in forest order. Its working arrays
+ * also hold halo blocks: the other ranks' leaves its ghost fill reads.
+ * The batched step is then driven by the caller, which owns the transport between ranks:
+ *   tgh_shard_begin(u)
+ *   per step, per stage s = 0..3:
+ *     per phase f = 0 .. tgh_shard_phases() - 1:        (0: copies and Dirichlet ghosts;
+ *       tgh_shard_pack(s, f, send)                        f >= 1: level f's prolongation)
+ *       exchange: send holds, peer after peer, send_count[r] points of 20 doubles for rank r;
+ *                 recv receives recv_count[r] points from rank r likewise (tgh_shard_counts)
+ *       tgh_shard_unpack(s, f, recv); tgh_shard_fill(s, f, t, dt)
+ *     tgh_shard_rhs(s, t, dt)
+ *   tgh_shard_end(u)
+ * Every call is ordered on the problem's stream; send and recv are device buffers. With one
+ * rank the sequence is the batched step without its graph. The plain form's verbs refuse a
+ * problem of more than one rank. */
+int tgh_partition(const tgh_mesh* mesh, int nranks, int* owner);
+/* host-only view of rank's exchange in one fill phase: per peer the point counts and, when the
+ * arrays are given (2 ints per point), the (forest leaf, work index) pairs sent and received,
+ * peer-major; the lists tgh_problem_create_shard builds. errbuf (nullable) receives a failure. */
+int tgh_shard_plan(const tgh_config* cfg, const tgh_mesh* mesh, const int* owner, int rank, int nranks, int phase,
+                   long* send_count, long* recv_count, int* send_pts, int* recv_pts, char* errbuf, int errlen);
+int tgh_problem_create_shard(const tgh_config* cfg, const tgh_mesh* mesh, const int* owner, int rank, int nranks,
+                             void* cuda_stream, int margin_check, tgh_problem** out);
+int tgh_shard_phases(const tgh_problem* p);
+int tgh_shard_counts(tgh_problem* p, int phase, long* send_count, long* recv_count);
+int tgh_shard_begin(tgh_problem* p, const double* u);
+int tgh_shard_pack(tgh_problem* p, int stage, int phase, double* send);
+int tgh_shard_unpack(tgh_problem* p, int stage, int phase, const double* recv);
+int tgh_shard_fill(tgh_problem* p, int stage, int phase, double t, double dt);
+int tgh_shard_rhs(tgh_problem* p, int stage, double t, double dt);
+int tgh_shard_end(tgh_problem* p, double* u);
 
 #ifdef __cplusplus
 }

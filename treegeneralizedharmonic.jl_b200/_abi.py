@@ -72,6 +72,19 @@ SIGNATURES = {
     "tgh_error_norm": (ctypes.c_int, [_VP, _VP, _D, ctypes.POINTER(_D), ctypes.POINTER(_D)]),
     "tgh_max_speed_noalloc": (ctypes.c_int, [ctypes.POINTER(Config), ctypes.POINTER(Mesh), _VP, _D, _VP,
                                              ctypes.POINTER(_D), ctypes.c_char_p, ctypes.c_int]),
+    "tgh_partition": (ctypes.c_int, [ctypes.POINTER(Mesh), ctypes.c_int, _VP]),
+    "tgh_shard_plan": (ctypes.c_int, [ctypes.POINTER(Config), ctypes.POINTER(Mesh), _VP, ctypes.c_int, ctypes.c_int,
+                                      ctypes.c_int, _VP, _VP, _VP, _VP, ctypes.c_char_p, ctypes.c_int]),
+    "tgh_problem_create_shard": (ctypes.c_int, [ctypes.POINTER(Config), ctypes.POINTER(Mesh), _VP, ctypes.c_int,
+                                                ctypes.c_int, _VP, ctypes.c_int, ctypes.POINTER(_VP)]),
+    "tgh_shard_phases": (ctypes.c_int, [_VP]),
+    "tgh_shard_counts": (ctypes.c_int, [_VP, ctypes.c_int, _VP, _VP]),
+    "tgh_shard_begin": (ctypes.c_int, [_VP, _VP]),
+    "tgh_shard_pack": (ctypes.c_int, [_VP, ctypes.c_int, ctypes.c_int, _VP]),
+    "tgh_shard_unpack": (ctypes.c_int, [_VP, ctypes.c_int, ctypes.c_int, _VP]),
+    "tgh_shard_fill": (ctypes.c_int, [_VP, ctypes.c_int, ctypes.c_int, _D, _D]),
+    "tgh_shard_rhs": (ctypes.c_int, [_VP, ctypes.c_int, _D, _D]),
+    "tgh_shard_end": (ctypes.c_int, [_VP, _VP]),
 }
 EXTRA_SIGNATURES = {
     "tgh_fp64_probe": (ctypes.c_double, [_VP, ctypes.c_int]),

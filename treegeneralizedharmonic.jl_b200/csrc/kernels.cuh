@@ -309,6 +309,37 @@ __global__ void gather_kernel(const double* __restrict__ work, double* __restric
   for (int v = 0; v < NV; ++v) o[v * g.S] = q[v * g.Wv];
 }
 
+// the owned points of the first npts / S blocks of a working array from the state vector u
+__global__ void scatter_owned_kernel(const double* __restrict__ u, double* __restrict__ work, Geo g, long npts) {
+  const long p = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= npts) return;
+  const int b = (int)(p / g.S);
+  const long ip = p - (long)b * g.S;
+  const int k = (int)(ip / ((long)g.N1 * g.N1)), j = (int)((ip / g.N1) % g.N1), i = (int)(ip % g.N1);
+  double* q = work + (long)b * NV * g.Wv + (i + g.G) + (long)g.Wd * ((j + g.G) + (long)g.Wd * (k + g.G));
+  const double* s = u + (long)b * NV * g.S + ip;
+#pragma unroll
+  for (int v = 0; v < NV; ++v) q[v * g.Wv] = s[v * g.S];
+}
+
+// The exchange of a sharded fill: the listed (block, work index) points of a working array
+// packed into, or unpacked from, a buffer of 20 values per point (point-major), one thread per
+// value.
+__global__ void pack_kernel(const HookPt* __restrict__ pts, long n, const double* __restrict__ work, Geo g,
+                            double* __restrict__ buf) {
+  const long id = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (id >= n * NV) return;
+  const HookPt pt = pts[id / NV];
+  buf[id] = work[(long)pt.b * NV * g.Wv + (id % NV) * g.Wv + pt.w];
+}
+__global__ void unpack_kernel(const HookPt* __restrict__ pts, long n, const double* __restrict__ buf,
+                              double* __restrict__ work, Geo g) {
+  const long id = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (id >= n * NV) return;
+  const HookPt pt = pts[id / NV];
+  work[(long)pt.b * NV * g.Wv + (id % NV) * g.Wv + pt.w] = buf[id];
+}
+
 // one point's analytic state (20) and gauge tuple (20), for diagnostics
 __global__ void point_physics_kernel(const Case cs, double t, const double* x, double* out) {
   exact_state(cs, t, x, out);

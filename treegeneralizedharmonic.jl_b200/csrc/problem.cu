@@ -8,6 +8,7 @@
 #include <cstdint>
 #include <cstring>
 #include <string>
+#include <map>
 #include <unordered_map>
 #include <vector>
 
@@ -22,12 +23,27 @@ struct GraphKey {
   int nsteps;
 };
 
+// One rank's share of the exchange of a fill phase: per peer, the (internal block, work index)
+// points packed for it (send) or unpacked from it into halo blocks (recv), peer-major.
+struct ExchangeList {
+  std::vector<long> send_count, recv_count;  // per peer rank
+  HookPt* send = nullptr;                    // device, sum(send_count) entries
+  HookPt* recv = nullptr;
+  long nsend = 0, nrecv = 0;
+};
+
 struct tgh_problem {
   tgh_config cfg;
-  int q, G, N, N1, Wd, nb, maxlevel = 0;
+  // nb: the blocks this rank computes (its own leaves); nwb: the working arrays' blocks, its
+  // own leaves first, then the halo: other ranks' leaves its fill reads
+  int q, G, N, N1, Wd, nb, nwb, maxlevel = 0;
   double lo[3], h0;
   int cells0[3], periodic[3];
-  std::vector<int> level, corner;
+  std::vector<int> level, corner;  // of every leaf of the forest (global numbering)
+  int rank = 0, nranks = 1;
+  std::vector<int> owner;          // per global leaf: the rank that computes it
+  std::vector<int> g2i, i2g;       // global leaf <-> internal block (-1: not held)
+  std::vector<ExchangeList> xch;   // per fill phase: 0 the copies, l >= 1 level l's prolongation
   std::vector<std::unordered_map<int64_t, int>> lut;
   Geo geo;
   long S, Wv, npts;
@@ -194,23 +210,60 @@ static Case make_case(const tgh_config& c) {
 
 static unsigned grid_for(long n, int threads) { return (unsigned)((n + threads - 1) / threads); }
 
-// The fill plan: for every point of every block's working array, where its value comes from.
-static int build_plan(tgh_problem* p) {
-  std::vector<CopyRun> runs;
+// The fill plan of one rank: where every point of its blocks' working arrays comes from, in the
+// rank's internal block numbering (its own leaves in forest order, then the halo: the other
+// ranks' leaves its fill reads, numbered as first met), and which points of other ranks'
+// leaves it must receive before each fill phase (phase 0: the copies' sources, owned points;
+// phase l >= 1: the coarse stencil boxes of level l's prolongation, read after the owner's
+// level l - 1 is filled). With one rank everything is local and the numbering is the forest's.
+struct HostPlan {
+  std::vector<int> g2i, i2g;
+  int nloc = 0;
+  std::vector<CopyRun> runs;  // the plain form's scatter (one rank only)
   std::vector<CopyPt> gpts;
   std::vector<HookPt> hooks;
-  std::vector<std::vector<ProlongPt>> prol(p->maxlevel + 1);
-  std::vector<uint8_t> prim((size_t)p->npts, 0);
+  std::vector<std::vector<ProlongPt>> prol;
+  std::vector<uint8_t> prim;
+  // (owner rank, phase) -> sorted distinct (global leaf, work index) read from that owner
+  std::map<std::pair<int, int>, std::vector<std::pair<int, int>>> req;
+};
+
+static bool plan_rank(const tgh_problem* p, int r, bool entries, HostPlan& hp, std::string& err) {
+  const int nleaf = (int)p->owner.size();
+  hp.g2i.assign(nleaf, -1);
+  hp.i2g.clear();
+  for (int g = 0; g < nleaf; ++g)
+    if (p->owner[g] == r) {
+      hp.g2i[g] = (int)hp.i2g.size();
+      hp.i2g.push_back(g);
+    }
+  hp.nloc = (int)hp.i2g.size();
+  auto intern = [&](int g) {
+    if (hp.g2i[g] < 0) {
+      hp.g2i[g] = (int)hp.i2g.size();
+      hp.i2g.push_back(g);
+    }
+    return hp.g2i[g];
+  };
+  auto& runs = hp.runs;
+  auto& gpts = hp.gpts;
+  auto& hooks = hp.hooks;
+  auto& prol = hp.prol;
+  auto& prim = hp.prim;
+  prol.assign(p->maxlevel + 1, {});
+  if (entries) prim.assign((size_t)hp.nloc * p->S, 0);
+  const bool one = p->nranks == 1;
   const int Wd = p->Wd, G = p->G, P = p->q + 2;
-  for (int b = 0; b < p->nb; ++b) {
-    const int l = p->level[b];
+  for (int b = 0; b < hp.nloc; ++b) {
+    const int gb = hp.i2g[b];
+    const int l = p->level[gb];
     for (int k = 0; k < Wd; ++k)
       for (int j = 0; j < Wd; ++j) {
         CopyRun cur{};
         bool open = false;
         for (int i = 0; i < Wd; ++i) {
-          int64_t n[3] = {(int64_t)p->corner[3 * b] + i - G, (int64_t)p->corner[3 * b + 1] + j - G,
-                          (int64_t)p->corner[3 * b + 2] + k - G};
+          int64_t n[3] = {(int64_t)p->corner[3 * gb] + i - G, (int64_t)p->corner[3 * gb + 1] + j - G,
+                          (int64_t)p->corner[3 * gb + 2] + k - G};
           bool outside = false;
           for (int d = 0; d < 3; ++d) {
             const int64_t per = (int64_t)p->cells0[d] << l;
@@ -226,18 +279,22 @@ static int build_plan(tgh_problem* p) {
           if (!outside && find_owner(p, l, n, leaf, loc, lev)) {
             const int step = 1 << (lev - l);
             const bool own = i >= G && i <= G + p->N && j >= G && j <= G + p->N && k >= G && k <= G + p->N;
-            if (own && leaf == b) {
-              prim[(size_t)b * p->S + (i - G) + (size_t)p->N1 * ((j - G) + (size_t)p->N1 * (k - G))] = 1;
+            const int sw = (loc[0] + G) + Wd * ((loc[1] + G) + Wd * (loc[2] + G));
+            if (own && leaf == gb) {
+              if (entries) prim[(size_t)b * p->S + (i - G) + (size_t)p->N1 * ((j - G) + (size_t)p->N1 * (k - G))] = 1;
             } else {
-              gpts.push_back(CopyPt{b, w, leaf, (loc[0] + G) + Wd * ((loc[1] + G) + Wd * (loc[2] + G))});
+              if (p->owner[leaf] != r) hp.req[{p->owner[leaf], 0}].push_back({leaf, sw});
+              if (entries) gpts.push_back(CopyPt{b, w, intern(leaf), sw});
             }
-            if (open && cur.src_b == leaf && cur.step == step && cur.sj == loc[1] && cur.sk == loc[2] &&
-                cur.si + cur.len * step == loc[0] && cur.dst_w + cur.len == w) {
-              cur.len++;
-            } else {
-              if (open) runs.push_back(cur);
-              cur = CopyRun{b, w, leaf, loc[0], loc[1], loc[2], 1, step};
-              open = true;
+            if (entries && one) {
+              if (open && cur.src_b == leaf && cur.step == step && cur.sj == loc[1] && cur.sk == loc[2] &&
+                  cur.si + cur.len * step == loc[0] && cur.dst_w + cur.len == w) {
+                cur.len++;
+              } else {
+                if (open) runs.push_back(cur);
+                cur = CopyRun{b, w, leaf, loc[0], loc[1], loc[2], 1, step};
+                open = true;
+              }
             }
             continue;
           }
@@ -246,16 +303,20 @@ static int build_plan(tgh_problem* p) {
             open = false;
           }
           if (outside) {
-            hooks.push_back(HookPt{b, w});
+            if (entries) hooks.push_back(HookPt{b, w});
             continue;
           }
-          if (l == 0) return fail(p, TGH_ERR_ARG, "a lattice point is covered by no leaf of the forest");
+          if (l == 0) {
+            err = "a lattice point is covered by no leaf of the forest";
+            return false;
+          }
           const int c = coarse_cover(p, l - 1, n);
-          if (c < 0)
-            return fail(p, TGH_ERR_ARG,
-                        "a prolonged ghost point has no covering leaf one level coarser (the forest is not 2:1 balanced)");
+          if (c < 0) {
+            err = "a prolonged ghost point has no covering leaf one level coarser (the forest is not 2:1 balanced)";
+            return false;
+          }
           int odd = 0;
-          int64_t base[3];
+          int64_t base[3], ext[3];
           for (int d = 0; d < 3; ++d) {
             if (n[d] & 1) {
               odd |= 1 << d;
@@ -264,16 +325,77 @@ static int build_plan(tgh_problem* p) {
               base[d] = n[d] >> 1;
             }
             const int64_t rel = base[d] - p->corner[3 * c + d] + G;
-            const int64_t ext = (n[d] & 1) ? P : 1;
-            if (rel < 0 || rel + ext > Wd)
-              return fail(p, TGH_ERR_ARG, "a prolongation stencil leaves the coarse block's ghost zone");
+            ext[d] = (n[d] & 1) ? P : 1;
+            if (rel < 0 || rel + ext[d] > Wd) {
+              err = "a prolongation stencil leaves the coarse block's ghost zone";
+              return false;
+            }
           }
           const int sw = (int)((base[0] - p->corner[3 * c] + G) +
                                Wd * ((base[1] - p->corner[3 * c + 1] + G) + (int64_t)Wd * (base[2] - p->corner[3 * c + 2] + G)));
-          prol[l].push_back(ProlongPt{b, w, c, sw, odd});
+          if (p->owner[c] != r) {
+            auto& v = hp.req[{p->owner[c], l}];
+            for (int64_t kz = 0; kz < ext[2]; ++kz)
+              for (int64_t ky = 0; ky < ext[1]; ++ky)
+                for (int64_t kx = 0; kx < ext[0]; ++kx) v.push_back({c, (int)(sw + kx + Wd * (ky + Wd * kz))});
+          }
+          if (entries) prol[l].push_back(ProlongPt{b, w, intern(c), sw, odd});
         }
         if (open) runs.push_back(cur);
       }
+  }
+  for (auto& kv : hp.req) {
+    std::sort(kv.second.begin(), kv.second.end());
+    kv.second.erase(std::unique(kv.second.begin(), kv.second.end()), kv.second.end());
+  }
+  return true;
+}
+
+// The plan of this problem's rank on the device, with the exchange lists: what this rank
+// receives into its halo (its own requests) and what it sends (every other rank's requests
+// to it, found by planning that rank's leaves: both sides derive the same sorted list).
+static int build_plan(tgh_problem* p) {
+  HostPlan hp;
+  std::string err;
+  if (!plan_rank(p, p->rank, true, hp, err)) return fail(p, TGH_ERR_ARG, err);
+  p->g2i = hp.g2i;
+  p->i2g = hp.i2g;
+  p->nwb = (int)hp.i2g.size();
+  const auto& runs = hp.runs;
+  const auto& gpts = hp.gpts;
+  const auto& hooks = hp.hooks;
+  const auto& prol = hp.prol;
+  const auto& prim = hp.prim;
+  const int nph = p->maxlevel + 1;
+  p->xch.assign(nph, ExchangeList{});
+  std::vector<std::vector<HookPt>> snd(nph), rcv(nph);
+  for (int ph = 0; ph < nph; ++ph) {
+    p->xch[ph].send_count.assign(p->nranks, 0);
+    p->xch[ph].recv_count.assign(p->nranks, 0);
+  }
+  for (int o = 0; o < p->nranks; ++o) {
+    if (o == p->rank) continue;
+    HostPlan hq;
+    if (!plan_rank(p, o, false, hq, err)) return fail(p, TGH_ERR_ARG, err);
+    for (int ph = 0; ph < nph; ++ph) {
+      auto mine = hp.req.find({o, ph});
+      if (mine != hp.req.end())
+        for (const auto& e : mine->second) rcv[ph].push_back(HookPt{p->g2i[e.first], e.second});
+      p->xch[ph].recv_count[o] = mine == hp.req.end() ? 0 : (long)mine->second.size();
+      auto theirs = hq.req.find({p->rank, ph});
+      if (theirs != hq.req.end())
+        for (const auto& e : theirs->second) snd[ph].push_back(HookPt{p->g2i[e.first], e.second});
+      p->xch[ph].send_count[o] = theirs == hq.req.end() ? 0 : (long)theirs->second.size();
+    }
+  }
+  for (int ph = 0; ph < nph; ++ph) {
+    ExchangeList& x = p->xch[ph];
+    x.nsend = (long)snd[ph].size();
+    x.nrecv = (long)rcv[ph].size();
+    CK(cudaMalloc(&x.send, std::max<size_t>(1, snd[ph].size()) * sizeof(HookPt)));
+    CK(cudaMalloc(&x.recv, std::max<size_t>(1, rcv[ph].size()) * sizeof(HookPt)));
+    if (x.nsend) CK(cudaMemcpy(x.send, snd[ph].data(), snd[ph].size() * sizeof(HookPt), cudaMemcpyHostToDevice));
+    if (x.nrecv) CK(cudaMemcpy(x.recv, rcv[ph].data(), rcv[ph].size() * sizeof(HookPt), cudaMemcpyHostToDevice));
   }
   p->nruns = (int)runs.size();
   p->ngpts = (long)gpts.size();
@@ -319,6 +441,8 @@ static void prolong_weights(int P, double* w) {
 // ---- the fill: stage 0 (copies, hooks), then prolongation level by level ----
 static int launch_fill(tgh_problem* p, const double* src, bool from_work, double* work, double t) {
   const int T = 256;
+  if (!from_work && p->nranks > 1)
+    return fail(p, TGH_ERR_ARG, "a sharded problem is filled through its exchange phases (tgh_shard_*), not from u");
   if (from_work) {
     if (p->ngpts) {
       fill_points_kernel<<<grid_for(p->ngpts, T), T, 0, p->stream>>>(p->gpts, p->ngpts, work, p->geo);
@@ -399,23 +523,50 @@ static int stage_limit_impl(tgh_problem* p, double* u, double t) {
 
 extern "C" {
 
-int tgh_problem_create(const tgh_config* cfg, const tgh_mesh* m, void* cuda_stream, int margin_check,
-                       tgh_problem** out) {
+// A problem over the leaves `owner` gives to `rank` of `nranks` (owner null: every leaf, one
+// rank). Its working arrays also hold the halo blocks its fill reads from other ranks.
+static int setup_host(tgh_problem* p, const tgh_config* cfg, const tgh_mesh* m, const int* owner, int rank,
+                      int nranks, int margin_check);
+static int setup_device(tgh_problem* p);
+
+static int create_impl(const tgh_config* cfg, const tgh_mesh* m, const int* owner, int rank, int nranks,
+                       void* cuda_stream, int margin_check, tgh_problem** out) {
   *out = nullptr;
   tgh_problem* p = new tgh_problem();
   *out = p;
-  p->cfg = *cfg;
   p->stream = (cudaStream_t)cuda_stream;
+  int s = setup_host(p, cfg, m, owner, rank, nranks, margin_check);
+  if (s) return s;
+  // the fill plan fixes the internal numbering (own leaves, then the halo)
+  if ((s = build_plan(p))) return s;
+  return setup_device(p);
+}
+
+// The problem's host state: the checked configuration, the forest, the owner ranks.
+static int setup_host(tgh_problem* p, const tgh_config* cfg, const tgh_mesh* m, const int* owner, int rank,
+                      int nranks, int margin_check) {
+  p->cfg = *cfg;
   const int q = cfg->q;
   if (q < 2 || q > 8 || q % 2) return fail(p, TGH_ERR_ARG, "the finite-difference order must be even and in 2..8, got " + std::to_string(q));
   if (m->N < 2 * (q / 2 + 1)) return fail(p, TGH_ERR_ARG, "the block edge N must be at least 2G");
   if (m->nblocks < 1) return fail(p, TGH_ERR_ARG, "the forest has no leaves");
+  if (nranks < 1 || rank < 0 || rank >= nranks) return fail(p, TGH_ERR_ARG, "the rank must lie in 0 .. nranks - 1");
+  p->rank = rank;
+  p->nranks = nranks;
+  p->owner.assign(m->nblocks, 0);
+  if (owner) {
+    for (int g = 0; g < m->nblocks; ++g) {
+      if (owner[g] < 0 || owner[g] >= nranks) return fail(p, TGH_ERR_ARG, "a leaf's owner rank is out of range");
+      p->owner[g] = owner[g];
+    }
+  }
+  p->nb = (int)std::count(p->owner.begin(), p->owner.end(), rank);
+  if (p->nb < 1) return fail(p, TGH_ERR_ARG, "this rank owns no leaf");
   p->q = q;
   p->G = q / 2 + 1;
   p->N = m->N;
   p->N1 = m->N + 1;
   p->Wd = m->N + 2 * p->G + 1;
-  p->nb = m->nblocks;
   p->h0 = m->h0;
   for (int d = 0; d < 3; ++d) {
     p->lo[d] = m->lo[d];
@@ -425,14 +576,14 @@ int tgh_problem_create(const tgh_config* cfg, const tgh_mesh* m, void* cuda_stre
   }
   p->level.assign(m->level, m->level + m->nblocks);
   p->corner.assign(m->corner, m->corner + 3 * m->nblocks);
-  for (int b = 0; b < p->nb; ++b) {
+  for (int b = 0; b < m->nblocks; ++b) {
     if (p->level[b] < 0 || p->level[b] > 20) return fail(p, TGH_ERR_ARG, "block level out of range");
     p->maxlevel = std::max(p->maxlevel, p->level[b]);
     for (int d = 0; d < 3; ++d)
       if (p->corner[3 * b + d] % p->N) return fail(p, TGH_ERR_ARG, "a block corner is not a multiple of N");
   }
   p->lut.resize(p->maxlevel + 1);
-  for (int b = 0; b < p->nb; ++b) {
+  for (int b = 0; b < m->nblocks; ++b) {
     auto key = bkey(p->corner[3 * b] / p->N, p->corner[3 * b + 1] / p->N, p->corner[3 * b + 2] / p->N);
     if (!p->lut[p->level[b]].emplace(key, b).second) return fail(p, TGH_ERR_ARG, "two leaves share a corner and level");
   }
@@ -457,19 +608,26 @@ int tgh_problem_create(const tgh_config* cfg, const tgh_mesh* m, void* cuda_stre
         return fail(p, TGH_ERR_RADII, "the frozen core does not contain the chart's singular disk |x| <= |a|");
     }
   }
-  // per-block geometry
-  std::vector<double> blk(8 * (size_t)p->nb, 0.0);
-  for (int b = 0; b < p->nb; ++b) {
+  return TGH_OK;
+}
+
+// The problem's device state, once the plan has fixed the internal block numbering.
+static int setup_device(tgh_problem* p) {
+  const tgh_config* cfg = &p->cfg;
+  // per-block geometry, internal numbering
+  std::vector<double> blk(8 * (size_t)p->nwb, 0.0);
+  for (int b = 0; b < p->nwb; ++b) {
+    const int g = p->i2g[b];
     for (int d = 0; d < 3; ++d) {
       blk[8 * b + d] = p->lo[d];
-      blk[8 * b + 4 + d] = (double)p->corner[3 * b + d];
+      blk[8 * b + 4 + d] = (double)p->corner[3 * g + d];
     }
-    blk[8 * b + 3] = std::ldexp(p->h0, -p->level[b]);
+    blk[8 * b + 3] = std::ldexp(p->h0, -p->level[g]);
   }
   CK(cudaMalloc(&p->blk, blk.size() * sizeof(double)));
   CK(cudaMemcpy(p->blk, blk.data(), blk.size() * sizeof(double), cudaMemcpyHostToDevice));
-  CK(cudaMalloc(&p->work, (size_t)p->Wv * NV * p->nb * sizeof(double)));
-  CK(cudaMemsetAsync(p->work, 0, (size_t)p->Wv * NV * p->nb * sizeof(double), p->stream));
+  CK(cudaMalloc(&p->work, (size_t)p->Wv * NV * p->nwb * sizeof(double)));
+  CK(cudaMemsetAsync(p->work, 0, (size_t)p->Wv * NV * p->nwb * sizeof(double), p->stream));
   CK(cudaMalloc(&p->scratch, 2 * sizeof(unsigned long long)));
   CK(cudaMalloc(&p->coef, (size_t)NCOEF * p->npts * sizeof(double)));
   p->npart = (int)grid_for(p->npts, 128);
@@ -477,8 +635,6 @@ int tgh_problem_create(const tgh_config* cfg, const tgh_mesh* m, void* cuda_stre
   double wp[10] = {0};
   prolong_weights(p->q + 2, wp);
   CK(cudaMemcpyToSymbol(c_wprol, wp, sizeof(wp)));
-  int s = build_plan(p);
-  if (s) return s;
   if (cfg->gauge == TGH_GAUGE_SAMPLED) {
     CK(cudaMalloc(&p->Hsrc, (size_t)p->S * NV * p->nb * sizeof(double)));
     sample_gauge_kernel<<<grid_for(p->npts, 64), 64, 0, p->stream>>>(p->Hsrc, p->blk, p->geo, p->npts, p->cs, 0.0);
@@ -488,10 +644,24 @@ int tgh_problem_create(const tgh_config* cfg, const tgh_mesh* m, void* cuda_stre
   return TGH_OK;
 }
 
+int tgh_problem_create(const tgh_config* cfg, const tgh_mesh* m, void* cuda_stream, int margin_check,
+                       tgh_problem** out) {
+  return create_impl(cfg, m, nullptr, 0, 1, cuda_stream, margin_check, out);
+}
+
+int tgh_problem_create_shard(const tgh_config* cfg, const tgh_mesh* m, const int* owner, int rank, int nranks,
+                             void* cuda_stream, int margin_check, tgh_problem** out) {
+  return create_impl(cfg, m, owner, rank, nranks, cuda_stream, margin_check, out);
+}
+
 void tgh_problem_destroy(tgh_problem* p) {
   if (!p) return;
   if (p->gexec) cudaGraphExecDestroy(p->gexec);
   if (p->cap) cudaStreamDestroy(p->cap);
+  for (auto& x : p->xch) {
+    if (x.send) cudaFree(x.send);
+    if (x.recv) cudaFree(x.recv);
+  }
   void* bufs[] = {p->work, p->Hsrc, p->blk, p->primary, p->runs, p->gpts, p->hooks, p->scratch, p->part, p->coef,
                   p->k, p->acc, p->y, p->u0, p->W1, p->W2, p->bacc};
   for (void* b : bufs)
@@ -503,7 +673,7 @@ void tgh_problem_destroy(tgh_problem* p) {
 
 const char* tgh_last_error(const tgh_problem* p) { return p ? p->err.c_str() : "no problem"; }
 size_t tgh_state_length(const tgh_problem* p) { return (size_t)p->S * NV * p->nb; }
-size_t tgh_work_length(const tgh_problem* p) { return (size_t)p->Wv * NV * p->nb; }
+size_t tgh_work_length(const tgh_problem* p) { return (size_t)p->Wv * NV * p->nwb; }
 
 int tgh_copy_work(tgh_problem* p, double* dst) {
   CK(cudaMemcpyAsync(dst, p->work, tgh_work_length(p) * sizeof(double), cudaMemcpyDeviceToDevice, p->stream));
@@ -607,24 +777,80 @@ int tgh_rk4_step(tgh_problem* p, double* u, double t, double dt) {
 }
 
 // batched form, one step's launches on the stream (captured into a graph by the caller)
-static int batched_step(tgh_problem* p, double t, double dt) {
+// Stage st (0..3) of the batched form's RK4 step from t: the time it evaluates at, the working
+// array it reads (filled first) and the one it writes, and its update coefficients.
+struct StagePlan {
+  double ts, ca, cb;
+  double *rd, *wr;
+};
+static StagePlan stage_plan(tgh_problem* p, int st, double t, double dt) {
   const double b16 = dt / 6.0, b13 = dt / 3.0, a12 = 0.5 * dt;
   const double ts[4] = {t, t + 0.5 * dt, t + 0.5 * dt, t + dt};
   const double ca[4] = {a12, a12, dt, 0.0}, cb[4] = {b16, b13, b13, b16};
   double* rd[4] = {p->work, p->W1, p->W2, p->W1};
   double* wr[4] = {p->W1, p->W2, p->W1, p->work};
+  return StagePlan{ts[st], ca[st], cb[st], rd[st], wr[st]};
+}
+
+static int stage_rhs(tgh_problem* p, const StagePlan& sp, int st) {
+  RhsArgs a = base_args(p, sp.rd, sp.ts);
+  a.u0 = p->work;
+  a.acc = p->bacc;
+  a.next = sp.wr;
+  a.ca = sp.ca;
+  a.cb = sp.cb;
+  a.stage = st + 1;
+  return launch_rhs(p, a, MODE_STAGE);
+}
+
+static int batched_step(tgh_problem* p, double t, double dt) {
   int s;
   for (int st = 0; st < 4; ++st) {
-    if ((s = launch_fill(p, rd[st], true, rd[st], ts[st]))) return s;
-    RhsArgs a = base_args(p, rd[st], ts[st]);
-    a.u0 = p->work;
-    a.acc = p->bacc;
-    a.next = wr[st];
-    a.ca = ca[st];
-    a.cb = cb[st];
-    a.stage = st + 1;
-    if ((s = launch_rhs(p, a, MODE_STAGE))) return s;
+    const StagePlan sp = stage_plan(p, st, t, dt);
+    if ((s = launch_fill(p, sp.rd, true, sp.rd, sp.ts))) return s;
+    if ((s = stage_rhs(p, sp, st))) return s;
   }
+  return TGH_OK;
+}
+
+// One phase of the batched form's fill of `work` on this rank: phase 0 the copies and the
+// Dirichlet hook, phase l >= 1 level l's prolongation. The halo values a phase reads must have
+// been unpacked first.
+static int launch_fill_phase(tgh_problem* p, double* work, int phase, double t) {
+  const int T = 256;
+  if (phase == 0) {
+    if (p->ngpts) {
+      fill_points_kernel<<<grid_for(p->ngpts, T), T, 0, p->stream>>>(p->gpts, p->ngpts, work, p->geo);
+      CK(cudaGetLastError());
+    }
+    if (p->nhooks) {
+      fill_hook_kernel<<<grid_for(p->nhooks, 128), 128, 0, p->stream>>>(p->hooks, p->nhooks, p->blk, work, p->geo,
+                                                                        p->cs, t);
+      CK(cudaGetLastError());
+    }
+    return TGH_OK;
+  }
+  const int l = phase;
+  if (!p->nprol[l]) return TGH_OK;
+  const long n = (long)p->nprol[l] * NV;
+  switch (p->q + 2) {
+    case 4: fill_prolong_kernel<4><<<grid_for(n, T), T, 0, p->stream>>>(p->prol[l], p->nprol[l], work, p->geo); break;
+    case 6: fill_prolong_kernel<6><<<grid_for(n, T), T, 0, p->stream>>>(p->prol[l], p->nprol[l], work, p->geo); break;
+    case 8: fill_prolong_kernel<8><<<grid_for(n, T), T, 0, p->stream>>>(p->prol[l], p->nprol[l], work, p->geo); break;
+    default: fill_prolong_kernel<10><<<grid_for(n, T), T, 0, p->stream>>>(p->prol[l], p->nprol[l], work, p->geo); break;
+  }
+  CK(cudaGetLastError());
+  return TGH_OK;
+}
+
+static int batched_buffers(tgh_problem* p) {
+  if (p->W1) return TGH_OK;
+  const size_t Lw = tgh_work_length(p), L = tgh_state_length(p);
+  CK(cudaMalloc(&p->W1, Lw * sizeof(double)));
+  CK(cudaMalloc(&p->W2, Lw * sizeof(double)));
+  CK(cudaMalloc(&p->bacc, L * sizeof(double)));
+  CK(cudaMemsetAsync(p->W1, 0, Lw * sizeof(double), p->stream));
+  CK(cudaMemsetAsync(p->W2, 0, Lw * sizeof(double), p->stream));
   return TGH_OK;
 }
 
@@ -632,17 +858,10 @@ int tgh_step_batched(tgh_problem* p, double* u, double t, double dt, int nsteps)
   if (nsteps < 1) return fail(p, TGH_ERR_ARG, "nsteps must be positive");
   if (p->cfg.interior == TGH_INT_PASTED)
     return fail(p, TGH_ERR_ARG, "the batched form has no :pasted limiter; use tgh_rk4_step");
-  const size_t Lw = tgh_work_length(p), L = tgh_state_length(p);
-  if (!p->W1) {
-    CK(cudaMalloc(&p->W1, Lw * sizeof(double)));
-    CK(cudaMalloc(&p->W2, Lw * sizeof(double)));
-    CK(cudaMalloc(&p->bacc, L * sizeof(double)));
-    CK(cudaMemsetAsync(p->W1, 0, Lw * sizeof(double), p->stream));
-    CK(cudaMemsetAsync(p->W2, 0, Lw * sizeof(double), p->stream));
-  }
-  // the state into W0's owned points (and ghosts), outside the graph
-  int s = launch_fill(p, u, false, p->work, t);
+  int s = batched_buffers(p);
   if (s) return s;
+  // the state into W0's owned points (and ghosts), outside the graph
+  if ((s = launch_fill(p, u, false, p->work, t))) return s;
   const bool reuse = p->gexec && p->gkey.t == t && p->gkey.dt == dt && p->gkey.nsteps == nsteps;
   if (!reuse) {
     if (p->gexec) {
@@ -681,6 +900,163 @@ int tgh_step_batched(tgh_problem* p, double* u, double t, double dt, int nsteps)
   gather_kernel<<<grid_for(p->npts, 256), 256, 0, p->stream>>>(p->work, u, p->geo, p->npts);
   CK(cudaGetLastError());
   p->last_launches = fill_launches(p, false) + p->graph_kernels + 1;
+  return TGH_OK;
+}
+
+// ---- the sharded batched step (one rank per GPU), driven by the caller ----
+// tgh_shard_begin; per step, per stage st = 0..3: for phase = 0 .. tgh_shard_phases - 1:
+// tgh_shard_pack -> the caller's exchange (peer-major buffers, counts from tgh_shard_counts) ->
+// tgh_shard_unpack -> tgh_shard_fill; then tgh_shard_rhs; finally tgh_shard_end. Every call
+// is stream-ordered on the problem's stream.
+
+int tgh_partition(const tgh_mesh* m, int nranks, int* owner) {
+  if (nranks < 1 || m->nblocks < 1 || m->N < 1) return TGH_ERR_ARG;
+  // per level, the leaves in Morton order of their block coordinates, cut into nranks
+  // contiguous runs of (nearly) equal length
+  int maxl = 0;
+  for (int b = 0; b < m->nblocks; ++b) maxl = std::max(maxl, m->level[b]);
+  auto spread = [](uint64_t x) {
+    x &= 0x1fffff;
+    x = (x | x << 32) & 0x1f00000000ffffULL;
+    x = (x | x << 16) & 0x1f0000ff0000ffULL;
+    x = (x | x << 8) & 0x100f00f00f00f00fULL;
+    x = (x | x << 4) & 0x10c30c30c30c30c3ULL;
+    x = (x | x << 2) & 0x1249249249249249ULL;
+    return x;
+  };
+  for (int l = 0; l <= maxl; ++l) {
+    std::vector<std::pair<uint64_t, int>> v;
+    for (int b = 0; b < m->nblocks; ++b)
+      if (m->level[b] == l) {
+        const uint64_t bx = (uint64_t)(m->corner[3 * b] / m->N), by = (uint64_t)(m->corner[3 * b + 1] / m->N),
+                       bz = (uint64_t)(m->corner[3 * b + 2] / m->N);
+        v.push_back({spread(bx) | spread(by) << 1 | spread(bz) << 2, b});
+      }
+    std::sort(v.begin(), v.end());
+    const size_t n = v.size();
+    for (size_t i = 0; i < n; ++i) owner[v[i].second] = (int)((i * (size_t)nranks) / n);
+  }
+  return TGH_OK;
+}
+
+// Host-only view of `rank`'s exchange in fill phase `phase`, for tests and tooling: per peer
+// rank the counts, and (when the arrays are given, 2 ints per point) the (global leaf, work
+// index) pairs this rank sends and receives, peer-major. Touches no GPU.
+int tgh_shard_plan(const tgh_config* cfg, const tgh_mesh* m, const int* owner, int rank, int nranks, int phase,
+                   long* send_count, long* recv_count, int* send_pts, int* recv_pts, char* errbuf, int errlen) {
+  tgh_problem p;
+  int s = setup_host(&p, cfg, m, owner, rank, nranks, 0);
+  std::string err = p.err;
+  if (!s && (phase < 0 || phase > p.maxlevel)) {
+    s = TGH_ERR_ARG;
+    err = "no such fill phase";
+  }
+  HostPlan mine;
+  if (!s && !plan_rank(&p, rank, false, mine, err)) s = TGH_ERR_ARG;
+  long ns = 0, nr = 0;
+  for (int o = 0; !s && o < nranks; ++o) {
+    send_count[o] = recv_count[o] = 0;
+    if (o == rank) continue;
+    HostPlan theirs;
+    if (!plan_rank(&p, o, false, theirs, err)) {
+      s = TGH_ERR_ARG;
+      break;
+    }
+    auto a = theirs.req.find({rank, phase});
+    if (a != theirs.req.end()) {
+      send_count[o] = (long)a->second.size();
+      for (const auto& e : a->second)
+        if (send_pts) {
+          send_pts[2 * ns] = e.first;
+          send_pts[2 * ns++ + 1] = e.second;
+        }
+    }
+    auto b = mine.req.find({o, phase});
+    if (b != mine.req.end()) {
+      recv_count[o] = (long)b->second.size();
+      for (const auto& e : b->second)
+        if (recv_pts) {
+          recv_pts[2 * nr] = e.first;
+          recv_pts[2 * nr++ + 1] = e.second;
+        }
+    }
+  }
+  if (s && errbuf && errlen > 0) {
+    std::strncpy(errbuf, err.c_str(), (size_t)errlen - 1);
+    errbuf[errlen - 1] = 0;
+  }
+  return s;
+}
+
+int tgh_shard_phases(const tgh_problem* p) { return p->maxlevel + 1; }
+
+int tgh_shard_counts(tgh_problem* p, int phase, long* send_count, long* recv_count) {
+  if (phase < 0 || phase > p->maxlevel) return fail(p, TGH_ERR_ARG, "no such fill phase");
+  for (int r = 0; r < p->nranks; ++r) {
+    send_count[r] = p->xch[phase].send_count[r];
+    recv_count[r] = p->xch[phase].recv_count[r];
+  }
+  return TGH_OK;
+}
+
+int tgh_shard_begin(tgh_problem* p, const double* u) {
+  if (p->cfg.interior == TGH_INT_PASTED)
+    return fail(p, TGH_ERR_ARG, "the batched form has no :pasted limiter; use tgh_rk4_step");
+  int s = batched_buffers(p);
+  if (s) return s;
+  scatter_owned_kernel<<<grid_for(p->npts, 256), 256, 0, p->stream>>>(u, p->work, p->geo, p->npts);
+  CK(cudaGetLastError());
+  return TGH_OK;
+}
+
+static int shard_check(tgh_problem* p, int stage, int phase) {
+  if (!p->W1) return fail(p, TGH_ERR_ARG, "tgh_shard_begin has not been called");
+  if (stage < 0 || stage > 3) return fail(p, TGH_ERR_ARG, "the stage must lie in 0..3");
+  if (phase < 0 || phase > p->maxlevel) return fail(p, TGH_ERR_ARG, "no such fill phase");
+  return TGH_OK;
+}
+
+int tgh_shard_pack(tgh_problem* p, int stage, int phase, double* send) {
+  int s = shard_check(p, stage, phase);
+  if (s) return s;
+  const ExchangeList& x = p->xch[phase];
+  if (x.nsend) {
+    pack_kernel<<<grid_for(x.nsend * NV, 256), 256, 0, p->stream>>>(x.send, x.nsend, stage_plan(p, stage, 0, 0).rd,
+                                                                    p->geo, send);
+    CK(cudaGetLastError());
+  }
+  return TGH_OK;
+}
+
+int tgh_shard_unpack(tgh_problem* p, int stage, int phase, const double* recv) {
+  int s = shard_check(p, stage, phase);
+  if (s) return s;
+  const ExchangeList& x = p->xch[phase];
+  if (x.nrecv) {
+    unpack_kernel<<<grid_for(x.nrecv * NV, 256), 256, 0, p->stream>>>(x.recv, x.nrecv, recv,
+                                                                      stage_plan(p, stage, 0, 0).rd, p->geo);
+    CK(cudaGetLastError());
+  }
+  return TGH_OK;
+}
+
+int tgh_shard_fill(tgh_problem* p, int stage, int phase, double t, double dt) {
+  int s = shard_check(p, stage, phase);
+  if (s) return s;
+  const StagePlan sp = stage_plan(p, stage, t, dt);
+  return launch_fill_phase(p, sp.rd, phase, sp.ts);
+}
+
+int tgh_shard_rhs(tgh_problem* p, int stage, double t, double dt) {
+  int s = shard_check(p, stage, 0);
+  if (s) return s;
+  return stage_rhs(p, stage_plan(p, stage, t, dt), stage);
+}
+
+int tgh_shard_end(tgh_problem* p, double* u) {
+  if (!p->W1) return fail(p, TGH_ERR_ARG, "tgh_shard_begin has not been called");
+  gather_kernel<<<grid_for(p->npts, 256), 256, 0, p->stream>>>(p->work, u, p->geo, p->npts);
+  CK(cudaGetLastError());
   return TGH_OK;
 }
 
