@@ -198,6 +198,93 @@ def run_reference(args):
     return 0
 
 
+def run_sharded(args, tgh, world, rank, local, case, forest, cfg, gauge, perturbed):
+    """--gpus N > 1: the workload's mesh sharded over the N ranks (per-level Morton partition),
+    each fill phase preceded by one NCCL all-to-all of the halo points; the mesh is the same
+    for every N (strong scaling). Device time, max over ranks."""
+    import torch
+    import torch.distributed as dist
+    stream = torch.cuda.current_stream()
+    owner = tgh.partition(forest, world)
+    S = tgh.ShardedGHProblem(case, forest, 4, rank, world, owner=owner, margin_check=False)
+    u0 = S.initial_state(S.statevector(), 0.0)
+    if perturbed:
+        u0 += S.local(torch.from_numpy(tgh.perturbation(forest, amplitude=1e-4)).cuda())
+
+    def gmax(x):
+        t = torch.tensor([float(x)], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    dt = 0.25 * h_min(forest) / gmax(S.max_speed(u0, 0.0))
+    K, W = args.steps, max(3, args.warmup)
+    u = u0.clone()
+    for _ in range(-(-W // K)):
+        u.copy_(u0)
+        S.step(u, 0.0, dt, K)
+    torch.cuda.synchronize()
+    u.copy_(u0)
+    clocks = Clocks(local)
+    time.sleep(0.3)
+    dist.barrier()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    S.step(u, 0.0, dt, K)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    dist.barrier()
+    ms = gmax(e0.elapsed_time(e1))
+    ck = clocks.stop()
+    launches = S.last_launch_count()
+    if gmax(0.0 if bool(torch.isfinite(u).all()) else 1.0) > 0.0:
+        raise SystemExit("the evolved state is not finite")
+    pts = forest.points()
+    value = pts * K / (ms * 1e-3)
+    rhs_ms = gmax(S.time_rhs(u, 0.0, nlaunch=max(2, K // 10)))
+    n1pts = (forest.N + 1) ** 3 * forest.nblocks
+    achieved = FLOP_PER_POINT_RHS[gauge] * n1pts / (rhs_ms * 1e-3) / 1e12
+    peak = tgh.fp64_peak_tflops() * world
+    # end to end: per step this rank's state in from pinned host memory and back
+    uh = u0.cpu().pin_memory()
+    res_h = torch.empty_like(uh).pin_memory()
+    ud = torch.empty_like(u0)
+    dist.barrier()
+    torch.cuda.synchronize()
+    e2, e3 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e2.record(stream)
+    for _ in range(K):
+        ud.copy_(uh, non_blocking=True)
+        S.step(ud, 0.0, dt, 1)
+        res_h.copy_(ud, non_blocking=True)
+    e3.record(stream)
+    torch.cuda.synchronize()
+    e2e_ms = gmax(e2.elapsed_time(e3))
+    nbytes = uh.numel() * 8
+    out = {"metric": "RK4 point-updates/s", "value": value, "unit": "point-updates/s", "n_gpus": world,
+           "steps": K, "warmup": W, "ms_per_step": ms / K, "higher_is_better": True, "scaling": "strong",
+           "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+           "config": {**cfg, "form": "batched, sharded (host-driven stages, no graph)", "points": pts,
+                      "l2_flush": "inputs larger than L2 on every rank" if S.state_length * 8 > 126e6
+                      else "per-rank working set below L2 size",
+                      "parallelism": f"sharded x{world}: per-level Morton partition, NCCL all-to-all per fill phase",
+                      "blocks_per_rank": int(len(S.leaves))},
+           "roofline": {"bound": "fp64", "kernel": "rhs_head_kernel + rhs_pi_kernel (one RHS, RK4 stage epilogue)",
+                        "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
+                        "traffic": None, "flop_per_point": FLOP_PER_POINT_RHS[gauge], "points_per_launch": n1pts,
+                        "ms_per_launch": rhs_ms,
+                        "peak_source": f"measured FP64 FMA probe x {world} GPUs"},
+           "e2e": {"value": pts * K / (e2e_ms * 1e-3), "unit": "point-updates/s",
+                   "h2d_bytes_per_step": nbytes * world, "d2h_bytes_per_step": nbytes * world},
+           "plain_form": {"skipped": "the plain form runs on one GPU"},
+           "gpu_launches": launches, "clocks": ck}
+    if rank == 0:
+        print(json.dumps(out))
+    S.close()
+    dist.destroy_process_group()
+    return 0
+
+
 def end_to_end(P, u0, dt, K, world, pts, stream, dist):
     """The metric through the public API with host buffers: per step the state is copied in
     from pinned host memory, stepped, and copied back, all inside the timed region."""
@@ -233,6 +320,8 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="kerr_schild_static", choices=["kerr_schild_static", "fourier", "hierarchy"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--shard", action="store_true",
+                    help="run the sharded step (the --gpus N > 1 path) even on one GPU")
     ap.add_argument("--rhs-only", action="store_true",
                     help="time only the right-hand side (head + Pi kernels, stage epilogue) on the workload: "
                          "the command the kernel profiles are taken with")
@@ -246,11 +335,16 @@ def main():
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
     torch.cuda.set_device(local)
-    if world > 1:
+    if world > 1 or args.shard:
         import datetime
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+        os.environ.setdefault("MASTER_ADDR", "127.0.0.1")
+        os.environ.setdefault("MASTER_PORT", "29533")
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), rank=rank, world_size=world,
+                                device_id=torch.device("cuda", local))
     tgh = load_package()
     case, forest, scase, sforest, cfg, gauge, perturbed = workload(tgh, args.workload)
+    if world > 1 or args.shard:
+        return run_sharded(args, tgh, world, rank, local, case, forest, cfg, gauge, perturbed)
     stream = torch.cuda.current_stream()
     P = tgh.GHProblem(case, forest, 4, margin_check=False)
     u0 = initial(tgh, P, forest, perturbed)

@@ -76,7 +76,8 @@ struct tgh_problem {
   cudaGraphExec_t gexec = nullptr;
   GraphKey gkey{0, 0, 0};
   long graph_kernels = 0;  // kernel nodes of the captured graph
-  long last_launches = 0;  // kernels the last tgh_step_batched call ran
+  long last_launches = 0;  // kernels the last tgh_step_batched call (or sharded step) ran
+  long launches = 0;       // kernels launched since tgh_shard_begin
   const double* gu = nullptr;
 };
 
@@ -1006,6 +1007,7 @@ int tgh_shard_begin(tgh_problem* p, const double* u) {
   if (s) return s;
   scatter_owned_kernel<<<grid_for(p->npts, 256), 256, 0, p->stream>>>(u, p->work, p->geo, p->npts);
   CK(cudaGetLastError());
+  p->launches = 1;
   return TGH_OK;
 }
 
@@ -1024,6 +1026,7 @@ int tgh_shard_pack(tgh_problem* p, int stage, int phase, double* send) {
     pack_kernel<<<grid_for(x.nsend * NV, 256), 256, 0, p->stream>>>(x.send, x.nsend, stage_plan(p, stage, 0, 0).rd,
                                                                     p->geo, send);
     CK(cudaGetLastError());
+    ++p->launches;
   }
   return TGH_OK;
 }
@@ -1036,6 +1039,7 @@ int tgh_shard_unpack(tgh_problem* p, int stage, int phase, const double* recv) {
     unpack_kernel<<<grid_for(x.nrecv * NV, 256), 256, 0, p->stream>>>(x.recv, x.nrecv, recv,
                                                                       stage_plan(p, stage, 0, 0).rd, p->geo);
     CK(cudaGetLastError());
+    ++p->launches;
   }
   return TGH_OK;
 }
@@ -1044,12 +1048,14 @@ int tgh_shard_fill(tgh_problem* p, int stage, int phase, double t, double dt) {
   int s = shard_check(p, stage, phase);
   if (s) return s;
   const StagePlan sp = stage_plan(p, stage, t, dt);
+  p->launches += phase == 0 ? (p->ngpts ? 1 : 0) + (p->nhooks ? 1 : 0) : (p->nprol[phase] ? 1 : 0);
   return launch_fill_phase(p, sp.rd, phase, sp.ts);
 }
 
 int tgh_shard_rhs(tgh_problem* p, int stage, double t, double dt) {
   int s = shard_check(p, stage, 0);
   if (s) return s;
+  p->launches += 2;
   return stage_rhs(p, stage_plan(p, stage, t, dt), stage);
 }
 
@@ -1057,6 +1063,7 @@ int tgh_shard_end(tgh_problem* p, double* u) {
   if (!p->W1) return fail(p, TGH_ERR_ARG, "tgh_shard_begin has not been called");
   gather_kernel<<<grid_for(p->npts, 256), 256, 0, p->stream>>>(p->work, u, p->geo, p->npts);
   CK(cudaGetLastError());
+  p->last_launches = p->launches + 1;
   return TGH_OK;
 }
 
@@ -1072,7 +1079,9 @@ int tgh_time_rhs(tgh_problem* p, const double* u, double t, int mode, int nlaunc
     CK(cudaMalloc(&p->bacc, L * sizeof(double)));
     CK(cudaMemsetAsync(p->bacc, 0, L * sizeof(double), p->stream));
   }
-  int s = tgh_prepare(p, u, t);
+  // a rank of a sharded problem cannot fill from u alone: it is timed on its working array as
+  // its last step left it (filled)
+  int s = p->nranks > 1 ? TGH_OK : tgh_prepare(p, u, t);
   if (s) return s;
   RhsArgs a = base_args(p, p->work, t);
   a.du = p->k;

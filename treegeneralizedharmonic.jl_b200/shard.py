@@ -117,6 +117,35 @@ class ShardedGHProblem:
         per = u_all.numel() // self.forest.nblocks
         return u_all.view(self.forest.nblocks, per)[torch.as_tensor(self.leaves, device=u_all.device)].reshape(-1)
 
+    # ---- pointwise verbs on this rank's leaves ----
+    def initial_state(self, u, t):
+        """The analytic state (through the core rule) at this rank's owned points."""
+        self._check(self.lib.tgh_initial_state(self._h, _ptr(u), float(t)))
+        return u
+
+    def max_speed(self, u, t):
+        """The largest characteristic speed over this rank's evolved points; the caller takes
+        the maximum over ranks."""
+        lam = ctypes.c_double()
+        st = self.lib.tgh_max_speed(self._h, _ptr(u), float(t), ctypes.byref(lam))
+        if st == _abi.TGH_ERR_SPEED and lam.value == 0.0:
+            return 0.0  # no evolved point on this rank (all inside a frozen core)
+        self._check(st)
+        return lam.value
+
+    def last_launch_count(self):
+        """Kernels the last sharded step launched on this rank."""
+        n = ctypes.c_long()
+        self._check(self.lib.tgh_last_launch_count(self._h, ctypes.byref(n)))
+        return n.value
+
+    def time_rhs(self, u, t, nlaunch=2):
+        """ms per right-hand side (batched form, head + Pi) on this rank's leaves, timed on the
+        working array as the last step left it."""
+        ms = ctypes.c_double()
+        self._check(self.lib.tgh_time_rhs(self._h, _ptr(u), float(t), 1, int(nlaunch), ctypes.byref(ms)))
+        return ms.value
+
     # ---- the step's pieces (include/tgh.h) ----
     def begin(self, u):
         self._check(self.lib.tgh_shard_begin(self._h, _ptr(u)))
