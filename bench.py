@@ -8,6 +8,11 @@ point is an owned point counted N^3 per block, as the reference counts it.
     python bench.py [--gpus N] [--steps K] [--warmup W] [--workload kerr_schild_static|fourier|hierarchy]
     python bench.py --impl reference ...   # the CPU restatement of the reference's path
 
+One GPU: the batched form (the whole K-step run one CUDA graph). N GPUs (torchrun, one rank
+per GPU): the workload's mesh sharded over the ranks, per-level Morton partition, one NCCL
+all-to-all of halo points before each fill phase; the mesh is the same for every N (strong
+scaling). --shard runs that sharded path on one GPU.
+
 Workloads (seeded synthetic inputs, fully specified by their parameters):
   kerr_schild_static  static Kerr-Schild hole M=1, a=7/10 on [-8,8]^3, 64 blocks of 32^3
                       (h = 1/8), Dirichlet faces, :damped interior r_0=0.8 r_1=1.3 rho_max=4/M,
