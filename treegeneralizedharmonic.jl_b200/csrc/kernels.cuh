@@ -82,9 +82,10 @@ __global__ void fill_points_kernel(const CopyPt* __restrict__ pts, long n, doubl
   for (int k = 0; k < NV; ++k) dst[k * g.Wv] = v[k];
 }
 
-// the Dirichlet hook: the analytic state (through the core rule) at each outer ghost point
+// the Dirichlet hook: the analytic state (through the core rule) at each outer ghost point;
+// with `cache` (stationary cases) the values are also kept, 20 per point
 __global__ void fill_hook_kernel(const HookPt* __restrict__ pts, int n, const double* __restrict__ blk,
-                                 double* __restrict__ work, Geo g, const Case cs, double t) {
+                                 double* __restrict__ work, Geo g, const Case cs, double t, double* cache) {
   const int id = blockIdx.x * blockDim.x + threadIdx.x;
   if (id >= n) return;
   const HookPt p = pts[id];
@@ -96,6 +97,19 @@ __global__ void fill_hook_kernel(const HookPt* __restrict__ pts, int n, const do
   double* dst = work + (long)p.b * NV * g.Wv + p.w;
 #pragma unroll
   for (int v = 0; v < NV; ++v) dst[v * g.Wv] = v20[v];
+  if (cache) {
+#pragma unroll
+    for (int v = 0; v < NV; ++v) cache[(long)id * NV + v] = v20[v];
+  }
+}
+
+// the Dirichlet hook of a stationary case from the values kept by fill_hook_kernel
+__global__ void hook_copy_kernel(const HookPt* __restrict__ pts, int n, const double* __restrict__ cache,
+                                 double* __restrict__ work, Geo g) {
+  const long id = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (id >= (long)n * NV) return;
+  const HookPt p = pts[id / NV];
+  work[(long)p.b * NV * g.Wv + (id % NV) * g.Wv + p.w] = cache[id];
 }
 
 // tensor-product Lagrange prolongation of order P from the coarse block's filled working

@@ -63,6 +63,8 @@ struct tgh_problem {
   long ngpts = 0;
   HookPt* hooks = nullptr;
   int nhooks = 0;
+  double* hook_cache = nullptr;  // stationary cases: the Dirichlet ghosts' values, 20 per point
+  bool hook_cache_valid = false;
   std::vector<ProlongPt*> prol;  // per level 1..maxlevel
   std::vector<int> nprol;
   unsigned long long* scratch = nullptr;  // speed reduction: max bits, non-finite count
@@ -439,6 +441,22 @@ static void prolong_weights(int P, double* w) {
   }
 }
 
+// The Dirichlet ghosts of `work` at time t. A stationary case (its analytic state does not
+// depend on t) evaluates them once and copies the kept values afterwards.
+static int launch_hooks(tgh_problem* p, double* work, double t) {
+  if (!p->nhooks) return TGH_OK;
+  if (p->hook_cache && p->hook_cache_valid) {
+    hook_copy_kernel<<<grid_for((long)p->nhooks * NV, 256), 256, 0, p->stream>>>(p->hooks, p->nhooks, p->hook_cache,
+                                                                                work, p->geo);
+  } else {
+    fill_hook_kernel<<<grid_for(p->nhooks, 128), 128, 0, p->stream>>>(p->hooks, p->nhooks, p->blk, work, p->geo,
+                                                                      p->cs, t, p->hook_cache);
+    p->hook_cache_valid = p->hook_cache != nullptr;
+  }
+  CK(cudaGetLastError());
+  return TGH_OK;
+}
+
 // ---- the fill: stage 0 (copies, hooks), then prolongation level by level ----
 static int launch_fill(tgh_problem* p, const double* src, bool from_work, double* work, double t) {
   const int T = 256;
@@ -453,11 +471,8 @@ static int launch_fill(tgh_problem* p, const double* src, bool from_work, double
     fill_copy_kernel<<<grid_for((long)p->nruns * 32, T), T, 0, p->stream>>>(p->runs, p->nruns, src, work, p->geo);
     CK(cudaGetLastError());
   }
-  if (p->nhooks) {
-    fill_hook_kernel<<<grid_for(p->nhooks, 128), 128, 0, p->stream>>>(p->hooks, p->nhooks, p->blk, work, p->geo,
-                                                                      p->cs, t);
-    CK(cudaGetLastError());
-  }
+  int s = launch_hooks(p, work, t);
+  if (s) return s;
   for (int l = 1; l <= p->maxlevel; ++l) {
     if (!p->nprol[l]) continue;
     const long n = (long)p->nprol[l] * NV;
@@ -612,9 +627,21 @@ static int setup_host(tgh_problem* p, const tgh_config* cfg, const tgh_mesh* m, 
   return TGH_OK;
 }
 
+// Whether the analytic state at a fixed position is the same at every time: a static
+// background (Minkowski, shifted Minkowski, Kerr-Schild without a boost) and an interior that
+// does not move. Its Dirichlet ghosts are then evaluated once.
+static bool stationary(const tgh_config& c) {
+  const double* u = c.bg.boost;
+  const bool bg = c.bg.kind == TGH_BG_MINKOWSKI || c.bg.kind == TGH_BG_SHIFTED_MINKOWSKI ||
+                  (c.bg.kind == TGH_BG_KERR_SCHILD && u[0] == 0.0 && u[1] == 0.0 && u[2] == 0.0);
+  const bool core = c.interior == TGH_INT_NONE || (c.int_v[0] == 0.0 && c.int_v[1] == 0.0 && c.int_v[2] == 0.0);
+  return bg && core;
+}
+
 // The problem's device state, once the plan has fixed the internal block numbering.
 static int setup_device(tgh_problem* p) {
   const tgh_config* cfg = &p->cfg;
+  if (p->nhooks && stationary(*cfg)) CK(cudaMalloc(&p->hook_cache, (size_t)p->nhooks * NV * sizeof(double)));
   // per-block geometry, internal numbering
   std::vector<double> blk(8 * (size_t)p->nwb, 0.0);
   for (int b = 0; b < p->nwb; ++b) {
@@ -663,7 +690,8 @@ void tgh_problem_destroy(tgh_problem* p) {
     if (x.send) cudaFree(x.send);
     if (x.recv) cudaFree(x.recv);
   }
-  void* bufs[] = {p->work, p->Hsrc, p->blk, p->primary, p->runs, p->gpts, p->hooks, p->scratch, p->part, p->coef,
+  void* bufs[] = {p->work, p->Hsrc, p->blk, p->primary, p->runs, p->gpts, p->hooks, p->hook_cache, p->scratch,
+                  p->part, p->coef,
                   p->k, p->acc, p->y, p->u0, p->W1, p->W2, p->bacc};
   for (void* b : bufs)
     if (b) cudaFree(b);
@@ -824,12 +852,7 @@ static int launch_fill_phase(tgh_problem* p, double* work, int phase, double t) 
       fill_points_kernel<<<grid_for(p->ngpts, T), T, 0, p->stream>>>(p->gpts, p->ngpts, work, p->geo);
       CK(cudaGetLastError());
     }
-    if (p->nhooks) {
-      fill_hook_kernel<<<grid_for(p->nhooks, 128), 128, 0, p->stream>>>(p->hooks, p->nhooks, p->blk, work, p->geo,
-                                                                        p->cs, t);
-      CK(cudaGetLastError());
-    }
-    return TGH_OK;
+    return launch_hooks(p, work, t);
   }
   const int l = phase;
   if (!p->nprol[l]) return TGH_OK;
