@@ -325,6 +325,8 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="kerr_schild_static", choices=["kerr_schild_static", "fourier", "hierarchy"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"],
+                    help="mixed: FP32 stencil sums and algebra on the FP64 state (one GPU)")
     ap.add_argument("--shard", action="store_true",
                     help="run the sharded step (the --gpus N > 1 path) even on one GPU")
     ap.add_argument("--rhs-only", action="store_true",
@@ -351,7 +353,7 @@ def main():
     if world > 1 or args.shard:
         return run_sharded(args, tgh, world, rank, local, case, forest, cfg, gauge, perturbed)
     stream = torch.cuda.current_stream()
-    P = tgh.GHProblem(case, forest, 4, margin_check=False)
+    P = tgh.GHProblem(case, forest, 4, margin_check=False, precision=args.precision)
     u0 = initial(tgh, P, forest, perturbed)
     if args.rhs_only:
         ms = P.time_rhs(u0, 0.0, mode=1, nlaunch=2)
@@ -442,8 +444,10 @@ def main():
 
     out = {"metric": "RK4 point-updates/s", "value": value, "unit": "point-updates/s", "n_gpus": world,
            "steps": K, "warmup": W, "ms_per_step": ms / K, "higher_is_better": True, "scaling": "weak",
-           "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+           "vs_baseline": None, "dtype": "f64" if args.precision == "fp64" else "f32 arithmetic, f64 state",
+           "data": "synthetic",
            "config": {**cfg, "form": "batched (fused RK4 epilogue, CUDA graph)", "points": pts,
+                      "precision": args.precision,
                       "l2_flush": "inputs larger than L2 (working arrays %.0f MB)" % (P.work_length * 8 / 1e6),
                       "parallelism": f"replicas x{world}" if world > 1 else "single GPU"},
            "roofline": {"bound": "fp64", "kernel": "rhs_head_kernel + rhs_pi_kernel (one RHS, RK4 stage epilogue)",

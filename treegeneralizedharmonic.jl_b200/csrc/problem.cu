@@ -49,6 +49,7 @@ struct tgh_problem {
   long S, Wv, npts;
   Case cs;
   bool diss = false, intr = false;
+  bool mixed = false;  // TGH_PREC_MIXED: FP32 stencil sums and algebra, FP64 state and metric
   cudaStream_t stream = nullptr;
   cudaStream_t cap = nullptr;  // the stream graphs are captured on
   std::string err;
@@ -497,11 +498,19 @@ static long fill_launches(const tgh_problem* p, bool from_work) {
 }
 
 static cudaError_t launch_part(tgh_problem* p, int part, int mode, cudaStream_t s, const RhsArgs& a) {
+  if (p->mixed) {
+    switch (p->q) {
+      case 2: return launch_rhs_q2_f32(part, p->diss, mode, p->intr, s, p->cs, a);
+      case 4: return launch_rhs_q4_f32(part, p->diss, mode, p->intr, s, p->cs, a);
+      case 6: return launch_rhs_q6_f32(part, p->diss, mode, p->intr, s, p->cs, a);
+      default: return launch_rhs_q8_f32(part, p->diss, mode, p->intr, s, p->cs, a);
+    }
+  }
   switch (p->q) {
-    case 2: return launch_rhs_q2(part, p->diss, mode, p->intr, s, p->cs, a);
-    case 4: return launch_rhs_q4(part, p->diss, mode, p->intr, s, p->cs, a);
-    case 6: return launch_rhs_q6(part, p->diss, mode, p->intr, s, p->cs, a);
-    default: return launch_rhs_q8(part, p->diss, mode, p->intr, s, p->cs, a);
+    case 2: return launch_rhs_q2_f64(part, p->diss, mode, p->intr, s, p->cs, a);
+    case 4: return launch_rhs_q4_f64(part, p->diss, mode, p->intr, s, p->cs, a);
+    case 6: return launch_rhs_q6_f64(part, p->diss, mode, p->intr, s, p->cs, a);
+    default: return launch_rhs_q8_f64(part, p->diss, mode, p->intr, s, p->cs, a);
   }
 }
 
@@ -610,6 +619,9 @@ static int setup_host(tgh_problem* p, const tgh_config* cfg, const tgh_mesh* m, 
   p->cs = make_case(*cfg);
   p->diss = cfg->dissipation == TGH_DISS_CONSTANT ? cfg->eps_ko != 0.0 : !(cfg->eps_out == 0.0 && cfg->eps_in == 0.0);
   p->intr = cfg->interior != TGH_INT_NONE;
+  if (cfg->precision != TGH_PREC_FP64 && cfg->precision != TGH_PREC_MIXED)
+    return fail(p, TGH_ERR_ARG, "the precision must be TGH_PREC_FP64 or TGH_PREC_MIXED");
+  p->mixed = cfg->precision == TGH_PREC_MIXED;
   if (p->intr) {
     if (!(cfg->r0 > 0.0 && cfg->r1 > cfg->r0))
       return fail(p, TGH_ERR_RADII, "the interior needs 0 < r_0 < r_1");

@@ -62,24 +62,51 @@ template <> struct W<8> {
 
 template <class T> __device__ __forceinline__ T ld(const double* p) { return T(__ldg(p)); }
 
+// The stencils. With T = double the sums are the reference's, term by term. With T = float
+// (the mixed form) every difference of state values is formed in FP64, where it cancels, and
+// rounded once; the weighted sum then runs in FP32. The symmetric stencils use that their
+// weights sum to zero: w_0 c + sum_k w_k (u_k + u_-k) = sum_k w_k ((u_k - c) + (u_-k - c)).
+template <class T> __host__ __device__ constexpr bool is_fp64() { return sizeof(T) == sizeof(double); }
+
 // sum_k w_k u[k s] on the antisymmetric first-derivative stencil (center weight zero)
 template <int Q, class T> __device__ __forceinline__ T st_d1(const double* p, long s) {
   T acc = T(0.0);
 #pragma unroll
-  for (int k = 1; k <= W<Q>::R; ++k) acc = fma(T(W<Q>::d1(k)), ld<T>(p + k * s) - ld<T>(p - k * s), acc);
+  for (int k = 1; k <= W<Q>::R; ++k) {
+    if constexpr (is_fp64<T>()) acc = fma(T(W<Q>::d1(k)), ld<T>(p + k * s) - ld<T>(p - k * s), acc);
+    else acc = fma(T(W<Q>::d1(k)), T(ld<double>(p + k * s) - ld<double>(p - k * s)), acc);
+  }
   return acc;
 }
 template <int Q, class T> __device__ __forceinline__ T st_d2(const double* p, long s, T c) {
-  T acc = T(W<Q>::d2(0)) * c;
+  if constexpr (is_fp64<T>()) {
+    T acc = T(W<Q>::d2(0)) * c;
 #pragma unroll
-  for (int k = 1; k <= W<Q>::R; ++k) acc = fma(T(W<Q>::d2(k)), ld<T>(p + k * s) + ld<T>(p - k * s), acc);
-  return acc;
+    for (int k = 1; k <= W<Q>::R; ++k) acc = fma(T(W<Q>::d2(k)), ld<T>(p + k * s) + ld<T>(p - k * s), acc);
+    return acc;
+  } else {
+    const double c0 = ld<double>(p);
+    T acc = T(0.0);
+#pragma unroll
+    for (int k = 1; k <= W<Q>::R; ++k)
+      acc = fma(T(W<Q>::d2(k)), T((ld<double>(p + k * s) - c0) + (ld<double>(p - k * s) - c0)), acc);
+    return acc;
+  }
 }
 template <int Q, class T> __device__ __forceinline__ T st_ko(const double* p, long s, T c) {
-  T acc = T(W<Q>::ko(0)) * c;
+  if constexpr (is_fp64<T>()) {
+    T acc = T(W<Q>::ko(0)) * c;
 #pragma unroll
-  for (int k = 1; k <= W<Q>::RD; ++k) acc = fma(T(W<Q>::ko(k)), ld<T>(p + k * s) + ld<T>(p - k * s), acc);
-  return acc;
+    for (int k = 1; k <= W<Q>::RD; ++k) acc = fma(T(W<Q>::ko(k)), ld<T>(p + k * s) + ld<T>(p - k * s), acc);
+    return acc;
+  } else {
+    const double c0 = ld<double>(p);
+    T acc = T(0.0);
+#pragma unroll
+    for (int k = 1; k <= W<Q>::RD; ++k)
+      acc = fma(T(W<Q>::ko(k)), T((ld<double>(p + k * s) - c0) + (ld<double>(p - k * s) - c0)), acc);
+    return acc;
+  }
 }
 // d_1 d_2 as the tensor product of two first-derivative stencils
 template <int Q, class T> __device__ __forceinline__ T st_mixed(const double* p, long s1, long s2) {
@@ -91,7 +118,11 @@ template <int Q, class T> __device__ __forceinline__ T st_mixed(const double* p,
     for (int e = 1; e <= W<Q>::R; ++e) {
       const double* pp = p + a * s1;
       const double* pm = p - a * s1;
-      T d = (ld<T>(pp + e * s2) - ld<T>(pp - e * s2)) - (ld<T>(pm + e * s2) - ld<T>(pm - e * s2));
+      T d;
+      if constexpr (is_fp64<T>())
+        d = (ld<T>(pp + e * s2) - ld<T>(pp - e * s2)) - (ld<T>(pm + e * s2) - ld<T>(pm - e * s2));
+      else
+        d = T((ld<double>(pp + e * s2) - ld<double>(pp - e * s2)) - (ld<double>(pm + e * s2) - ld<double>(pm - e * s2)));
       in = fma(T(W<Q>::d1(e)), d, in);
     }
     acc = fma(T(W<Q>::d1(a)), in, acc);
@@ -207,32 +238,55 @@ template <int Q, int N1S> __device__ __forceinline__ RhsArgs fixed_geometry(cons
 }
 
 // Steps 1-2 of the streaming order at one point (src/evolution.jl:258-285): the state, the
-// 30 first derivatives of h, the coefficient set and d_t h (with the dissipation).
+// 30 first derivatives of h, the coefficient set and d_t h (with the dissipation). The state
+// and the coefficient set (inverse metric, lapse, sqrt(gamma)) are FP64 in every form; the
+// derivatives and d_t h are in T (FP32 in the mixed form).
 template <int Q, bool DISS, class T>
 __device__ __forceinline__ void rhs_dt(const Case& cs, const RhsArgs& A, const double* wk, long sv,
-                                       const double* x, double inv_h, T hv[NC], T dh0[NC], T dh1[NC],
-                                       T dh2[NC], Coef<T>& C, T dth[NC], T& eh) {
+                                       const double* x, double inv_h, double hv[NC], T dh0[NC], T dh1[NC],
+                                       T dh2[NC], Coef<double>& C, T dth[NC], T& eh) {
   const long s1 = 1, s2 = A.Wd, s3 = (long)A.Wd * A.Wd;
   const T ih = T(inv_h);
   eh = T(DISS ? dissipation_rate(cs, A.t, x) * inv_h : 0.0);
 #pragma unroll
   for (int v = 0; v < NC; ++v) {
     const double* p = wk + v * sv;
-    hv[v] = ld<T>(p);
+    hv[v] = ld<double>(p);
     dh0[v] = ih * st_d1<Q, T>(p, s1);
     dh1[v] = ih * st_d1<Q, T>(p, s2);
     dh2[v] = ih * st_d1<Q, T>(p, s3);
     // the dissipation stencils read the same rows: sum them here, scale them below
-    if (DISS) dth[v] = st_ko<Q, T>(p, s1, hv[v]) + st_ko<Q, T>(p, s2, hv[v]) + st_ko<Q, T>(p, s3, hv[v]);
+    if (DISS) dth[v] = st_ko<Q, T>(p, s1, T(hv[v])) + st_ko<Q, T>(p, s2, T(hv[v])) + st_ko<Q, T>(p, s3, T(hv[v]));
   }
   metric_quantities(hv, C);
-  const T a_div = C.alpha / C.sqrtg;
+  const T a_div = T(C.alpha / C.sqrtg);
 #pragma unroll
   for (int v = 0; v < NC; ++v) {
     const double* p = wk + v * sv;
-    T s = C.beta[0] * dh0[v] + C.beta[1] * dh1[v] + C.beta[2] * dh2[v] + a_div * ld<T>(p + NC * sv);
+    T s = T(C.beta[0]) * dh0[v] + T(C.beta[1]) * dh1[v] + T(C.beta[2]) * dh2[v] + a_div * ld<T>(p + NC * sv);
     if (DISS) s = fma(eh, dth[v], s);
     dth[v] = s;
+  }
+}
+
+// the coefficient set in the right-hand side's arithmetic
+template <class T> __device__ __forceinline__ Coef<T> coef_in(const Coef<double>& C) {
+  if constexpr (is_fp64<T>()) {
+    return C;
+  } else {
+    Coef<T> c;
+#pragma unroll
+    for (int n = 0; n < NC; ++n) {
+      c.g[n] = T(C.g[n]);
+      c.gu[n] = T(C.gu[n]);
+    }
+    c.alpha = T(C.alpha);
+    c.sqrtg = T(C.sqrtg);
+#pragma unroll
+    for (int i = 0; i < 3; ++i) c.beta[i] = T(C.beta[i]);
+#pragma unroll
+    for (int i = 0; i < 6; ++i) c.gamu[i] = T(C.gamu[i]);
+    return c;
   }
 }
 
@@ -311,8 +365,8 @@ __device__ __forceinline__ void rhs_source(const Case& cs, const RhsArgs& A, int
 // branches of gh_rhs_point! (src/evolution.jl:489-695): a frozen core is finished here and
 // never reaches a stencil; a layer point combines w F - rho (u - u_exact) (+ the moving
 // target's rate), the Pi half as w * (stencil part) + coef[CF_M0 + v].
-template <int Q, bool DISS, int MODE, bool INT, int N1S>
-__global__ void __launch_bounds__(128) rhs_head_kernel(const Case cs, const RhsArgs A0) {
+template <int Q, bool DISS, int MODE, bool INT, int N1S, class T>
+__global__ void __launch_bounds__(128, is_fp64<T>() ? 1 : 3) rhs_head_kernel(const Case cs, const RhsArgs A0) {
   const RhsArgs A = fixed_geometry<Q, N1S>(A0);
   const long p = A.p0 + (long)blockIdx.x * blockDim.x + threadIdx.x;
   if (p >= A.p1) return;
@@ -377,34 +431,38 @@ __global__ void __launch_bounds__(128) rhs_head_kernel(const Case cs, const RhsA
     if (r < cs.r1) layer_profiles(cs, r, w, rho);
   }
   // d_t h first, emitted at once (in the layer r_0 <= r < r_1 combined with the target)
-  double hv[NC], dh0[NC], dh1[NC], dh2[NC], dth[NC], eh;
+  double hv[NC];
+  T dh0[NC], dh1[NC], dh2[NC], dth[NC], eh;
   Coef<double> C;
-  rhs_dt<Q, DISS, double>(cs, A, wk, sv, q.x, inv_h, hv, dh0, dh1, dh2, C, dth, eh);
+  rhs_dt<Q, DISS, T>(cs, A, wk, sv, q.x, inv_h, hv, dh0, dh1, dh2, C, dth, eh);
   const bool layer = INT && r < cs.r1;
   const bool follows = INT && core_follows(cs);
   if (!layer) {
 #pragma unroll
-    for (int v = 0; v < NC; ++v) put_dth(v, dth[v]);
+    for (int v = 0; v < NC; ++v) put_dth(v, (double)dth[v]);
   } else if (follows) {
     double hm[NC], Pm[NC], dthm[NC];
     background_state(cs, A.t, q.x, hm, Pm, dthm);
     const double om = 1.0 - w;
-    for (int v = 0; v < NC; ++v) put_dth(v, w * dth[v] + om * dthm[v] - rho * (wk[v * sv] - hm[v]));
+    for (int v = 0; v < NC; ++v) put_dth(v, w * (double)dth[v] + om * dthm[v] - rho * (wk[v * sv] - hm[v]));
   } else {
     double he[NC], Pe[NC];
     background_state(cs, A.t, q.x, he, Pe);
-    for (int v = 0; v < NC; ++v) put_dth(v, w * dth[v] - rho * (wk[v * sv] - he[v]));
+    for (int v = 0; v < NC; ++v) put_dth(v, w * (double)dth[v] - rho * (wk[v * sv] - he[v]));
   }
-  // the Pi coefficients (and the matter term), then the source
-  const double* dh[3] = {dh0, dh1, dh2};
-  store_pi_coefficients(C, dh, eh, cfo, A.npts);
-  if (A.matter) store_matter(C, A, q.b, q.ip, cfo);
-  double msrc[NC];
-  const double* D[4] = {dth, dh0, dh1, dh2};
-  rhs_source(cs, A, q.b, q.ip, q.x, hv, C, D, msrc);
+  // the Pi coefficients (and the matter term), then the source, in the form's arithmetic
+  const T* dh[3] = {dh0, dh1, dh2};
+  const Coef<T> Ct = coef_in<T>(C);
+  store_pi_coefficients(Ct, dh, eh, cfo, A.npts);
+  if (A.matter) store_matter(Ct, A, q.b, q.ip, cfo);
+  T msrc[NC], ht[NC];
+#pragma unroll
+  for (int v = 0; v < NC; ++v) ht[v] = T(hv[v]);
+  const T* D[4] = {dth, dh0, dh1, dh2};
+  rhs_source(cs, A, q.b, q.ip, q.x, ht, Ct, D, msrc);
   if (A.matter) {
 #pragma unroll
-    for (int v = 0; v < NC; ++v) msrc[v] += cfo[(CF_M0 + v) * A.npts];
+    for (int v = 0; v < NC; ++v) msrc[v] += T(cfo[(CF_M0 + v) * A.npts]);
   }
   if (!layer) {
 #pragma unroll

@@ -2,5 +2,5 @@
 #include "rhs_inst.cuh"
 
 namespace tgh {
-TGH_DEFINE_RHS_LAUNCH(4)
+TGH_DEFINE_RHS_LAUNCH(4, f64, double)
 }  // namespace tgh

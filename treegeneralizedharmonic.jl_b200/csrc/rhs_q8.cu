@@ -2,5 +2,5 @@
 #include "rhs_inst.cuh"
 
 namespace tgh {
-TGH_DEFINE_RHS_LAUNCH(8)
+TGH_DEFINE_RHS_LAUNCH(8, f64, double)
 }  // namespace tgh
