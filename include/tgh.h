@@ -180,6 +180,26 @@ int tgh_error_norm(tgh_problem* p, const double* u, double t, double* l2, double
 int tgh_max_speed_noalloc(const tgh_config* cfg, const tgh_mesh* mesh, const double* u, double t,
                           void* cuda_stream, double* lambda, char* errbuf, int errlen);
 
+/* --- derivatives (the tangent-linear plain form; forward mode along one direction) ---
+ * The reference's gradients of the masked error (the error of src/constraints.jl:311-396 against
+ * the analytic solution) with respect to the interior layer's parameters, the damping strength
+ * and the initial data, taken one direction at a time: ut is the tangent of the state u (the
+ * derivative of u along the direction), and `direction` adds one parameter's own dependence:
+ *   TGH_TAN_STATE      none (the initial data's amplitudes enter through ut alone)
+ *   TGH_TAN_RHO_MAX    the layer's rho_max
+ *   TGH_TAN_RAMP       the layer's ramp width (w_ramp and rho_ramp together)
+ *   TGH_TAN_DAMP_NEAR  the damping strength (ConstantDamping's gamma0, GaussianDamping's near)
+ * tgh_tangent_rhs: du = gh_rhs!(u, t) and dut its derivative (du agrees with tgh_gh_rhs's to
+ * roundoff).
+ * tgh_tangent_rk4_step: one plain-form RK4 step of (u, ut) together.
+ * tgh_tangent_error_norm: the masked volume-weighted L2 error of u and its derivative.
+ * FP64, one rank, no matter term, an interior that does not move and is not :pasted. */
+enum { TGH_TAN_STATE = 0, TGH_TAN_RHO_MAX = 1, TGH_TAN_RAMP = 2, TGH_TAN_DAMP_NEAR = 3 };
+int tgh_tangent_rhs(tgh_problem* p, double* du, double* dut, const double* u, const double* ut, double t,
+                    int direction);
+int tgh_tangent_rk4_step(tgh_problem* p, double* u, double* ut, double t, double dt, int direction);
+int tgh_tangent_error_norm(tgh_problem* p, const double* u, const double* ut, double t, double* l2, double* dl2);
+
 /* --- one rank per GPU (TreeAMR's distribution of a forest's blocks over the ranks of a
  * communicator, src/distributed.jl:1-22; the forest itself is on every rank) ---
  * tgh_partition: the owner rank of every leaf: per refinement level, the level's leaves in

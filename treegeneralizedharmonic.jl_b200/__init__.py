@@ -13,6 +13,7 @@ Public surface, named after the reference's:
   problem    GHProblem with prepare, rhs, gh_rhs, settle, stage_limit, step_limit, max_speed,
              initial_state, gh_dt, rk4_step, step_batched, gh_solve, error_norm
   shard      partition, exchange_plan, ShardedGHProblem (one rank per GPU)
+  gradient   MaskedErrorStudy, MaskedError: the masked error's gradient by forward-mode tangents
 """
 from . import _abi
 from .cases import (Case, gauge_wave_case, horizon_min_radius, kerr_schild_case, minkowski_case,
@@ -21,10 +22,11 @@ from .forest import Forest, gh_forest, hole_forest
 from .initialdata import fourier_modes, perturbation
 from .problem import GHProblem, fp64_peak_tflops
 from .shard import ShardedGHProblem, exchange_plan, partition
+from .gradient import MaskedError, MaskedErrorStudy
 
 __all__ = ["Case", "Forest", "GHProblem", "gauge_wave_case", "gh_forest", "hole_forest", "kerr_schild_case",
            "minkowski_case", "perturbed_minkowski_case", "shifted_minkowski_case", "horizon_min_radius",
            "fourier_modes", "perturbation", "fp64_peak_tflops", "load_library", "ShardedGHProblem",
-           "exchange_plan", "partition"]
+           "exchange_plan", "partition", "MaskedError", "MaskedErrorStudy"]
 
 load_library = _abi.load_library

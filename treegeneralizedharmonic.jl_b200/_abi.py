@@ -72,6 +72,9 @@ SIGNATURES = {
     "tgh_error_norm": (ctypes.c_int, [_VP, _VP, _D, ctypes.POINTER(_D), ctypes.POINTER(_D)]),
     "tgh_max_speed_noalloc": (ctypes.c_int, [ctypes.POINTER(Config), ctypes.POINTER(Mesh), _VP, _D, _VP,
                                              ctypes.POINTER(_D), ctypes.c_char_p, ctypes.c_int]),
+    "tgh_tangent_rhs": (ctypes.c_int, [_VP, _VP, _VP, _VP, _VP, _D, ctypes.c_int]),
+    "tgh_tangent_rk4_step": (ctypes.c_int, [_VP, _VP, _VP, _D, _D, ctypes.c_int]),
+    "tgh_tangent_error_norm": (ctypes.c_int, [_VP, _VP, _VP, _D, ctypes.POINTER(_D), ctypes.POINTER(_D)]),
     "tgh_partition": (ctypes.c_int, [ctypes.POINTER(Mesh), ctypes.c_int, _VP]),
     "tgh_shard_plan": (ctypes.c_int, [ctypes.POINTER(Config), ctypes.POINTER(Mesh), _VP, ctypes.c_int, ctypes.c_int,
                                       ctypes.c_int, _VP, _VP, _VP, _VP, ctypes.c_char_p, ctypes.c_int]),

@@ -354,6 +354,65 @@ __global__ void unpack_kernel(const HookPt* __restrict__ pts, long n, const doub
   work[(long)pt.b * NV * g.Wv + (id % NV) * g.Wv + pt.w] = buf[id];
 }
 
+// The masked error norm's sums and their tangents over the evolved primaries
+// (src/constraints.jl:311-396): per CTA sum w e^2, sum w e.de and sum w, w = h^3,
+// e = |u - u_exact| over the 20 variables.
+__global__ void error_tangent_kernel(const double* __restrict__ work, const double* __restrict__ twork,
+                                     const double* __restrict__ blk, const uint8_t* __restrict__ primary, Geo g,
+                                     long npts, const Case cs, double t, double* part) {
+  __shared__ double sh[3][128];
+  const long p = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  double a = 0.0, b = 0.0, vol = 0.0;
+  if (p < npts && primary[p]) {
+    const int bk = (int)(p / g.S);
+    const long ip = p - (long)bk * g.S;
+    const int k = (int)(ip / ((long)g.N1 * g.N1)), j = (int)((ip / g.N1) % g.N1), i = (int)(ip % g.N1);
+    double x[3];
+    point_pos(blk, bk, i, j, k, x);
+    if (cs.interior == TGH_INT_NONE || interior_radius(cs, t, x) >= cs.r1) {
+      double ex[NV];
+      exact_state(cs, t, x, ex);
+      const long o = (long)bk * NV * g.Wv + (i + g.G) + (long)g.Wd * ((j + g.G) + (long)g.Wd * (k + g.G));
+      double e2 = 0.0, ed = 0.0;
+      for (int v = 0; v < NV; ++v) {
+        const double d = work[o + v * g.Wv] - ex[v];
+        e2 = __dadd_rn(e2, __dmul_rn(d, d));
+        ed = fma(d, twork[o + v * g.Wv], ed);
+      }
+      const double h = blk[8 * bk + 3];
+      vol = h * h * h;
+      a = e2 * vol;
+      b = ed * vol;
+    }
+  }
+  sh[0][threadIdx.x] = a;
+  sh[1][threadIdx.x] = b;
+  sh[2][threadIdx.x] = vol;
+  __syncthreads();
+  for (int o = blockDim.x / 2; o > 0; o >>= 1) {
+    if (threadIdx.x < o) {
+      sh[0][threadIdx.x] += sh[0][threadIdx.x + o];
+      sh[1][threadIdx.x] += sh[1][threadIdx.x + o];
+      sh[2][threadIdx.x] += sh[2][threadIdx.x + o];
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    part[3 * blockIdx.x] = sh[0][0];
+    part[3 * blockIdx.x + 1] = sh[1][0];
+    part[3 * blockIdx.x + 2] = sh[2][0];
+  }
+}
+
+// the tangent working array's Dirichlet ghosts: the analytic data do not depend on the
+// parameters or the initial perturbation, so their tangent is zero
+__global__ void hook_zero_kernel(const HookPt* __restrict__ pts, int n, double* __restrict__ work, Geo g) {
+  const long id = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (id >= (long)n * NV) return;
+  const HookPt p = pts[id / NV];
+  work[(long)p.b * NV * g.Wv + (id % NV) * g.Wv + p.w] = 0.0;
+}
+
 // one point's analytic state (20) and gauge tuple (20), for diagnostics
 __global__ void point_physics_kernel(const Case cs, double t, const double* x, double* out) {
   exact_state(cs, t, x, out);

@@ -15,6 +15,7 @@
 #include "../../include/tgh.h"
 #include "kernels.cuh"
 #include "rhs_inst.cuh"
+#include "tangent_rhs.cuh"
 
 using namespace tgh;
 
@@ -76,6 +77,8 @@ struct tgh_problem {
   double *k = nullptr, *acc = nullptr, *y = nullptr, *u0 = nullptr;
   // batched-form buffers
   double *W1 = nullptr, *W2 = nullptr, *bacc = nullptr;
+  // tangent-linear buffers: the tangent working array, and the plain form's k, acc, y tangents
+  double *twork = nullptr, *kt = nullptr, *acct = nullptr, *yt = nullptr;
   cudaGraphExec_t gexec = nullptr;
   GraphKey gkey{0, 0, 0};
   long graph_kernels = 0;  // kernel nodes of the captured graph
@@ -704,7 +707,7 @@ void tgh_problem_destroy(tgh_problem* p) {
   }
   void* bufs[] = {p->work, p->Hsrc, p->blk, p->primary, p->runs, p->gpts, p->hooks, p->hook_cache, p->scratch,
                   p->part, p->coef,
-                  p->k, p->acc, p->y, p->u0, p->W1, p->W2, p->bacc};
+                  p->k, p->acc, p->y, p->u0, p->W1, p->W2, p->bacc, p->twork, p->kt, p->acct, p->yt};
   for (void* b : bufs)
     if (b) cudaFree(b);
   for (auto* pp : p->prol)
@@ -1140,6 +1143,114 @@ int tgh_time_rhs(tgh_problem* p, const double* u, double t, int mode, int nlaunc
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
   *ms_per_launch = ms / nlaunch;
+  return TGH_OK;
+}
+
+// ---- the tangent-linear plain form: derivatives of the right-hand side, an RK4 step and the
+// masked error along one direction (the state's tangent and, optionally, one parameter) ----
+
+static int tangent_check(tgh_problem* p, int dir) {
+  if (dir < TAN_STATE || dir > TAN_DAMP_NEAR) return fail(p, TGH_ERR_ARG, "unknown tangent direction");
+  if (p->nranks > 1) return fail(p, TGH_ERR_ARG, "the tangent-linear form runs on one rank");
+  if (p->mixed) return fail(p, TGH_ERR_ARG, "the tangent-linear form is FP64");
+  if (p->intr && (core_follows(p->cs) || p->cfg.interior == TGH_INT_PASTED))
+    return fail(p, TGH_ERR_ARG, "the tangent-linear form takes a static :damped or :frozen interior");
+  const size_t L = tgh_state_length(p), Lw = tgh_work_length(p);
+  if (!p->twork) {
+    CK(cudaMalloc(&p->twork, Lw * sizeof(double)));
+    CK(cudaMemsetAsync(p->twork, 0, Lw * sizeof(double), p->stream));
+  }
+  if (!p->kt) {
+    CK(cudaMalloc(&p->kt, L * sizeof(double)));
+    CK(cudaMalloc(&p->acct, L * sizeof(double)));
+    CK(cudaMalloc(&p->yt, L * sizeof(double)));
+  }
+  return TGH_OK;
+}
+
+// The same fill on the tangent working array: copies and prolongation are linear; the
+// Dirichlet data depend neither on the parameters nor on the initial perturbation.
+static int launch_fill_tangent(tgh_problem* p, const double* ut) {
+  const int T = 256;
+  if (p->nruns) {
+    fill_copy_kernel<<<grid_for((long)p->nruns * 32, T), T, 0, p->stream>>>(p->runs, p->nruns, ut, p->twork, p->geo);
+    CK(cudaGetLastError());
+  }
+  if (p->nhooks) {
+    hook_zero_kernel<<<grid_for((long)p->nhooks * NV, T), T, 0, p->stream>>>(p->hooks, p->nhooks, p->twork, p->geo);
+    CK(cudaGetLastError());
+  }
+  for (int l = 1; l <= p->maxlevel; ++l) {
+    if (!p->nprol[l]) continue;
+    const long n = (long)p->nprol[l] * NV;
+    switch (p->q + 2) {
+      case 4: fill_prolong_kernel<4><<<grid_for(n, T), T, 0, p->stream>>>(p->prol[l], p->nprol[l], p->twork, p->geo); break;
+      case 6: fill_prolong_kernel<6><<<grid_for(n, T), T, 0, p->stream>>>(p->prol[l], p->nprol[l], p->twork, p->geo); break;
+      case 8: fill_prolong_kernel<8><<<grid_for(n, T), T, 0, p->stream>>>(p->prol[l], p->nprol[l], p->twork, p->geo); break;
+      default: fill_prolong_kernel<10><<<grid_for(n, T), T, 0, p->stream>>>(p->prol[l], p->nprol[l], p->twork, p->geo); break;
+    }
+    CK(cudaGetLastError());
+  }
+  return TGH_OK;
+}
+
+int tgh_tangent_rhs(tgh_problem* p, double* du, double* dut, const double* u, const double* ut, double t, int dir) {
+  int s = tangent_check(p, dir);
+  if (s) return s;
+  if ((s = launch_fill(p, u, false, p->work, t))) return s;
+  if ((s = launch_fill_tangent(p, ut))) return s;
+  RhsArgs a = base_args(p, p->work, t);
+  a.du = du;
+  CK(launch_rhs_tangent(p->q, p->diss, p->intr, p->stream, p->cs, a, TanArgs{dut, dir}, (long)(p->twork - p->work)));
+  return TGH_OK;
+}
+
+int tgh_tangent_rk4_step(tgh_problem* p, double* u, double* ut, double t, double dt, int dir) {
+  int s = tangent_check(p, dir);
+  if (s) return s;
+  const size_t L = tgh_state_length(p);
+  if (!p->k) CK(cudaMalloc(&p->k, L * sizeof(double)));
+  if (!p->acc) {
+    CK(cudaMalloc(&p->acc, L * sizeof(double)));
+    CK(cudaMalloc(&p->y, L * sizeof(double)));
+  }
+  const double b16 = dt / 6.0, b13 = dt / 3.0, a12 = 0.5 * dt;
+  const double ts[4] = {t, t + 0.5 * dt, t + 0.5 * dt, t + dt};
+  const double ca[4] = {a12, a12, dt, 0.0}, cb[4] = {b16, b13, b13, b16};
+  const unsigned g = 148 * 8;
+  for (int st = 0; st < 4; ++st) {
+    const double* x = st == 0 ? u : p->y;
+    const double* xt = st == 0 ? ut : p->yt;
+    if ((s = tgh_tangent_rhs(p, p->k, p->kt, x, xt, ts[st], dir))) return s;
+    const int kind = st == 0 ? 0 : (st == 3 ? 2 : 1);
+    stage_update_kernel<<<g, 256, 0, p->stream>>>(kind, (long)L, p->k, u, p->acc, p->y, u, ca[st], cb[st]);
+    CK(cudaGetLastError());
+    stage_update_kernel<<<g, 256, 0, p->stream>>>(kind, (long)L, p->kt, ut, p->acct, p->yt, ut, ca[st], cb[st]);
+    CK(cudaGetLastError());
+  }
+  return TGH_OK;
+}
+
+int tgh_tangent_error_norm(tgh_problem* p, const double* u, const double* ut, double t, double* l2, double* dl2) {
+  int s = tangent_check(p, TAN_STATE);
+  if (s) return s;
+  if ((s = launch_fill(p, u, false, p->work, t))) return s;
+  if ((s = launch_fill_tangent(p, ut))) return s;
+  error_tangent_kernel<<<p->npart, 128, 0, p->stream>>>(p->work, p->twork, p->blk, p->primary, p->geo, p->npts, p->cs,
+                                                         t, p->part);
+  CK(cudaGetLastError());
+  std::vector<double> h(3 * (size_t)p->npart);
+  CK(cudaMemcpyAsync(h.data(), p->part, h.size() * sizeof(double), cudaMemcpyDeviceToHost, p->stream));
+  CK(cudaStreamSynchronize(p->stream));
+  double a = 0.0, b = 0.0, w = 0.0;  // summed in block order, on the host
+  for (int i = 0; i < p->npart; ++i) {
+    a += h[3 * i];
+    b += h[3 * i + 1];
+    w += h[3 * i + 2];
+  }
+  if (!(w > 0.0)) return fail(p, TGH_ERR_ARG, "no evolved point to measure the error on");
+  *l2 = std::sqrt(a / w);
+  *dl2 = *l2 > 0.0 ? (b / w) / *l2 : 0.0;
   return TGH_OK;
 }
 

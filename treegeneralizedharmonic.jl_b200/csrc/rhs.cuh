@@ -14,6 +14,7 @@
 //               working array are written, u_n read (the batched form)
 #pragma once
 #include "algebra.cuh"
+#include "tangent.cuh"
 
 namespace tgh {
 
@@ -61,25 +62,29 @@ template <> struct W<8> {
 };
 
 template <class T> __device__ __forceinline__ T ld(const double* p) { return T(__ldg(p)); }
+// in the tangent-linear kernel a working-array value comes with its tangent
+template <> __device__ __forceinline__ Tan ld<Tan>(const double* p) { return Tan(__ldg(p), __ldg(p + c_tan_off)); }
+// a value that carries no tangent (the sampled gauge source, the matter term)
+template <class T> __device__ __forceinline__ T ldk(const double* p) { return T(__ldg(p)); }
 
-// The stencils. With T = double the sums are the reference's, term by term. With T = float
-// (the mixed form) every difference of state values is formed in FP64, where it cancels, and
-// rounded once; the weighted sum then runs in FP32. The symmetric stencils use that their
-// weights sum to zero: w_0 c + sum_k w_k (u_k + u_-k) = sum_k w_k ((u_k - c) + (u_-k - c)).
-template <class T> __host__ __device__ constexpr bool is_fp64() { return sizeof(T) == sizeof(double); }
+// The stencils. With T = double (and its tangent) the sums are the reference's, term by term.
+// With T = float (the mixed form) every difference of state values is formed in FP64, where
+// it cancels, and rounded once; the weighted sum then runs in FP32. The symmetric stencils use
+// that their weights sum to zero: w_0 c + sum_k w_k (u_k + u_-k) = sum_k w_k ((u_k - c) + (u_-k - c)).
+template <class T> __host__ __device__ constexpr bool is_fp32() { return sizeof(T) == sizeof(float); }
 
 // sum_k w_k u[k s] on the antisymmetric first-derivative stencil (center weight zero)
 template <int Q, class T> __device__ __forceinline__ T st_d1(const double* p, long s) {
   T acc = T(0.0);
 #pragma unroll
   for (int k = 1; k <= W<Q>::R; ++k) {
-    if constexpr (is_fp64<T>()) acc = fma(T(W<Q>::d1(k)), ld<T>(p + k * s) - ld<T>(p - k * s), acc);
+    if constexpr (!is_fp32<T>()) acc = fma(T(W<Q>::d1(k)), ld<T>(p + k * s) - ld<T>(p - k * s), acc);
     else acc = fma(T(W<Q>::d1(k)), T(ld<double>(p + k * s) - ld<double>(p - k * s)), acc);
   }
   return acc;
 }
 template <int Q, class T> __device__ __forceinline__ T st_d2(const double* p, long s, T c) {
-  if constexpr (is_fp64<T>()) {
+  if constexpr (!is_fp32<T>()) {
     T acc = T(W<Q>::d2(0)) * c;
 #pragma unroll
     for (int k = 1; k <= W<Q>::R; ++k) acc = fma(T(W<Q>::d2(k)), ld<T>(p + k * s) + ld<T>(p - k * s), acc);
@@ -94,7 +99,7 @@ template <int Q, class T> __device__ __forceinline__ T st_d2(const double* p, lo
   }
 }
 template <int Q, class T> __device__ __forceinline__ T st_ko(const double* p, long s, T c) {
-  if constexpr (is_fp64<T>()) {
+  if constexpr (!is_fp32<T>()) {
     T acc = T(W<Q>::ko(0)) * c;
 #pragma unroll
     for (int k = 1; k <= W<Q>::RD; ++k) acc = fma(T(W<Q>::ko(k)), ld<T>(p + k * s) + ld<T>(p - k * s), acc);
@@ -119,7 +124,7 @@ template <int Q, class T> __device__ __forceinline__ T st_mixed(const double* p,
       const double* pp = p + a * s1;
       const double* pm = p - a * s1;
       T d;
-      if constexpr (is_fp64<T>())
+      if constexpr (!is_fp32<T>())
         d = (ld<T>(pp + e * s2) - ld<T>(pp - e * s2)) - (ld<T>(pm + e * s2) - ld<T>(pm - e * s2));
       else
         d = T((ld<double>(pp + e * s2) - ld<double>(pp - e * s2)) - (ld<double>(pm + e * s2) - ld<double>(pm - e * s2)));
@@ -237,21 +242,31 @@ template <int Q, int N1S> __device__ __forceinline__ RhsArgs fixed_geometry(cons
   return B;
 }
 
+// The arithmetic of the state and the coefficient set (inverse metric, lapse, sqrt(gamma)):
+// FP64 in the FP64 and the mixed form, and with its tangent in the tangent-linear kernel.
+template <class T> struct StateT {
+  using type = double;
+};
+template <> struct StateT<Tan> {
+  using type = Tan;
+};
+
 // Steps 1-2 of the streaming order at one point (src/evolution.jl:258-285): the state, the
 // 30 first derivatives of h, the coefficient set and d_t h (with the dissipation). The state
-// and the coefficient set (inverse metric, lapse, sqrt(gamma)) are FP64 in every form; the
-// derivatives and d_t h are in T (FP32 in the mixed form).
+// and the coefficient set are in StateT<T>; the derivatives and d_t h in T (FP32 in the
+// mixed form).
 template <int Q, bool DISS, class T>
 __device__ __forceinline__ void rhs_dt(const Case& cs, const RhsArgs& A, const double* wk, long sv,
-                                       const double* x, double inv_h, double hv[NC], T dh0[NC], T dh1[NC],
-                                       T dh2[NC], Coef<double>& C, T dth[NC], T& eh) {
+                                       const double* x, double inv_h, typename StateT<T>::type hv[NC], T dh0[NC],
+                                       T dh1[NC], T dh2[NC], Coef<typename StateT<T>::type>& C, T dth[NC], T& eh) {
+  using H = typename StateT<T>::type;
   const long s1 = 1, s2 = A.Wd, s3 = (long)A.Wd * A.Wd;
   const T ih = T(inv_h);
   eh = T(DISS ? dissipation_rate(cs, A.t, x) * inv_h : 0.0);
 #pragma unroll
   for (int v = 0; v < NC; ++v) {
     const double* p = wk + v * sv;
-    hv[v] = ld<double>(p);
+    hv[v] = ld<H>(p);
     dh0[v] = ih * st_d1<Q, T>(p, s1);
     dh1[v] = ih * st_d1<Q, T>(p, s2);
     dh2[v] = ih * st_d1<Q, T>(p, s3);
@@ -270,8 +285,8 @@ __device__ __forceinline__ void rhs_dt(const Case& cs, const RhsArgs& A, const d
 }
 
 // the coefficient set in the right-hand side's arithmetic
-template <class T> __device__ __forceinline__ Coef<T> coef_in(const Coef<double>& C) {
-  if constexpr (is_fp64<T>()) {
+template <class T> __device__ __forceinline__ Coef<T> coef_in(const Coef<typename StateT<T>::type>& C) {
+  if constexpr (!is_fp32<T>()) {
     return C;
   } else {
     Coef<T> c;
@@ -322,18 +337,17 @@ __device__ __forceinline__ void store_matter(const Coef<T>& C, const RhsArgs& A,
   const double* q = A.matter + (long)b * 10 * S + ip;
   T m[10], ms[NC];
 #pragma unroll
-  for (int k = 0; k < 10; ++k) m[k] = ld<T>(q + k * S);
+  for (int k = 0; k < 10; ++k) m[k] = ldk<T>(q + k * S);
   matter_source(C, m, ms);
 #pragma unroll
-  for (int v = 0; v < NC; ++v) cfo[(CF_M0 + v) * A.npts] = ms[v];
+  for (int v = 0; v < NC; ++v) cfo[(CF_M0 + v) * A.npts] = value(ms[v]);
 }
 
 // Step 3 (src/evolution.jl:286-297): the gauge source (sampled, closed-form Kerr-Schild or
 // none) and the reduced source with damping, from D[c] = d_c h (c = t, x, y, z).
 template <class T>
-__device__ __forceinline__ void rhs_source(const Case& cs, const RhsArgs& A, int b, long ip, const double* x,
-                                           const T hv[NC], const Coef<T>& C, const T* const D[4], T msrc[NC]) {
-  const T g0 = T(damping_rate(cs, A.t, x));
+__device__ __forceinline__ void rhs_source(const Case& cs, const RhsArgs& A, int b, long ip, T g0, const T hv[NC],
+                                           const Coef<T>& C, const T* const D[4], T msrc[NC]) {
   if (cs.gauge == TGH_GAUGE_NONE) {
     gh_source<T, false>(C, D, nullptr, nullptr, g0, T(cs.g2), msrc);
     return;
@@ -344,11 +358,11 @@ __device__ __forceinline__ void rhs_source(const Case& cs, const RhsArgs& A, int
     const long S = (long)A.N1 * A.N1 * A.N1;
     const double* q = A.Hsrc + (long)b * NV * S + ip;
 #pragma unroll
-    for (int a = 0; a < 4; ++a) Hl[a] = ld<T>(q + a * S);
+    for (int a = 0; a < 4; ++a) Hl[a] = ldk<T>(q + a * S);
 #pragma unroll
     for (int n = 0; n < NC; ++n) {
       const int a = prow(n), c = pcol(n);
-      dHs[n] = ld<T>(q + (4 + a + 4 * c) * S) + ld<T>(q + (4 + c + 4 * a) * S);
+      dHs[n] = ldk<T>(q + (4 + a + 4 * c) * S) + ldk<T>(q + (4 + c + 4 * a) * S);
     }
   } else {
     T dHl[4][4];
@@ -366,7 +380,7 @@ __device__ __forceinline__ void rhs_source(const Case& cs, const RhsArgs& A, int
 // never reaches a stencil; a layer point combines w F - rho (u - u_exact) (+ the moving
 // target's rate), the Pi half as w * (stencil part) + coef[CF_M0 + v].
 template <int Q, bool DISS, int MODE, bool INT, int N1S, class T>
-__global__ void __launch_bounds__(128, is_fp64<T>() ? 1 : 3) rhs_head_kernel(const Case cs, const RhsArgs A0) {
+__global__ void __launch_bounds__(128, is_fp32<T>() ? 3 : 1) rhs_head_kernel(const Case cs, const RhsArgs A0) {
   const RhsArgs A = fixed_geometry<Q, N1S>(A0);
   const long p = A.p0 + (long)blockIdx.x * blockDim.x + threadIdx.x;
   if (p >= A.p1) return;
@@ -434,6 +448,7 @@ __global__ void __launch_bounds__(128, is_fp64<T>() ? 1 : 3) rhs_head_kernel(con
   double hv[NC];
   T dh0[NC], dh1[NC], dh2[NC], dth[NC], eh;
   Coef<double> C;
+  static_assert(sizeof(typename StateT<T>::type) == sizeof(double), "the head kernel's state is FP64");
   rhs_dt<Q, DISS, T>(cs, A, wk, sv, q.x, inv_h, hv, dh0, dh1, dh2, C, dth, eh);
   const bool layer = INT && r < cs.r1;
   const bool follows = INT && core_follows(cs);
@@ -459,7 +474,7 @@ __global__ void __launch_bounds__(128, is_fp64<T>() ? 1 : 3) rhs_head_kernel(con
 #pragma unroll
   for (int v = 0; v < NC; ++v) ht[v] = T(hv[v]);
   const T* D[4] = {dth, dh0, dh1, dh2};
-  rhs_source(cs, A, q.b, q.ip, q.x, ht, Ct, D, msrc);
+  rhs_source(cs, A, q.b, q.ip, T(damping_rate(cs, A.t, q.x)), ht, Ct, D, msrc);
   if (A.matter) {
 #pragma unroll
     for (int v = 0; v < NC; ++v) msrc[v] += T(cfo[(CF_M0 + v) * A.npts]);

@@ -115,6 +115,26 @@ class GHProblem:
         self._check(self.lib.tgh_error_norm(self._h, _ptr(u), float(t), ctypes.byref(l2), ctypes.byref(li)))
         return l2.value, li.value
 
+    # ---- derivatives: the tangent-linear plain form (include/tgh.h) ----
+    TANGENTS = {"state": 0, "rho_max": 1, "ramp": 2, "damp_near": 3}
+
+    def tangent_rhs(self, du, dut, u, ut, t, direction="state"):
+        """du = gh_rhs!(u, t) and dut its derivative along (ut, direction)."""
+        self._check(self.lib.tgh_tangent_rhs(self._h, _ptr(du), _ptr(dut), _ptr(u), _ptr(ut), float(t),
+                                             self.TANGENTS[direction]))
+
+    def tangent_rk4_step(self, u, ut, t, dt, direction="state"):
+        """One plain-form RK4 step of u and of its tangent ut, in place."""
+        self._check(self.lib.tgh_tangent_rk4_step(self._h, _ptr(u), _ptr(ut), float(t), float(dt),
+                                                  self.TANGENTS[direction]))
+
+    def tangent_error_norm(self, u, ut, t):
+        """The masked L2 error of u and its derivative along ut."""
+        l2, dl2 = ctypes.c_double(), ctypes.c_double()
+        self._check(self.lib.tgh_tangent_error_norm(self._h, _ptr(u), _ptr(ut), float(t), ctypes.byref(l2),
+                                                    ctypes.byref(dl2)))
+        return l2.value, dl2.value
+
     def copy_work(self):
         w = torch.empty(self.work_length, dtype=torch.float64, device="cuda")
         self._check(self.lib.tgh_copy_work(self._h, _ptr(w)))
