@@ -99,17 +99,20 @@ __global__ void fill_hook_kernel(const HookPt* __restrict__ pts, int n, const do
   for (int v = 0; v < NV; ++v) dst[v * g.Wv] = v20[v];
   if (cache) {
 #pragma unroll
-    for (int v = 0; v < NV; ++v) cache[(long)id * NV + v] = v20[v];
+    for (int v = 0; v < NV; ++v) cache[(long)v * n + id] = v20[v];
   }
 }
 
-// the Dirichlet hook of a stationary case from the values kept by fill_hook_kernel
+// the Dirichlet hook of a stationary case from the values kept by fill_hook_kernel (variable
+// after variable, so that consecutive points read and write consecutive doubles)
 __global__ void hook_copy_kernel(const HookPt* __restrict__ pts, int n, const double* __restrict__ cache,
                                  double* __restrict__ work, Geo g) {
-  const long id = (long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (id >= (long)n * NV) return;
-  const HookPt p = pts[id / NV];
-  work[(long)p.b * NV * g.Wv + (id % NV) * g.Wv + p.w] = cache[id];
+  const int id = blockIdx.x * blockDim.x + threadIdx.x;
+  if (id >= n) return;
+  const HookPt p = pts[id];
+  double* dst = work + (long)p.b * NV * g.Wv + p.w;
+#pragma unroll
+  for (int v = 0; v < NV; ++v) dst[v * g.Wv] = cache[(long)v * n + id];
 }
 
 // tensor-product Lagrange prolongation of order P from the coarse block's filled working

@@ -450,8 +450,8 @@ static void prolong_weights(int P, double* w) {
 static int launch_hooks(tgh_problem* p, double* work, double t) {
   if (!p->nhooks) return TGH_OK;
   if (p->hook_cache && p->hook_cache_valid) {
-    hook_copy_kernel<<<grid_for((long)p->nhooks * NV, 256), 256, 0, p->stream>>>(p->hooks, p->nhooks, p->hook_cache,
-                                                                                work, p->geo);
+    hook_copy_kernel<<<grid_for(p->nhooks, 256), 256, 0, p->stream>>>(p->hooks, p->nhooks, p->hook_cache, work,
+                                                                       p->geo);
   } else {
     fill_hook_kernel<<<grid_for(p->nhooks, 128), 128, 0, p->stream>>>(p->hooks, p->nhooks, p->blk, work, p->geo,
                                                                       p->cs, t, p->hook_cache);
