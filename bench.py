@@ -293,18 +293,20 @@ def run_sharded(args, tgh, world, rank, local, case, forest, cfg, gauge, perturb
 def end_to_end(P, u0, dt, K, world, pts, stream, dist):
     """The metric through the public API with host buffers: per step the state is copied in
     from pinned host memory, stepped, and copied back, all inside the timed region. The steps
-    are independent requests, pipelined over two device buffers: step n+1's upload (one copy
-    stream) and step n-1's download (another) run while step n computes."""
+    are independent requests, pipelined over three device buffers: step n+1's upload (one copy
+    stream) and step n-1's download (another) run while step n computes, and no upload waits
+    for the download of the buffer it refills (that one was step n-2's, long finished)."""
     import torch
+    NB = 3
     uh = u0.cpu().pin_memory()
-    res_h = [torch.empty_like(uh).pin_memory() for _ in range(2)]
+    res_h = [torch.empty_like(uh).pin_memory() for _ in range(NB)]
     P.step_batched(u0.clone(), 0.0, dt, 1)  # graph for one step
     torch.cuda.synchronize()
-    ud = [torch.empty_like(u0) for _ in range(2)]
+    ud = [torch.empty_like(u0) for _ in range(NB)]
     s_in, s_out = torch.cuda.Stream(), torch.cuda.Stream()
-    ev_in = [torch.cuda.Event() for _ in range(2)]
-    ev_done = [torch.cuda.Event() for _ in range(2)]
-    ev_out = [torch.cuda.Event() for _ in range(2)]
+    ev_in = [torch.cuda.Event() for _ in range(NB)]
+    ev_done = [torch.cuda.Event() for _ in range(NB)]
+    ev_out = [torch.cuda.Event() for _ in range(NB)]
     for e in ev_out:
         e.record(stream)
     e2, e3 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -312,7 +314,7 @@ def end_to_end(P, u0, dt, K, world, pts, stream, dist):
     s_in.wait_event(e2)
     s_out.wait_event(e2)
     for n in range(K):
-        i = n % 2
+        i = n % NB
         s_in.wait_event(ev_out[i])  # buffer i's previous result has been read back
         with torch.cuda.stream(s_in):
             ud[i].copy_(uh, non_blocking=True)
@@ -336,7 +338,7 @@ def end_to_end(P, u0, dt, K, world, pts, stream, dist):
     nbytes = uh.numel() * 8
     return {"value": world * pts * K / (e2e_ms * 1e-3), "unit": "point-updates/s",
             "h2d_bytes_per_step": nbytes, "d2h_bytes_per_step": nbytes,
-            "pipelining": "step n+1's upload and step n-1's download overlap step n (two buffers, two copy streams)"}
+            "pipelining": "step n+1's upload and step n-1's download overlap step n (three buffers, two copy streams)"}
 
 
 def main():
