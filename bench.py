@@ -290,6 +290,32 @@ def run_sharded(args, tgh, world, rank, local, case, forest, cfg, gauge, perturb
     return 0
 
 
+def time_monitors(P, u, stream, reps=5):
+    """The gauge and ADM constraint monitors and the norms' fold on the workload's state: CUDA
+    events around `reps` calls each (each monitor call includes its prepare, the scatter and
+    ghost fill at t, as the reference's gh_constraint! and adm_constraint! do)."""
+    import torch
+    out = {}
+    for name, fn in (("gh_constraint", lambda: P.gh_constraint(u, 0.0)),
+                     ("adm_constraint", lambda: P.adm_constraint(u, 0.0))):
+        fn()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(reps):
+            fn()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        out[name + "_ms"] = e0.elapsed_time(e1) / reps
+    t0 = time.perf_counter()
+    n = P.constraint_norms()
+    out["norms_ms_host"] = (time.perf_counter() - t0) * 1e3
+    out["gauge_l2"] = n["gauge_l2"]
+    out["ham_l2"] = n["ham_l2"]
+    out["mom_l2"] = n["mom_l2"]
+    return out
+
+
 def end_to_end(P, u0, dt, K, world, pts, stream, dist):
     """The metric through the public API with host buffers: per step the state is copied in
     from pinned host memory, stepped, and copied back, all inside the timed region. The steps
@@ -459,6 +485,9 @@ def main():
             if len(parts) >= 3 and parts[0] == cfg["workload"] and parts[1] == "rhs_stage":
                 traffic = float(parts[2])
 
+    # the constraint monitors on the same state (their per-chunk cadence: not part of a step)
+    monitors = time_monitors(P, u0, stream)
+
     # end to end through the public API with host buffers: per step the state is copied in
     # from pinned host memory and the result copied back
     if big:
@@ -482,6 +511,7 @@ def main():
                         "peak_source": "measured FP64 FMA probe on this GPU (MEASURED_PEAKS.json has no FP64)"},
            "e2e": e2e,
            "plain_form": plain,
+           "monitors": monitors,
            "gpu_launches": launches, "clocks": ck}
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         out["cpu_baseline"] = cpu_baseline(tgh, scase, sforest, perturbed)

@@ -20,6 +20,9 @@
  *                                                          tgh_step_batched (fused, graph-captured form)
  *   error_norms / gh_error_kernel! src/constraints.jl:311-396, 716-792
  *                                                          tgh_error_norm
+ *   gh_constraint!, adm_constraint!, constraint_norms     tgh_gh_constraint,
+ *     src/constraints.jl:211-271, 432-532, 559-609, 848    tgh_adm_constraint,
+ *                                                          tgh_constraint_norms
  *
  * Conventions (all as in the reference):
  *  - The state vector holds, per block, (N+1)^3 owned points (closed blocks: both face
@@ -165,6 +168,36 @@ int tgh_step_batched(tgh_problem* p, double* u, double t, double dt, int nsteps)
 /* --- analysis (src/constraints.jl:311-396, 716-792) ---
  * masked, volume-weighted L2 and max of |u - u_exact| over the evolved primaries */
 int tgh_error_norm(tgh_problem* p, const double* u, double t, double* l2, double* linf);
+
+/* --- constraint monitors (src/constraints.jl:211-271, 432-532, 716-865) ---
+ * The monitors write the problem's diag field set: per block TGH_NDIAG slots of (N+1)^3
+ * points, slot-major like the state vector. Slots 0..3 hold the gauge constraint C_a
+ * (the reference's DIAG_CGH), 4 the ADM Hamiltonian constraint (DIAG_HAM), 5..7 the
+ * momentum constraint M_i (DIAG_MOM), 8 the mask indicator (DIAG_MASK). Each monitor
+ * first runs prepare at t (scatter and fill, as _prepare_monitor! does), so the working
+ * array is overwritten, and writes only its own slots and the mask.
+ *   mask: TGH_MASK_INTERIOR (the interior's r >= r_1; every point without an interior) or
+ *         TGH_MASK_ALL (AllPoints). A masked point holds zeros.
+ *   tgh_gh_constraint    gh_constraint!(p, u, t; mask)            src/constraints.jl:559
+ *   tgh_adm_constraint   adm_constraint!(p, u, t; mask, matter)   src/constraints.jl:584
+ *                        matter: null, or (N+1)^3 x 10 per block (rho, S_i, S_ij packed
+ *                        xx,xy,xz,yy,yz,zz), as for tgh_rhs; the constraints are then
+ *                        H - 16 pi rho and M_i - 8 pi S_i
+ *   tgh_constraint_norms constraint_norms(p; weighting, at_level) src/constraints.jl:848
+ *                        one fold over the primaries of what the monitors last wrote;
+ *                        weighting 0 = volume (h^3), 1 = points; at_level < 0: all levels.
+ *                        out[16] = gauge_l2[4], gauge_linf[4], ham_l2, ham_linf, mom_l2[3],
+ *                        mom_linf[3]; L2 = sqrt(sum u^2 w / evolved volume), 0 when nothing
+ *                        is evolved; L-infinity keeps NaN.
+ * Problems of one rank only (TGH_ERR_ARG for a shard). */
+#define TGH_NDIAG 9
+enum { TGH_MASK_INTERIOR = 0, TGH_MASK_ALL = 1 };
+int tgh_gh_constraint(tgh_problem* p, const double* u, double t, int mask);
+int tgh_adm_constraint(tgh_problem* p, const double* u, double t, int mask, const double* matter);
+int tgh_constraint_norms(tgh_problem* p, int weighting, int at_level, double* out);
+/* the diag field set: its length in doubles, and a copy of it into a device buffer */
+size_t tgh_diag_length(const tgh_problem* p);
+int tgh_copy_diag(tgh_problem* p, double* out);
 
 /* --- allocation-free speed (no counterpart in the reference) ---
  * tgh_max_speed without a problem handle, for callers that cannot allocate device memory

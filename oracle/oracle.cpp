@@ -101,6 +101,21 @@ static bool find_owner(const Problem& P, int l, const int64_t nin[3], int& leaf,
   return false;
 }
 
+// whether block b holds the primary copy of its owned point (i, j, k): the lattice point,
+// wrapped on a periodic axis (the upper periodic face is the lower one), has b as its owner
+static bool is_primary(const Problem& P, int b, int i, int j, int k) {
+  const int l = P.level[b];
+  int64_t n[3] = {(int64_t)P.corner[3 * b] + i, (int64_t)P.corner[3 * b + 1] + j, (int64_t)P.corner[3 * b + 2] + k};
+  for (int d = 0; d < 3; ++d)
+    if (P.periodic[d]) {
+      const int64_t per = (int64_t)P.cells0[d] << l;
+      n[d] %= per;
+      if (n[d] < 0) n[d] += per;
+    }
+  int leaf, loc[3];
+  return find_owner(P, l, n, leaf, loc) && leaf == b;
+}
+
 static void hook_value(const Problem& P, double t, const double x[3], double out[NV]) {
   double xc[3], dh[3][NC], dg[NC];
   P.in.core_position(t, x, xc);
@@ -536,8 +551,7 @@ static void error_norm(Problem& P, const double* u, double t, double* l2, double
         for (int i = 0; i < P.N1; ++i) {
           int64_t n[3] = {(int64_t)P.corner[3 * b] + i, (int64_t)P.corner[3 * b + 1] + j,
                           (int64_t)P.corner[3 * b + 2] + k};
-          int leaf, loc[3];
-          if (!find_owner(P, P.level[b], n, leaf, loc) || leaf != b) continue;
+          if (!is_primary(P, b, i, j, k)) continue;
           double x[3];
           P.position(P.level[b], n, x);
           if (!is_evolved(P, t, x)) continue;
@@ -557,6 +571,226 @@ static void error_norm(Problem& P, const double* u, double t, double* l2, double
   }
   *l2 = vol == 0.0 ? 0.0 : std::sqrt(s2 / vol);
   *linf = mx;
+}
+
+// ---- the constraint monitors (src/constraints.jl:211-271, 432-532) into a diag field set:
+// per block NDIAG slots of (N+1)^3 points, C_a (4), H, M_i (3), the mask indicator ----
+static const int NDIAG = 9;
+enum { DG_CGH = 0, DG_HAM = 4, DG_MOM = 5, DG_MASK = 8 };
+
+static PointCtx point_ctx(const Problem& P, int b, const int I[3], double x[3]) {
+  PointCtx c;
+  c.wk = P.work.data() + (size_t)b * NV * P.npt_work();
+  c.sv = P.npt_work();
+  c.st[0] = 1;
+  c.st[1] = P.W;
+  c.st[2] = P.W * P.W;
+  c.var = (size_t)(I[0] + P.G) + P.W * ((size_t)(I[1] + P.G) + (size_t)P.W * (I[2] + P.G));
+  int64_t n[3] = {(int64_t)P.corner[3 * b] + I[0], (int64_t)P.corner[3 * b + 1] + I[1],
+                  (int64_t)P.corner[3 * b + 2] + I[2]};
+  P.position(P.level[b], n, x);
+  return c;
+}
+
+// gh_constraint_kernel!: C_a = g_ab (Gamma^b + H^b), d_t g from the first evolution equation
+// without the dissipation; a masked point writes zeros and reads nothing
+static void gh_constraint(Problem& P, const double* u, double t, bool all, double* diag) {
+  prepare(P, u, t);
+  const size_t S = P.npt_state();
+#pragma omp parallel for schedule(dynamic) collapse(2)
+  for (int b = 0; b < P.nb; ++b)
+    for (int k = 0; k < P.N1; ++k)
+      for (int j = 0; j < P.N1; ++j)
+        for (int i = 0; i < P.N1; ++i) {
+          int I[3] = {i, j, k};
+          double x[3];
+          PointCtx c = point_ctx(P, b, I, x);
+          size_t o = (size_t)b * NDIAG * S + i + P.N1 * (j + (size_t)P.N1 * k);
+          if (!all && !is_evolved(P, t, x)) {
+            for (int a = 0; a < 4; ++a) diag[o + (DG_CGH + a) * S] = 0.0;
+            diag[o + DG_MASK * S] = 0.0;
+            continue;
+          }
+          const double inv_h = 1.0 / P.spacing(P.level[b]);
+          double hv[NC], Pv[NC], dhs[3][NC], dth[NC];
+          for (int v = 0; v < NC; ++v) {
+            hv[v] = c.wk[c.var + v * c.sv];
+            Pv[v] = c.wk[c.var + (NC + v) * c.sv];
+          }
+          for (int d = 0; d < 3; ++d)
+            for (int v = 0; v < NC; ++v) dhs[d][v] = inv_h * axis_stencil(P.st.w1, c.wk, c.var + v * c.sv, c.st[d]);
+          const double* dh[3] = {dhs[0], dhs[1], dhs[2]};
+          Coef<double> C;
+          metric_quantities(hv, C);
+          const double a_div = C.alpha / C.sqrtg;
+          for (int v = 0; v < NC; ++v)
+            dth[v] = C.beta[0] * dh[0][v] + C.beta[1] * dh[1][v] + C.beta[2] * dh[2][v] + a_div * Pv[v];
+          double Hl[4], dHl[4][4];
+          gauge_at_point<double>(P, b, I, hv, dth, dh, Hl, dHl);
+          double dgl[4][4][4], Hup[4], Cup[4];
+          for (int a = 0; a < 4; ++a)
+            for (int e = 0; e < 4; ++e)
+              for (int cc = 0; cc < 4; ++cc) dgl[a][e][cc] = cc == 0 ? dth[pairindex(a, e)] : dh[cc - 1][pairindex(a, e)];
+          for (int a = 0; a < 4; ++a) {
+            double s = C.gu4[a][0] * Hl[0];
+            for (int e = 1; e < 4; ++e) s = s + C.gu4[a][e] * Hl[e];
+            Hup[a] = s;
+          }
+          gauge_constraint_at_node(C.g4, dgl, Hup, Cup);
+          for (int a = 0; a < 4; ++a) {
+            double s = C.g4[a][0] * Cup[0];
+            for (int e = 1; e < 4; ++e) s = s + C.g4[a][e] * Cup[e];
+            diag[o + (DG_CGH + a) * S] = s;
+          }
+          diag[o + DG_MASK * S] = 1.0;
+        }
+}
+
+// adm_constraint_kernel!: every second derivative of g, the d_t d_i and d_t d_t blocks from the
+// evolution equations (d_t Pi from gh_node_rhs_expanded, source and damping included, no
+// dissipation), then the Ricci assembly; with matter, H - 16 pi rho and M_i - 8 pi S_i
+static void adm_constraint(Problem& P, const double* u, double t, bool all, const double* matter, double* diag) {
+  prepare(P, u, t);
+  const size_t S = P.npt_state();
+  static const int P3[3][3] = {{0, 1, 2}, {1, 3, 4}, {2, 4, 5}};
+#pragma omp parallel for schedule(dynamic) collapse(2)
+  for (int b = 0; b < P.nb; ++b)
+    for (int k = 0; k < P.N1; ++k)
+      for (int j = 0; j < P.N1; ++j)
+        for (int i = 0; i < P.N1; ++i) {
+          int I[3] = {i, j, k};
+          double x[3];
+          PointCtx c = point_ctx(P, b, I, x);
+          size_t o = (size_t)b * NDIAG * S + i + P.N1 * (j + (size_t)P.N1 * k);
+          if (!all && !is_evolved(P, t, x)) {
+            diag[o + DG_HAM * S] = 0.0;
+            for (int a = 0; a < 3; ++a) diag[o + (DG_MOM + a) * S] = 0.0;
+            diag[o + DG_MASK * S] = 0.0;
+            continue;
+          }
+          const double inv_h = 1.0 / P.spacing(P.level[b]);
+          const double inv_h2 = inv_h * inv_h;
+          double hv[NC], Pv[NC], dhs[3][NC], dPs[3][NC], dds[6][NC];
+          for (int v = 0; v < NC; ++v) {
+            hv[v] = c.wk[c.var + v * c.sv];
+            Pv[v] = c.wk[c.var + (NC + v) * c.sv];
+          }
+          for (int d = 0; d < 3; ++d)
+            for (int v = 0; v < NC; ++v) {
+              dhs[d][v] = inv_h * axis_stencil(P.st.w1, c.wk, c.var + v * c.sv, c.st[d]);
+              dPs[d][v] = inv_h * axis_stencil(P.st.w1, c.wk, c.var + (NC + v) * c.sv, c.st[d]);
+            }
+          static const int D1[6] = {0, 0, 0, 1, 1, 2}, D2[6] = {0, 1, 2, 1, 2, 2};
+          for (int n = 0; n < 6; ++n)
+            for (int v = 0; v < NC; ++v) {
+              size_t bh = c.var + v * c.sv;
+              dds[n][v] = inv_h2 * (D1[n] == D2[n] ? axis_stencil(P.st.w2, c.wk, bh, c.st[D1[n]])
+                                                   : mixed_stencil(P.st.w1, c.wk, bh, c.st[D1[n]], c.st[D2[n]]));
+            }
+          const double* dh[3] = {dhs[0], dhs[1], dhs[2]};
+          const double* dP[3] = {dPs[0], dPs[1], dPs[2]};
+          const double* ddh[6] = {dds[0], dds[1], dds[2], dds[3], dds[4], dds[5]};
+          Coef<double> C;
+          metric_quantities(hv, C);
+          const double a_div = C.alpha / C.sqrtg;
+          double dth0[NC];
+          for (int v = 0; v < NC; ++v)
+            dth0[v] = C.beta[0] * dh[0][v] + C.beta[1] * dh[1][v] + C.beta[2] * dh[2][v] + a_div * Pv[v];
+          double Hl[4], dHl[4][4];
+          gauge_at_point<double>(P, b, I, hv, dth0, dh, Hl, dHl);
+          const double g0 = P.pr.damping_rate(t, x);
+          double dth[NC], dtPi[NC];
+          gh_node_rhs_expanded(hv, Pv, dh, dP, ddh, Hl, dHl, g0, P.cfg.gamma2, dth, dtPi);
+          double rho = 0.0, S3[3] = {0.0, 0.0, 0.0};
+          if (matter) {
+            size_t om = (size_t)b * 10 * S + i + P.N1 * (j + (size_t)P.N1 * k);
+            double m[10];
+            for (int q = 0; q < 10; ++q) m[q] = matter[om + q * S];
+            rho = m[0];
+            S3[0] = m[1];
+            S3[1] = m[2];
+            S3[2] = m[3];
+            double Sij[3][3] = {{m[4], m[5], m[6]}, {m[5], m[7], m[8]}, {m[6], m[8], m[9]}};
+            double ms[NC];
+            matter_source(C, rho, S3, Sij, ms);
+            for (int v = 0; v < NC; ++v) dtPi[v] = dtPi[v] + ms[v];
+          }
+          const double phi = C.alpha / C.sqrtg;
+          double dtd[3][NC];
+          for (int d = 0; d < 3; ++d) {
+            double dal, dbeta[3], dsq, dgamu[3][3];
+            metric_derivatives_along(C, dh[d], dal, dbeta, dsq, dgamu);
+            const double dphi = (dal - phi * dsq) / C.sqrtg;
+            for (int v = 0; v < NC; ++v) {
+              double acc = dphi * Pv[v] + phi * dP[d][v];
+              dtd[d][v] = acc + (dbeta[0] * dh[0][v] + dbeta[1] * dh[1][v] + dbeta[2] * dh[2][v]) +
+                          (C.beta[0] * ddh[P3[d][0]][v] + C.beta[1] * ddh[P3[d][1]][v] + C.beta[2] * ddh[P3[d][2]][v]);
+            }
+          }
+          double dalt, dbt[3], dsqt, dgut[3][3], dtt[NC];
+          metric_derivatives_along(C, dth, dalt, dbt, dsqt, dgut);
+          const double dphit = (dalt - phi * dsqt) / C.sqrtg;
+          for (int v = 0; v < NC; ++v)
+            dtt[v] = dphit * Pv[v] + phi * dtPi[v] + (dbt[0] * dh[0][v] + dbt[1] * dh[1][v] + dbt[2] * dh[2][v]) +
+                     (C.beta[0] * dtd[0][v] + C.beta[1] * dtd[1][v] + C.beta[2] * dtd[2][v]);
+          const double* dd[NC] = {dtt, dtd[0], dtd[1], dtd[2], ddh[0], ddh[1], ddh[2], ddh[3], ddh[4], ddh[5]};
+          double dg[4][4][4], ddg[4][4][4][4];
+          dg4(dth, dh, dg);
+          for (int m = 0; m < 4; ++m)
+            for (int n = 0; n < 4; ++n)
+              for (int a = 0; a < 4; ++a)
+                for (int e = 0; e < 4; ++e) ddg[m][n][a][e] = dd[pairindex(m, n)][pairindex(a, e)];
+          double ham, mom[3];
+          adm_constraints_at_node(C.g4, C.gu4, C.alpha, C.beta, dg, ddg, ham, mom);
+          if (matter) {
+            const double c8 = 8.0 * M_PI;
+            ham = ham - 2.0 * (c8 * rho);
+            for (int a = 0; a < 3; ++a) mom[a] = mom[a] - c8 * S3[a];
+          }
+          diag[o + DG_HAM * S] = ham;
+          for (int a = 0; a < 3; ++a) diag[o + (DG_MOM + a) * S] = mom[a];
+          diag[o + DG_MASK * S] = 1.0;
+        }
+}
+
+static inline double nanmax(double a, double b) { return (a != a || b != b) ? NAN : (a > b ? a : b); }
+
+// diag_norms over the slots C_a .. mask (src/constraints.jl:716-778, 825-865): each lattice point
+// once, at its primary copy; weight h^3 (volume) or 1 (points), blocks of level at_level only
+// when at_level >= 0; L2 = sqrt(sum u^2 w / evolved volume), Linf the largest |u| (NaN kept).
+// out: gauge_l2[4], gauge_linf[4], ham_l2, ham_linf, mom_l2[3], mom_linf[3]
+static void constraint_norms(const Problem& P, const double* diag, bool volume, int at_level, double out[16]) {
+  const size_t S = P.npt_state();
+  double vol = 0.0, s2[8] = {0}, mx[8] = {0};
+  for (int b = 0; b < P.nb; ++b) {
+    if (at_level >= 0 && P.level[b] != at_level) continue;
+    const double h = P.spacing(P.level[b]);
+    const double w = volume ? h * h * h : 1.0;
+    for (int k = 0; k < P.N1; ++k)
+      for (int j = 0; j < P.N1; ++j)
+        for (int i = 0; i < P.N1; ++i) {
+          if (!is_primary(P, b, i, j, k)) continue;
+          size_t o = (size_t)b * NDIAG * S + i + P.N1 * (j + (size_t)P.N1 * k);
+          vol += diag[o + DG_MASK * S] * w;
+          for (int s = 0; s < 8; ++s) {
+            double uu = diag[o + s * S];
+            s2[s] += uu * uu * w;
+            mx[s] = nanmax(mx[s], std::fabs(uu));
+          }
+        }
+  }
+  double l2[8];
+  for (int s = 0; s < 8; ++s) l2[s] = vol == 0.0 ? 0.0 : std::sqrt(s2[s] / vol);
+  for (int a = 0; a < 4; ++a) {
+    out[a] = l2[DG_CGH + a];
+    out[4 + a] = mx[DG_CGH + a];
+  }
+  out[8] = l2[DG_HAM];
+  out[9] = mx[DG_HAM];
+  for (int a = 0; a < 3; ++a) {
+    out[10 + a] = l2[DG_MOM + a];
+    out[13 + a] = mx[DG_MOM + a];
+  }
 }
 
 }  // namespace orc
@@ -693,6 +927,60 @@ int orc_rk4_step(void* p, double* u, double t, double dt) {
 int orc_error_norm(void* p, const double* u, double t, double* l2, double* linf) {
   error_norm(*(Problem*)p, u, t, l2, linf);
   return TGH_OK;
+}
+size_t orc_diag_length(void* p) { Problem* P = (Problem*)p; return P->npt_state() * NDIAG * P->nb; }
+int orc_gh_constraint(void* p, const double* u, double t, int allpoints, double* diag) {
+  gh_constraint(*(Problem*)p, u, t, allpoints != 0, diag);
+  return TGH_OK;
+}
+int orc_adm_constraint(void* p, const double* u, double t, int allpoints, const double* matter, double* diag) {
+  adm_constraint(*(Problem*)p, u, t, allpoints != 0, matter, diag);
+  return TGH_OK;
+}
+int orc_constraint_norms(void* p, const double* diag, int weighting, int at_level, double* out16) {
+  constraint_norms(*(Problem*)p, diag, weighting == 0, at_level, out16);
+  return TGH_OK;
+}
+// the pointwise pieces alone, for the pins of test/constraints_tests.jl:63-158
+void orc_ddmetric(const tgh_background* bg, const double* p4, double* g16, double* dg64, double* ddg256) {
+  double g[4][4], dg[4][4][4], ddg[4][4][4][4];
+  ddmetric(*bg, p4, g, dg, ddg);
+  std::memcpy(g16, g, sizeof(g));
+  std::memcpy(dg64, dg, sizeof(dg));
+  std::memcpy(ddg256, ddg, sizeof(ddg));
+}
+void orc_adm_at_node(const double* h10, const double* dg64, const double* ddg256, double* out4) {
+  Coef<double> C;
+  metric_quantities(h10, C);
+  double dg[4][4][4], ddg[4][4][4][4], ham, mom[3];
+  std::memcpy(dg, dg64, sizeof(dg));
+  std::memcpy(ddg, ddg256, sizeof(ddg));
+  adm_constraints_at_node(C.g4, C.gu4, C.alpha, C.beta, dg, ddg, ham, mom);
+  out4[0] = ham;
+  for (int a = 0; a < 3; ++a) out4[1 + a] = mom[a];
+}
+// out: d alpha, d beta (3), d sqrt(gamma), d gamma^{jk} (9) along the direction of dg10
+void orc_metric_derivatives_along(const double* h10, const double* dg10, double* out14) {
+  Coef<double> C;
+  metric_quantities(h10, C);
+  double dal, dbeta[3], dsq, dgamu[3][3];
+  metric_derivatives_along(C, dg10, dal, dbeta, dsq, dgamu);
+  out14[0] = dal;
+  for (int j = 0; j < 3; ++j) out14[1 + j] = dbeta[j];
+  out14[4] = dsq;
+  for (int j = 0; j < 3; ++j)
+    for (int k = 0; k < 3; ++k) out14[5 + 3 * j + k] = dgamu[j][k];
+}
+// metric_derivatives at a point (three directions): d alpha (3), d beta [i][j] (9), dA [i][j][k] (27)
+void orc_metric_derivatives(const double* h10, const double* dh30, double* out39) {
+  Coef<double> C;
+  metric_quantities(h10, C);
+  const double* dh[3] = {dh30, dh30 + NC, dh30 + 2 * NC};
+  double dal[3], dbeta[3][3], dA[3][3][3];
+  metric_derivatives(C, dh, dal, dbeta, dA);
+  for (int i = 0; i < 3; ++i) out39[i] = dal[i];
+  std::memcpy(out39 + 3, dbeta, sizeof(dbeta));
+  std::memcpy(out39 + 12, dA, sizeof(dA));
 }
 
 // test/evolution_tests.jl:37-89: the expanded reference spelling at one owned point of

@@ -8,6 +8,9 @@
 //   metric_divergences, _dgu_row src/pointwise.jl:754-778
 //   gh_node_rhs_expanded         src/pointwise.jl:818-850
 //   matter_source                src/pointwise.jl:667-698
+//   metric_derivatives_along     src/pointwise.jl:530-546
+//   gauge_constraint_at_node     src/pointwise.jl:947-962
+//   adm_constraints_at_node      src/constraints.jl:136-190
 // Packed order (tt,tx,ty,tz,xx,xy,xz,yy,yz,zz); every index below is 0-based.
 // Sums are left folds in the reference's order; the file is compiled without
 // floating-point contraction so that each product is rounded, as Julia does by default.
@@ -497,6 +500,164 @@ static inline void gh_node_rhs_expanded(const T* h, const T* Pi, const T* const 
   T msrc[NC];
   gh_node_source(C, dg, Hl, dHl, g0, g2, msrc);
   for (int v = 0; v < NC; ++v) dtPi[v] = dtPi0[v] + msrc[v];
+}
+
+// src/pointwise.jl:530-546: the chain rule of metric_derivatives along one direction, with
+// d sqrt(gamma) and d gamma^{jk} returned apart (the monitors take them along time as well)
+template <class T>
+static inline void metric_derivatives_along(const Coef<T>& C, const T* dg10, T& dal, T dbeta[3], T& dsq,
+                                            T dgamu[3][3]) {
+  T gutt = C.gu4[0][0];
+  T dgl[4][4], tmp[4][4], dgu[4][4];
+  sym4(dg10, dgl);
+  for (int a = 0; a < 4; ++a)
+    for (int d = 0; d < 4; ++d) {
+      T s = C.gu4[a][0] * dgl[0][d];
+      for (int c = 1; c < 4; ++c) s = s + C.gu4[a][c] * dgl[c][d];
+      tmp[a][d] = s;
+    }
+  for (int a = 0; a < 4; ++a)
+    for (int b = 0; b < 4; ++b) {
+      T s = tmp[a][0] * C.gu4[0][b];
+      for (int d = 1; d < 4; ++d) s = s + tmp[a][d] * C.gu4[d][b];
+      dgu[a][b] = -s;
+    }
+  dal = C.alpha * C.alpha * C.alpha * dgu[0][0] / T(2);
+  for (int j = 0; j < 3; ++j) dbeta[j] = -(dgu[0][j + 1] + C.beta[j] * dgu[0][0]) / gutt;
+  T s = T(0);
+  bool first = true;
+  for (int k = 0; k < 3; ++k)
+    for (int j = 0; j < 3; ++j) {
+      T t = C.gamu[j][k] * dgl[j + 1][k + 1];
+      s = first ? t : s + t;
+      first = false;
+    }
+  dsq = C.sqrtg * s / T(2);
+  for (int j = 0; j < 3; ++j)
+    for (int k = 0; k < 3; ++k)
+      dgamu[j][k] = dgu[j + 1][k + 1] + C.beta[k] * dgu[0][j + 1] + C.beta[j] * dgu[0][k + 1] +
+                    C.beta[j] * C.beta[k] * dgu[0][0];
+}
+
+// src/pointwise.jl:947-962: C^mu = g^{ab} Gamma^mu_{ab} + H^mu, with the inverse of g formed here
+// (a general 4x4 inverse) and dgl[a][b][c] = d_c g_ab, the derivative axis last
+template <class T>
+static inline void gauge_constraint_at_node(const T g[4][4], const T dgl[4][4][4], const T Hup[4], T out[4]) {
+  T gu[4][4];
+  inv4(g, gu);
+  T Gl[4][4][4], G[4][4][4];
+  for (int a = 0; a < 4; ++a)
+    for (int b = 0; b < 4; ++b)
+      for (int c = 0; c < 4; ++c) Gl[a][b][c] = (dgl[a][c][b] + dgl[a][b][c] - dgl[b][c][a]) / T(2);
+  for (int m = 0; m < 4; ++m)
+    for (int a = 0; a < 4; ++a)
+      for (int b = 0; b < 4; ++b) {
+        T s = gu[m][0] * Gl[0][a][b];
+        for (int c = 1; c < 4; ++c) s = s + gu[m][c] * Gl[c][a][b];
+        G[m][a][b] = s;
+      }
+  for (int m = 0; m < 4; ++m) {
+    T s = T(0);
+    bool first = true;
+    for (int b = 0; b < 4; ++b)
+      for (int a = 0; a < 4; ++a) {
+        T t = gu[a][b] * G[m][a][b];
+        s = first ? t : s + t;
+        first = false;
+      }
+    out[m] = s + Hup[m];
+  }
+}
+
+// src/constraints.jl:136-190: the ADM Hamiltonian and momentum constraints from the
+// four-dimensional Ricci tensor, dg[a][b][c] = d_a g_bc and ddg[a][b][c][d] = d_a d_b g_cd
+// (derivative axes first):
+//   R_ab = d_c Gamma^c_ab - d_b Gamma^c_ca + Gamma^c_cd Gamma^d_ab - Gamma^c_bd Gamma^d_ca
+//   H = 2 R_nn + R,   M_i = -n^a (R_ai - g_ai R / 2),   n = (1, -beta) / alpha
+template <class T>
+static inline void adm_constraints_at_node(const T g4[4][4], const T gu4[4][4], T alpha, const T beta[3],
+                                           const T dg[4][4][4], const T ddg[4][4][4][4], T& ham, T mom[3]) {
+  T dgu[4][4][4];
+  for (int e = 0; e < 4; ++e) {
+    T tmp[4][4];
+    for (int a = 0; a < 4; ++a)
+      for (int d = 0; d < 4; ++d) {
+        T s = gu4[a][0] * dg[e][0][d];
+        for (int c = 1; c < 4; ++c) s = s + gu4[a][c] * dg[e][c][d];
+        tmp[a][d] = s;
+      }
+    for (int a = 0; a < 4; ++a)
+      for (int b = 0; b < 4; ++b) {
+        T s = tmp[a][0] * gu4[0][b];
+        for (int d = 1; d < 4; ++d) s = s + tmp[a][d] * gu4[d][b];
+        dgu[e][a][b] = -s;
+      }
+  }
+  T Gl[4][4][4], G4[4][4][4], Gtr[4];
+  for (int a = 0; a < 4; ++a)
+    for (int b = 0; b < 4; ++b)
+      for (int c = 0; c < 4; ++c) Gl[a][b][c] = (dg[b][a][c] + dg[c][a][b] - dg[a][b][c]) / T(2);
+  for (int a = 0; a < 4; ++a)
+    for (int b = 0; b < 4; ++b)
+      for (int c = 0; c < 4; ++c) {
+        T s = gu4[a][0] * Gl[0][b][c];
+        for (int x = 1; x < 4; ++x) s = s + gu4[a][x] * Gl[x][b][c];
+        G4[a][b][c] = s;
+      }
+  for (int d = 0; d < 4; ++d) Gtr[d] = ((G4[0][0][d] + G4[1][1][d]) + G4[2][2][d]) + G4[3][3][d];
+  T R[4][4];
+  for (int a = 0; a < 4; ++a)
+    for (int b = 0; b < 4; ++b) {
+      // A_ab = d_c Gamma^c_ab, B_ab = d_b Gamma^c_ca, each as its two sums (c fastest)
+      T A1 = T(0), A2 = T(0), B1 = T(0), B2 = T(0);
+      bool first = true;
+      for (int d = 0; d < 4; ++d)
+        for (int c = 0; c < 4; ++c) {
+          T a1 = dgu[c][c][d] * Gl[d][a][b];
+          T a2 = gu4[c][d] * (ddg[c][a][d][b] + ddg[c][b][d][a] - ddg[c][d][a][b]) / T(2);
+          T b1 = dgu[b][c][d] * Gl[d][c][a];
+          T b2 = gu4[c][d] * (ddg[b][c][d][a] + ddg[b][a][d][c] - ddg[b][d][c][a]) / T(2);
+          A1 = first ? a1 : A1 + a1;
+          A2 = first ? a2 : A2 + a2;
+          B1 = first ? b1 : B1 + b1;
+          B2 = first ? b2 : B2 + b2;
+          first = false;
+        }
+      T q1 = Gtr[0] * G4[0][a][b];
+      for (int d = 1; d < 4; ++d) q1 = q1 + Gtr[d] * G4[d][a][b];
+      T q2 = T(0);
+      first = true;
+      for (int d = 0; d < 4; ++d)
+        for (int c = 0; c < 4; ++c) {
+          T t = G4[c][b][d] * G4[d][c][a];
+          q2 = first ? t : q2 + t;
+          first = false;
+        }
+      R[a][b] = (A1 + A2) - (B1 + B2) + q1 - q2;
+    }
+  T Rs = T(0);
+  bool first = true;
+  for (int b = 0; b < 4; ++b)
+    for (int a = 0; a < 4; ++a) {
+      T t = gu4[a][b] * R[a][b];
+      Rs = first ? t : Rs + t;
+      first = false;
+    }
+  T n[4] = {T(1) / alpha, -beta[0] / alpha, -beta[1] / alpha, -beta[2] / alpha};
+  T Rnn = T(0);
+  first = true;
+  for (int b = 0; b < 4; ++b)
+    for (int a = 0; a < 4; ++a) {
+      T t = R[a][b] * n[a] * n[b];
+      Rnn = first ? t : Rnn + t;
+      first = false;
+    }
+  ham = T(2) * Rnn + Rs;
+  for (int i = 0; i < 3; ++i) {
+    T s = n[0] * (R[0][i + 1] - g4[0][i + 1] * Rs / T(2));
+    for (int a = 1; a < 4; ++a) s = s + n[a] * (R[a][i + 1] - g4[a][i + 1] * Rs / T(2));
+    mom[i] = -s;
+  }
 }
 
 // src/pointwise.jl:667-698; Sij symmetric, S3 = (S_x, S_y, S_z)

@@ -200,6 +200,29 @@ static inline void dmetric(const tgh_background& bg, const double p[4], double g
     }
 }
 
+// ddmetric: g, dg[a][b][c] = d_a g_bc and ddg[a][b][c][d] = d_a d_b g_cd (derivative axes
+// first) by nested duals: what the ADM pin of test/constraints_tests.jl:63-108 feeds the
+// Ricci assembly
+static inline void ddmetric(const tgh_background& bg, const double p[4], double g[4][4], double dg[4][4][4],
+                            double ddg[4][4][4][4]) {
+  Ddd x[4];
+  for (int i = 0; i < 4; ++i) {
+    x[i] = Ddd(p[i]);
+    x[i].v.d[i] = 1.0;
+    x[i].d[i] = Dd(1.0);
+  }
+  Ddd gg[4][4];
+  metric_eval(bg, x, gg);
+  for (int a = 0; a < 4; ++a)
+    for (int b = 0; b < 4; ++b) {
+      g[a][b] = gg[a][b].v.v;
+      for (int c = 0; c < 4; ++c) {
+        dg[c][a][b] = gg[a][b].v.d[c];
+        for (int e = 0; e < 4; ++e) ddg[e][c][a][b] = gg[a][b].d[e].d[c];
+      }
+    }
+}
+
 // src/initialdata.jl:1681-1694: h, Pi, dh from one dual pass (and d_t g)
 static inline void background_state(const tgh_background& bg, double t, const double x[3],
                                     double h[NC], double Pi[NC], double dh[3][NC],

@@ -58,6 +58,14 @@ class Oracle:
             "orc_gauge_source_grad": (None, [ctypes.POINTER(abi.Background), _DP, _DP, _DP]),
             "orc_algebraic_gauge_source": (None, [_D, _DP, _DP, _DP, _DP, _DP, _DP, _DP]),
             "orc_smoothstep": (_D, [_D]),
+            "orc_diag_length": (ctypes.c_size_t, [_VP]),
+            "orc_gh_constraint": (ctypes.c_int, [_VP, _DP, _D, ctypes.c_int, _DP]),
+            "orc_adm_constraint": (ctypes.c_int, [_VP, _DP, _D, ctypes.c_int, _DP, _DP]),
+            "orc_constraint_norms": (ctypes.c_int, [_VP, _DP, ctypes.c_int, ctypes.c_int, _DP]),
+            "orc_ddmetric": (None, [ctypes.POINTER(abi.Background), _DP, _DP, _DP, _DP]),
+            "orc_adm_at_node": (None, [_DP, _DP, _DP, _DP]),
+            "orc_metric_derivatives_along": (None, [_DP, _DP, _DP]),
+            "orc_metric_derivatives": (None, [_DP, _DP, _DP]),
         }
         for name, (res, args) in sig.items():
             fn = getattr(lib, name)
@@ -132,6 +140,32 @@ class Oracle:
         self.lib.orc_algebraic_gauge_source(M, *[_dp(x) for x in a], _dp(Hl), _dp(dHl))
         return Hl, dHl.reshape(4, 4)
 
+    def ddmetric(self, bg, p):
+        """g, dg[a,b,c] = d_a g_bc and ddg[a,b,c,d] = d_a d_b g_cd of a background, analytic."""
+        g, dg, ddg = np.zeros(16), np.zeros(64), np.zeros(256)
+        self.lib.orc_ddmetric(ctypes.byref(bg), _dp(np.ascontiguousarray(p, dtype=float)), _dp(g), _dp(dg),
+                              _dp(ddg))
+        return g.reshape(4, 4), dg.reshape(4, 4, 4), ddg.reshape(4, 4, 4, 4)
+
+    def adm_at_node(self, h, dg, ddg):
+        """(H, M_x, M_y, M_z) of the Ricci assembly at one point of offset h."""
+        out = np.zeros(4)
+        a = [np.ascontiguousarray(x, dtype=float).ravel() for x in (h, dg, ddg)]
+        self.lib.orc_adm_at_node(*[_dp(x) for x in a], _dp(out))
+        return out
+
+    def metric_derivatives_along(self, h, dg10):
+        out = np.zeros(14)
+        a = [np.ascontiguousarray(x, dtype=float) for x in (h, dg10)]
+        self.lib.orc_metric_derivatives_along(_dp(a[0]), _dp(a[1]), _dp(out))
+        return dict(dal=out[0], dbeta=out[1:4], dsq=out[4], dgamu=out[5:14].reshape(3, 3))
+
+    def metric_derivatives(self, h, dh):
+        out = np.zeros(39)
+        a = [np.ascontiguousarray(x, dtype=float).ravel() for x in (h, dh)]
+        self.lib.orc_metric_derivatives(_dp(a[0]), _dp(a[1]), _dp(out))
+        return dict(dal=out[:3], dbeta=out[3:12].reshape(3, 3), dA=out[12:39].reshape(3, 3, 3))
+
 
 class OracleProblem:
     def __init__(self, orc, case, forest, q, margin_check=False):
@@ -196,6 +230,25 @@ class OracleProblem:
     def host_rhs_at(self, b, i, j, k, t):
         out = np.zeros(20)
         self.lib.orc_host_rhs_at(self.h, b, i, j, k, t, _dp(out))
+        return out
+
+    # the constraint monitors: a diag field set of 9 slots per block (C_a, H, M_i, mask)
+    def diag(self):
+        return np.zeros(int(self.lib.orc_diag_length(self.h)))
+
+    def gh_constraint(self, diag, u, t, allpoints=False):
+        self.lib.orc_gh_constraint(self.h, _dp(u), t, int(allpoints), _dp(diag))
+        return diag
+
+    def adm_constraint(self, diag, u, t, allpoints=False, matter=None):
+        self.lib.orc_adm_constraint(self.h, _dp(u), t, int(allpoints), _dp(matter) if matter is not None else None,
+                                    _dp(diag))
+        return diag
+
+    def constraint_norms(self, diag, weighting="volume", at_level=None):
+        out = np.zeros(16)
+        self.lib.orc_constraint_norms(self.h, _dp(diag), 0 if weighting == "volume" else 1,
+                                      -1 if at_level is None else int(at_level), _dp(out))
         return out
 
     def rhs_scale(self, b, i, j, k):

@@ -17,6 +17,8 @@ DAMP_CONSTANT, DAMP_GAUSSIAN = range(2)
 DISS_CONSTANT, DISS_HORIZON = range(2)
 INT_NONE, INT_DAMPED, INT_FROZEN, INT_PASTED = range(4)
 PREC_FP64, PREC_MIXED = range(2)
+MASK_INTERIOR, MASK_ALL = range(2)
+NDIAG = 9  # diag slots per block: C_a (0..3), H (4), M_i (5..7), mask (8)
 
 D3 = ctypes.c_double * 3
 D4 = ctypes.c_double * 4
@@ -70,6 +72,11 @@ SIGNATURES = {
     "tgh_rk4_step": (ctypes.c_int, [_VP, _VP, _D, _D]),
     "tgh_step_batched": (ctypes.c_int, [_VP, _VP, _D, _D, ctypes.c_int]),
     "tgh_error_norm": (ctypes.c_int, [_VP, _VP, _D, ctypes.POINTER(_D), ctypes.POINTER(_D)]),
+    "tgh_gh_constraint": (ctypes.c_int, [_VP, _VP, _D, ctypes.c_int]),
+    "tgh_adm_constraint": (ctypes.c_int, [_VP, _VP, _D, ctypes.c_int, _VP]),
+    "tgh_constraint_norms": (ctypes.c_int, [_VP, ctypes.c_int, ctypes.c_int, ctypes.POINTER(_D)]),
+    "tgh_diag_length": (ctypes.c_size_t, [_VP]),
+    "tgh_copy_diag": (ctypes.c_int, [_VP, _VP]),
     "tgh_max_speed_noalloc": (ctypes.c_int, [ctypes.POINTER(Config), ctypes.POINTER(Mesh), _VP, _D, _VP,
                                              ctypes.POINTER(_D), ctypes.c_char_p, ctypes.c_int]),
     "tgh_tangent_rhs": (ctypes.c_int, [_VP, _VP, _VP, _VP, _VP, _D, ctypes.c_int]),

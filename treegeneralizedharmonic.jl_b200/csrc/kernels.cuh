@@ -171,10 +171,6 @@ __global__ void stage_update_kernel(int kind, long n, const double* __restrict__
   }
 }
 
-__device__ __forceinline__ bool evolved(const Case& cs, double t, const double* x) {
-  return cs.interior == TGH_INT_NONE ? true : interior_radius(cs, t, x) >= cs.r1;
-}
-
 // The speed lambda = alpha sqrt(tr gamma^{ij}) + |beta| at every evolved owned point and the
 // count of non-finite evolved values; reduced per CTA into scratch[0] (max, as the ordered
 // bits of a non-negative double or a NaN) and scratch[1] (count).

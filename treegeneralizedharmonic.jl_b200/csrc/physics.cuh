@@ -447,6 +447,10 @@ TGH_HD double interior_radius(const Case& c, double t, const double* x) {
          d3 = x[2] - (c.ic0[2] + t * c.iv[2]);
   return sqrt(d1 * d1 + d2 * d2 + d3 * d3);
 }
+// is_evolved(mask, x) of the interior's mask: r >= r_1 (src/constraints.jl:74-75)
+TGH_HD bool evolved(const Case& cs, double t, const double* x) {
+  return cs.interior == TGH_INT_NONE ? true : interior_radius(cs, t, x) >= cs.r1;
+}
 TGH_HD bool core_follows(const Case& c) {
   return c.interior == TGH_INT_DAMPED && !(c.iv[0] == 0.0 && c.iv[1] == 0.0 && c.iv[2] == 0.0);
 }

@@ -14,6 +14,7 @@
 
 #include "../../include/tgh.h"
 #include "kernels.cuh"
+#include "monitors.cuh"
 #include "rhs_inst.cuh"
 #include "tangent_rhs.cuh"
 
@@ -71,6 +72,8 @@ struct tgh_problem {
   std::vector<int> nprol;
   unsigned long long* scratch = nullptr;  // speed reduction: max bits, non-finite count
   double* part = nullptr;                 // error-norm partials + result
+  double* diag = nullptr;                 // the monitors' diag field set (NDIAG slots per block)
+  double* dpart = nullptr;                // constraint-norm partials (17 per CTA) + the fold
   double* coef = nullptr;                 // per-point coefficients between the two RHS kernels
   int npart = 0;
   // plain-form RK4 buffers (state layout)
@@ -675,6 +678,9 @@ static int setup_device(tgh_problem* p) {
   CK(cudaMalloc(&p->coef, (size_t)NCOEF * p->npts * sizeof(double)));
   p->npart = (int)grid_for(p->npts, 128);
   CK(cudaMalloc(&p->part, (3 * (size_t)p->npart + 2) * sizeof(double)));
+  CK(cudaMalloc(&p->diag, (size_t)NDIAG * p->npts * sizeof(double)));
+  CK(cudaMemsetAsync(p->diag, 0, (size_t)NDIAG * p->npts * sizeof(double), p->stream));
+  CK(cudaMalloc(&p->dpart, (17 * (size_t)p->npart + 17) * sizeof(double)));
   double wp[10] = {0};
   prolong_weights(p->q + 2, wp);
   CK(cudaMemcpyToSymbol(c_wprol, wp, sizeof(wp)));
@@ -706,7 +712,7 @@ void tgh_problem_destroy(tgh_problem* p) {
     if (x.recv) cudaFree(x.recv);
   }
   void* bufs[] = {p->work, p->Hsrc, p->blk, p->primary, p->runs, p->gpts, p->hooks, p->hook_cache, p->scratch,
-                  p->part, p->coef,
+                  p->part, p->coef, p->diag, p->dpart,
                   p->k, p->acc, p->y, p->u0, p->W1, p->W2, p->bacc, p->twork, p->kt, p->acct, p->yt};
   for (void* b : bufs)
     if (b) cudaFree(b);
@@ -726,6 +732,82 @@ int tgh_copy_work(tgh_problem* p, double* dst) {
 }
 
 int tgh_prepare(tgh_problem* p, const double* u, double t) { return launch_fill(p, u, false, p->work, t); }
+
+// ---- the constraint monitors (src/constraints.jl:535-609) ----
+static int monitor_prepare(tgh_problem* p, const double* u, double t, int mask, MonArgs& a) {
+  if (p->nranks > 1) return fail(p, TGH_ERR_ARG, "the constraint monitors run on a problem of one rank");
+  if (mask != TGH_MASK_INTERIOR && mask != TGH_MASK_ALL)
+    return fail(p, TGH_ERR_ARG, "mask must be TGH_MASK_INTERIOR or TGH_MASK_ALL");
+  int s = tgh_prepare(p, u, t);
+  if (s) return s;
+  std::memset(&a, 0, sizeof(a));
+  a.work = p->work;
+  a.Hsrc = p->Hsrc;
+  a.blk = p->blk;
+  a.diag = p->diag;
+  a.N1 = p->N1;
+  a.Wd = p->Wd;
+  a.G = p->G;
+  a.all = mask == TGH_MASK_ALL;
+  a.S = p->S;
+  a.Wv = p->Wv;
+  a.npts = p->npts;
+  a.t = t;
+  return TGH_OK;
+}
+
+int tgh_gh_constraint(tgh_problem* p, const double* u, double t, int mask) {
+  MonArgs a;
+  int s = monitor_prepare(p, u, t, mask, a);
+  if (s) return s;
+  CK(launch_gauge_constraint(p->q, p->stream, p->cs, a));
+  return TGH_OK;
+}
+
+int tgh_adm_constraint(tgh_problem* p, const double* u, double t, int mask, const double* matter) {
+  MonArgs a;
+  int s = monitor_prepare(p, u, t, mask, a);
+  if (s) return s;
+  a.matter = matter;
+  CK(launch_adm_constraint(p->q, p->stream, p->cs, a));
+  return TGH_OK;
+}
+
+int tgh_constraint_norms(tgh_problem* p, int weighting, int at_level, double* out) {
+  if (weighting != 0 && weighting != 1) return fail(p, TGH_ERR_ARG, "weighting must be 0 (volume) or 1 (points)");
+  if (at_level > 20) return fail(p, TGH_ERR_ARG, "at_level out of range");
+  const double hsel = at_level < 0 ? -1.0 : std::ldexp(p->h0, -at_level);
+  diag_norms_kernel<<<p->npart, 128, 0, p->stream>>>(p->diag, p->primary, p->blk, p->S, p->npts, weighting == 0,
+                                                      hsel, p->dpart);
+  CK(cudaGetLastError());
+  double* fold = p->dpart + 17 * (size_t)p->npart;
+  diag_norms_fold_kernel<<<1, 32, 0, p->stream>>>(p->dpart, p->npart, fold);
+  CK(cudaGetLastError());
+  double r[17];
+  CK(cudaMemcpyAsync(r, fold, sizeof(r), cudaMemcpyDeviceToHost, p->stream));
+  CK(cudaStreamSynchronize(p->stream));
+  const double vol = r[0];
+  double l2[8];
+  for (int s = 0; s < 8; ++s) l2[s] = vol == 0.0 ? 0.0 : std::sqrt(r[1 + s] / vol);
+  for (int a = 0; a < 4; ++a) {
+    out[a] = l2[DG_CGH + a];
+    out[4 + a] = r[9 + DG_CGH + a];
+  }
+  out[8] = l2[DG_HAM];
+  out[9] = r[9 + DG_HAM];
+  for (int a = 0; a < 3; ++a) {
+    out[10 + a] = l2[DG_MOM + a];
+    out[13 + a] = r[9 + DG_MOM + a];
+  }
+  return TGH_OK;
+}
+
+size_t tgh_diag_length(const tgh_problem* p) { return (size_t)NDIAG * p->npts; }
+
+int tgh_copy_diag(tgh_problem* p, double* out) {
+  CK(cudaMemcpyAsync(out, p->diag, (size_t)NDIAG * p->npts * sizeof(double), cudaMemcpyDeviceToDevice, p->stream));
+  return TGH_OK;
+}
 
 int tgh_rhs(tgh_problem* p, double* du, double t, const double* matter) {
   RhsArgs a = base_args(p, p->work, t);

@@ -115,6 +115,38 @@ class GHProblem:
         self._check(self.lib.tgh_error_norm(self._h, _ptr(u), float(t), ctypes.byref(l2), ctypes.byref(li)))
         return l2.value, li.value
 
+    # ---- the constraint monitors (src/constraints.jl:559-609, 848-865) ----
+    MASKS = {"interior": _abi.MASK_INTERIOR, "all": _abi.MASK_ALL}
+
+    def gh_constraint(self, u, t, mask="interior"):
+        """The gauge constraint C_a of u at t into the diag field set (gh_constraint!)."""
+        self._check(self.lib.tgh_gh_constraint(self._h, _ptr(u), float(t), self.MASKS[mask]))
+        return self
+
+    def adm_constraint(self, u, t, mask="interior", matter=None):
+        """The ADM Hamiltonian and momentum constraints of u at t into the diag field set
+        (adm_constraint!); matter as for rhs."""
+        self._check(self.lib.tgh_adm_constraint(self._h, _ptr(u), float(t), self.MASKS[mask], _ptr(matter)))
+        return self
+
+    def constraint_norms(self, weighting="volume", at_level=None):
+        """constraint_norms(p; weighting, at_level): masked L2 and Linf of what the monitors last
+        wrote, over the primaries (each lattice point once)."""
+        if weighting not in ("volume", "points"):
+            raise ValueError("weighting is 'volume' or 'points'")
+        out = (ctypes.c_double * 16)()
+        self._check(self.lib.tgh_constraint_norms(self._h, 0 if weighting == "volume" else 1,
+                                                  -1 if at_level is None else int(at_level), out))
+        o = list(out)
+        return {"gauge_l2": o[0:4], "gauge_linf": o[4:8], "ham_l2": o[8], "ham_linf": o[9],
+                "mom_l2": o[10:13], "mom_linf": o[13:16]}
+
+    def diag(self):
+        """A copy of the diag field set: per block 9 slots of (N+1)^3 points (C_a, H, M_i, mask)."""
+        d = torch.empty(int(self.lib.tgh_diag_length(self._h)), dtype=torch.float64, device="cuda")
+        self._check(self.lib.tgh_copy_diag(self._h, _ptr(d)))
+        return d
+
     # ---- derivatives: the tangent-linear plain form (include/tgh.h) ----
     TANGENTS = {"state": 0, "rho_max": 1, "ramp": 2, "damp_near": 3}
 
