@@ -47,6 +47,10 @@ PKG = ROOT / "treegeneralizedharmonic.jl_b200"
 FLOP_PER_POINT_RHS = {"none": 7909, "sampled": 7957, "algebraic": 8283}
 # RK4 stage arithmetic per point-update: 20 variables x (4 + 4 + 4 + 2) flops
 FLOP_PER_POINT_STAGES = 280
+# The constraint monitors' algorithmic FP64 operations per point at q = 4, counted the same way
+# (orc_count_monitor_flops) at the same points: the gauge constraint and the ADM constraints.
+FLOP_PER_POINT_MONITORS = {"gauge": {"none": 2169, "sampled": 2159, "algebraic": 2490},
+                           "adm": {"none": 16387, "sampled": 16447, "algebraic": 16783}}
 
 
 def load_package():
@@ -161,9 +165,20 @@ def cpu_baseline(tgh, sample_case, sample_forest, perturbed, seconds=10.0, max_s
         steps += 1
     el = time.perf_counter() - t0
     pts = sample_forest.points() * steps
+    # the constraint monitors on the sample's state, once each (prepare included, as on the GPU)
+    d = O.diag()
+    t1 = time.perf_counter()
+    O.gh_constraint(d, u, 0.0)
+    t2 = time.perf_counter()
+    O.adm_constraint(d, u, 0.0)
+    t3 = time.perf_counter()
+    npts = (sample_forest.N + 1) ** 3 * sample_forest.nblocks
+    monitors = {"gh_constraint_ms": (t2 - t1) * 1e3, "adm_constraint_ms": (t3 - t2) * 1e3,
+                "points": npts, "unit": "ms per call on the sample"}
     return {"value": pts / el, "unit": "point-updates/s", "cores": int(orc.lib.orc_get_threads()), "kind": "port",
             "sample": f"{sample_forest.nblocks} blocks of {sample_forest.N}^3 of the same configuration, "
-                      f"{steps} RK4 step(s), {el:.2f} s"}
+                      f"{steps} RK4 step(s), {el:.2f} s",
+            "monitors": monitors}
 
 
 def run_reference(args):
@@ -290,13 +305,15 @@ def run_sharded(args, tgh, world, rank, local, case, forest, cfg, gauge, perturb
     return 0
 
 
-def time_monitors(P, u, stream, reps=5):
+def time_monitors(P, u, stream, gauge, n1pts, peak, reps=5):
     """The gauge and ADM constraint monitors and the norms' fold on the workload's state: CUDA
-    events around `reps` calls each (each monitor call includes its prepare, the scatter and
-    ghost fill at t, as the reference's gh_constraint! and adm_constraint! do)."""
+    events around `reps` calls each. Each monitor call includes its prepare (the scatter and
+    ghost fill at t, as the reference's gh_constraint! and adm_constraint! do); the prepare is
+    timed alone too, and the kernel's time is the difference."""
     import torch
     out = {}
-    for name, fn in (("gh_constraint", lambda: P.gh_constraint(u, 0.0)),
+    for name, fn in (("prepare", lambda: P.prepare(u, 0.0)),
+                     ("gh_constraint", lambda: P.gh_constraint(u, 0.0)),
                      ("adm_constraint", lambda: P.adm_constraint(u, 0.0))):
         fn()
         torch.cuda.synchronize()
@@ -307,6 +324,13 @@ def time_monitors(P, u, stream, reps=5):
         e1.record(stream)
         torch.cuda.synchronize()
         out[name + "_ms"] = e0.elapsed_time(e1) / reps
+    for name, key in (("gauge", "gh_constraint"), ("adm", "adm_constraint")):
+        kms = out[key + "_ms"] - out["prepare_ms"]
+        flops = FLOP_PER_POINT_MONITORS[name][gauge]
+        out[name + "_kernel_ms"] = kms
+        out[name + "_flop_per_point"] = flops
+        out[name + "_tflops"] = flops * n1pts / (kms * 1e-3) / 1e12
+        out[name + "_frac"] = out[name + "_tflops"] / peak
     t0 = time.perf_counter()
     n = P.constraint_norms()
     out["norms_ms_host"] = (time.perf_counter() - t0) * 1e3
@@ -379,6 +403,9 @@ def main():
                     help="mixed: FP32 stencil sums and algebra on the FP64 state (one GPU)")
     ap.add_argument("--shard", action="store_true",
                     help="run the sharded step (the --gpus N > 1 path) even on one GPU")
+    ap.add_argument("--monitors-only", action="store_true",
+                    help="time only the constraint monitors (each with its prepare) on the workload's state: "
+                         "the command the monitor profiles are taken with")
     ap.add_argument("--rhs-only", action="store_true",
                     help="time only the right-hand side (head + Pi kernels, stage epilogue) on the workload: "
                          "the command the kernel profiles are taken with")
@@ -409,6 +436,12 @@ def main():
         ms = P.time_rhs(u0, 0.0, mode=1, nlaunch=2)
         print(json.dumps({"workload": cfg["workload"], "rhs_ms_per_launch": ms,
                           "points_per_launch": (forest.N + 1) ** 3 * forest.nblocks}))
+        P.close()
+        return 0
+    if args.monitors_only:
+        n1 = (forest.N + 1) ** 3 * forest.nblocks
+        print(json.dumps({"workload": cfg["workload"], "points": n1,
+                          **time_monitors(P, u0, stream, gauge, n1, tgh.fp64_peak_tflops(), reps=1)}))
         P.close()
         return 0
     lam = P.max_speed(u0, 0.0)
@@ -486,7 +519,7 @@ def main():
                 traffic = float(parts[2])
 
     # the constraint monitors on the same state (their per-chunk cadence: not part of a step)
-    monitors = time_monitors(P, u0, stream)
+    monitors = time_monitors(P, u0, stream, gauge, n1pts, peak)
 
     # end to end through the public API with host buffers: per step the state is copied in
     # from pinned host memory and the result copied back

@@ -592,8 +592,136 @@ static PointCtx point_ctx(const Problem& P, int b, const int I[3], double x[3]) 
   return c;
 }
 
-// gh_constraint_kernel!: C_a = g_ab (Gamma^b + H^b), d_t g from the first evolution equation
-// without the dissipation; a masked point writes zeros and reads nothing
+// gh_constraint_kernel! at one owned point: C_a = g_ab (Gamma^b + H^b), d_t g from the first
+// evolution equation without the dissipation
+template <class T>
+static void gh_constraint_point(const Problem& P, const PointCtx& c, int b, const int I[3], T out[4]) {
+  const T inv_h = T(1.0) / T(P.spacing(P.level[b]));
+  T hv[NC], Pv[NC], dhs[3][NC], dth[NC];
+  for (int v = 0; v < NC; ++v) {
+    hv[v] = T(c.wk[c.var + v * c.sv]);
+    Pv[v] = T(c.wk[c.var + (NC + v) * c.sv]);
+  }
+  for (int d = 0; d < 3; ++d)
+    for (int v = 0; v < NC; ++v) dhs[d][v] = inv_h * axis_stencil<T>(P.st.w1, c.wk, c.var + v * c.sv, c.st[d]);
+  const T* dh[3] = {dhs[0], dhs[1], dhs[2]};
+  Coef<T> C;
+  metric_quantities(hv, C);
+  const T a_div = C.alpha / C.sqrtg;
+  for (int v = 0; v < NC; ++v)
+    dth[v] = C.beta[0] * dh[0][v] + C.beta[1] * dh[1][v] + C.beta[2] * dh[2][v] + a_div * Pv[v];
+  T Hl[4], dHl[4][4];
+  gauge_at_point<T>(P, b, I, hv, dth, dh, Hl, dHl);
+  T dgl[4][4][4], Hup[4], Cup[4];
+  for (int a = 0; a < 4; ++a)
+    for (int e = 0; e < 4; ++e)
+      for (int cc = 0; cc < 4; ++cc) dgl[a][e][cc] = cc == 0 ? dth[pairindex(a, e)] : dh[cc - 1][pairindex(a, e)];
+  for (int a = 0; a < 4; ++a) {
+    T s = C.gu4[a][0] * Hl[0];
+    for (int e = 1; e < 4; ++e) s = s + C.gu4[a][e] * Hl[e];
+    Hup[a] = s;
+  }
+  gauge_constraint_at_node(C.g4, dgl, Hup, Cup);
+  for (int a = 0; a < 4; ++a) {
+    T s = C.g4[a][0] * Cup[0];
+    for (int e = 1; e < 4; ++e) s = s + C.g4[a][e] * Cup[e];
+    out[a] = s;
+  }
+}
+
+// adm_constraint_kernel! at one owned point: every second derivative of g, the d_t d_i and
+// d_t d_t blocks from the evolution equations (d_t Pi from gh_node_rhs_expanded, source and
+// damping included, no dissipation), then the Ricci assembly; with matter, H - 16 pi rho and
+// M_i - 8 pi S_i. out: H, M_x, M_y, M_z
+template <class T>
+static void adm_constraint_point(const Problem& P, const PointCtx& c, int b, const int I[3], const double x[3],
+                                 double t, const double* matter, T out[4]) {
+  static const int P3[3][3] = {{0, 1, 2}, {1, 3, 4}, {2, 4, 5}};
+  static const int D1[6] = {0, 0, 0, 1, 1, 2}, D2[6] = {0, 1, 2, 1, 2, 2};
+  const T inv_h = T(1.0) / T(P.spacing(P.level[b]));
+  const T inv_h2 = inv_h * inv_h;
+  T hv[NC], Pv[NC], dhs[3][NC], dPs[3][NC], dds[6][NC];
+  for (int v = 0; v < NC; ++v) {
+    hv[v] = T(c.wk[c.var + v * c.sv]);
+    Pv[v] = T(c.wk[c.var + (NC + v) * c.sv]);
+  }
+  for (int d = 0; d < 3; ++d)
+    for (int v = 0; v < NC; ++v) {
+      dhs[d][v] = inv_h * axis_stencil<T>(P.st.w1, c.wk, c.var + v * c.sv, c.st[d]);
+      dPs[d][v] = inv_h * axis_stencil<T>(P.st.w1, c.wk, c.var + (NC + v) * c.sv, c.st[d]);
+    }
+  for (int n = 0; n < 6; ++n)
+    for (int v = 0; v < NC; ++v) {
+      size_t bh = c.var + v * c.sv;
+      dds[n][v] = inv_h2 * (D1[n] == D2[n] ? axis_stencil<T>(P.st.w2, c.wk, bh, c.st[D1[n]])
+                                           : mixed_stencil<T>(P.st.w1, c.wk, bh, c.st[D1[n]], c.st[D2[n]]));
+    }
+  const T* dh[3] = {dhs[0], dhs[1], dhs[2]};
+  const T* dP[3] = {dPs[0], dPs[1], dPs[2]};
+  const T* ddh[6] = {dds[0], dds[1], dds[2], dds[3], dds[4], dds[5]};
+  Coef<T> C;
+  metric_quantities(hv, C);
+  const T a_div = C.alpha / C.sqrtg;
+  T dth0[NC];
+  for (int v = 0; v < NC; ++v)
+    dth0[v] = C.beta[0] * dh[0][v] + C.beta[1] * dh[1][v] + C.beta[2] * dh[2][v] + a_div * Pv[v];
+  T Hl[4], dHl[4][4];
+  gauge_at_point<T>(P, b, I, hv, dth0, dh, Hl, dHl);
+  const T g0 = T(P.pr.damping_rate(t, x));
+  T dth[NC], dtPi[NC];
+  gh_node_rhs_expanded(hv, Pv, dh, dP, ddh, Hl, dHl, g0, T(P.cfg.gamma2), dth, dtPi);
+  double rho = 0.0, S3[3] = {0.0, 0.0, 0.0};
+  if constexpr (std::is_same<T, double>::value) if (matter) {
+    const size_t S = P.npt_state();
+    size_t om = (size_t)b * 10 * S + I[0] + P.N1 * (I[1] + (size_t)P.N1 * I[2]);
+    double m[10];
+    for (int q = 0; q < 10; ++q) m[q] = matter[om + q * S];
+    rho = m[0];
+    S3[0] = m[1];
+    S3[1] = m[2];
+    S3[2] = m[3];
+    double Sij[3][3] = {{m[4], m[5], m[6]}, {m[5], m[7], m[8]}, {m[6], m[8], m[9]}};
+    double ms[NC];
+    matter_source(C, rho, S3, Sij, ms);
+    for (int v = 0; v < NC; ++v) dtPi[v] = dtPi[v] + ms[v];
+  }
+  const T phi = C.alpha / C.sqrtg;
+  T dtd[3][NC];
+  for (int d = 0; d < 3; ++d) {
+    T dal, dbeta[3], dsq, dgamu[3][3];
+    metric_derivatives_along(C, dh[d], dal, dbeta, dsq, dgamu);
+    const T dphi = (dal - phi * dsq) / C.sqrtg;
+    for (int v = 0; v < NC; ++v) {
+      T acc = dphi * Pv[v] + phi * dP[d][v];
+      dtd[d][v] = acc + (dbeta[0] * dh[0][v] + dbeta[1] * dh[1][v] + dbeta[2] * dh[2][v]) +
+                  (C.beta[0] * ddh[P3[d][0]][v] + C.beta[1] * ddh[P3[d][1]][v] + C.beta[2] * ddh[P3[d][2]][v]);
+    }
+  }
+  T dalt, dbt[3], dsqt, dgut[3][3], dtt[NC];
+  metric_derivatives_along(C, dth, dalt, dbt, dsqt, dgut);
+  const T dphit = (dalt - phi * dsqt) / C.sqrtg;
+  for (int v = 0; v < NC; ++v)
+    dtt[v] = dphit * Pv[v] + phi * dtPi[v] + (dbt[0] * dh[0][v] + dbt[1] * dh[1][v] + dbt[2] * dh[2][v]) +
+             (C.beta[0] * dtd[0][v] + C.beta[1] * dtd[1][v] + C.beta[2] * dtd[2][v]);
+  const T* dd[NC] = {dtt, dtd[0], dtd[1], dtd[2], ddh[0], ddh[1], ddh[2], ddh[3], ddh[4], ddh[5]};
+  T dg[4][4][4], ddg[4][4][4][4];
+  dg4(dth, dh, dg);
+  for (int m = 0; m < 4; ++m)
+    for (int n = 0; n < 4; ++n)
+      for (int a = 0; a < 4; ++a)
+        for (int e = 0; e < 4; ++e) ddg[m][n][a][e] = dd[pairindex(m, n)][pairindex(a, e)];
+  T ham, mom[3];
+  adm_constraints_at_node(C.g4, C.gu4, C.alpha, C.beta, dg, ddg, ham, mom);
+  if constexpr (std::is_same<T, double>::value) if (matter) {
+    const double c8 = 8.0 * M_PI;
+    ham = ham - 2.0 * (c8 * rho);
+    for (int a = 0; a < 3; ++a) mom[a] = mom[a] - c8 * S3[a];
+  }
+  out[0] = ham;
+  for (int a = 0; a < 3; ++a) out[1 + a] = mom[a];
+}
+
+// the monitors over every owned point; a masked point writes zeros and reads nothing
 static void gh_constraint(Problem& P, const double* u, double t, bool all, double* diag) {
   prepare(P, u, t);
   const size_t S = P.npt_state();
@@ -603,153 +731,33 @@ static void gh_constraint(Problem& P, const double* u, double t, bool all, doubl
       for (int j = 0; j < P.N1; ++j)
         for (int i = 0; i < P.N1; ++i) {
           int I[3] = {i, j, k};
-          double x[3];
+          double x[3], out[4] = {0.0, 0.0, 0.0, 0.0};
           PointCtx c = point_ctx(P, b, I, x);
           size_t o = (size_t)b * NDIAG * S + i + P.N1 * (j + (size_t)P.N1 * k);
-          if (!all && !is_evolved(P, t, x)) {
-            for (int a = 0; a < 4; ++a) diag[o + (DG_CGH + a) * S] = 0.0;
-            diag[o + DG_MASK * S] = 0.0;
-            continue;
-          }
-          const double inv_h = 1.0 / P.spacing(P.level[b]);
-          double hv[NC], Pv[NC], dhs[3][NC], dth[NC];
-          for (int v = 0; v < NC; ++v) {
-            hv[v] = c.wk[c.var + v * c.sv];
-            Pv[v] = c.wk[c.var + (NC + v) * c.sv];
-          }
-          for (int d = 0; d < 3; ++d)
-            for (int v = 0; v < NC; ++v) dhs[d][v] = inv_h * axis_stencil(P.st.w1, c.wk, c.var + v * c.sv, c.st[d]);
-          const double* dh[3] = {dhs[0], dhs[1], dhs[2]};
-          Coef<double> C;
-          metric_quantities(hv, C);
-          const double a_div = C.alpha / C.sqrtg;
-          for (int v = 0; v < NC; ++v)
-            dth[v] = C.beta[0] * dh[0][v] + C.beta[1] * dh[1][v] + C.beta[2] * dh[2][v] + a_div * Pv[v];
-          double Hl[4], dHl[4][4];
-          gauge_at_point<double>(P, b, I, hv, dth, dh, Hl, dHl);
-          double dgl[4][4][4], Hup[4], Cup[4];
-          for (int a = 0; a < 4; ++a)
-            for (int e = 0; e < 4; ++e)
-              for (int cc = 0; cc < 4; ++cc) dgl[a][e][cc] = cc == 0 ? dth[pairindex(a, e)] : dh[cc - 1][pairindex(a, e)];
-          for (int a = 0; a < 4; ++a) {
-            double s = C.gu4[a][0] * Hl[0];
-            for (int e = 1; e < 4; ++e) s = s + C.gu4[a][e] * Hl[e];
-            Hup[a] = s;
-          }
-          gauge_constraint_at_node(C.g4, dgl, Hup, Cup);
-          for (int a = 0; a < 4; ++a) {
-            double s = C.g4[a][0] * Cup[0];
-            for (int e = 1; e < 4; ++e) s = s + C.g4[a][e] * Cup[e];
-            diag[o + (DG_CGH + a) * S] = s;
-          }
-          diag[o + DG_MASK * S] = 1.0;
+          const bool keep = all || is_evolved(P, t, x);
+          if (keep) gh_constraint_point<double>(P, c, b, I, out);
+          for (int a = 0; a < 4; ++a) diag[o + (DG_CGH + a) * S] = out[a];
+          diag[o + DG_MASK * S] = keep ? 1.0 : 0.0;
         }
 }
 
-// adm_constraint_kernel!: every second derivative of g, the d_t d_i and d_t d_t blocks from the
-// evolution equations (d_t Pi from gh_node_rhs_expanded, source and damping included, no
-// dissipation), then the Ricci assembly; with matter, H - 16 pi rho and M_i - 8 pi S_i
 static void adm_constraint(Problem& P, const double* u, double t, bool all, const double* matter, double* diag) {
   prepare(P, u, t);
   const size_t S = P.npt_state();
-  static const int P3[3][3] = {{0, 1, 2}, {1, 3, 4}, {2, 4, 5}};
 #pragma omp parallel for schedule(dynamic) collapse(2)
   for (int b = 0; b < P.nb; ++b)
     for (int k = 0; k < P.N1; ++k)
       for (int j = 0; j < P.N1; ++j)
         for (int i = 0; i < P.N1; ++i) {
           int I[3] = {i, j, k};
-          double x[3];
+          double x[3], out[4] = {0.0, 0.0, 0.0, 0.0};
           PointCtx c = point_ctx(P, b, I, x);
           size_t o = (size_t)b * NDIAG * S + i + P.N1 * (j + (size_t)P.N1 * k);
-          if (!all && !is_evolved(P, t, x)) {
-            diag[o + DG_HAM * S] = 0.0;
-            for (int a = 0; a < 3; ++a) diag[o + (DG_MOM + a) * S] = 0.0;
-            diag[o + DG_MASK * S] = 0.0;
-            continue;
-          }
-          const double inv_h = 1.0 / P.spacing(P.level[b]);
-          const double inv_h2 = inv_h * inv_h;
-          double hv[NC], Pv[NC], dhs[3][NC], dPs[3][NC], dds[6][NC];
-          for (int v = 0; v < NC; ++v) {
-            hv[v] = c.wk[c.var + v * c.sv];
-            Pv[v] = c.wk[c.var + (NC + v) * c.sv];
-          }
-          for (int d = 0; d < 3; ++d)
-            for (int v = 0; v < NC; ++v) {
-              dhs[d][v] = inv_h * axis_stencil(P.st.w1, c.wk, c.var + v * c.sv, c.st[d]);
-              dPs[d][v] = inv_h * axis_stencil(P.st.w1, c.wk, c.var + (NC + v) * c.sv, c.st[d]);
-            }
-          static const int D1[6] = {0, 0, 0, 1, 1, 2}, D2[6] = {0, 1, 2, 1, 2, 2};
-          for (int n = 0; n < 6; ++n)
-            for (int v = 0; v < NC; ++v) {
-              size_t bh = c.var + v * c.sv;
-              dds[n][v] = inv_h2 * (D1[n] == D2[n] ? axis_stencil(P.st.w2, c.wk, bh, c.st[D1[n]])
-                                                   : mixed_stencil(P.st.w1, c.wk, bh, c.st[D1[n]], c.st[D2[n]]));
-            }
-          const double* dh[3] = {dhs[0], dhs[1], dhs[2]};
-          const double* dP[3] = {dPs[0], dPs[1], dPs[2]};
-          const double* ddh[6] = {dds[0], dds[1], dds[2], dds[3], dds[4], dds[5]};
-          Coef<double> C;
-          metric_quantities(hv, C);
-          const double a_div = C.alpha / C.sqrtg;
-          double dth0[NC];
-          for (int v = 0; v < NC; ++v)
-            dth0[v] = C.beta[0] * dh[0][v] + C.beta[1] * dh[1][v] + C.beta[2] * dh[2][v] + a_div * Pv[v];
-          double Hl[4], dHl[4][4];
-          gauge_at_point<double>(P, b, I, hv, dth0, dh, Hl, dHl);
-          const double g0 = P.pr.damping_rate(t, x);
-          double dth[NC], dtPi[NC];
-          gh_node_rhs_expanded(hv, Pv, dh, dP, ddh, Hl, dHl, g0, P.cfg.gamma2, dth, dtPi);
-          double rho = 0.0, S3[3] = {0.0, 0.0, 0.0};
-          if (matter) {
-            size_t om = (size_t)b * 10 * S + i + P.N1 * (j + (size_t)P.N1 * k);
-            double m[10];
-            for (int q = 0; q < 10; ++q) m[q] = matter[om + q * S];
-            rho = m[0];
-            S3[0] = m[1];
-            S3[1] = m[2];
-            S3[2] = m[3];
-            double Sij[3][3] = {{m[4], m[5], m[6]}, {m[5], m[7], m[8]}, {m[6], m[8], m[9]}};
-            double ms[NC];
-            matter_source(C, rho, S3, Sij, ms);
-            for (int v = 0; v < NC; ++v) dtPi[v] = dtPi[v] + ms[v];
-          }
-          const double phi = C.alpha / C.sqrtg;
-          double dtd[3][NC];
-          for (int d = 0; d < 3; ++d) {
-            double dal, dbeta[3], dsq, dgamu[3][3];
-            metric_derivatives_along(C, dh[d], dal, dbeta, dsq, dgamu);
-            const double dphi = (dal - phi * dsq) / C.sqrtg;
-            for (int v = 0; v < NC; ++v) {
-              double acc = dphi * Pv[v] + phi * dP[d][v];
-              dtd[d][v] = acc + (dbeta[0] * dh[0][v] + dbeta[1] * dh[1][v] + dbeta[2] * dh[2][v]) +
-                          (C.beta[0] * ddh[P3[d][0]][v] + C.beta[1] * ddh[P3[d][1]][v] + C.beta[2] * ddh[P3[d][2]][v]);
-            }
-          }
-          double dalt, dbt[3], dsqt, dgut[3][3], dtt[NC];
-          metric_derivatives_along(C, dth, dalt, dbt, dsqt, dgut);
-          const double dphit = (dalt - phi * dsqt) / C.sqrtg;
-          for (int v = 0; v < NC; ++v)
-            dtt[v] = dphit * Pv[v] + phi * dtPi[v] + (dbt[0] * dh[0][v] + dbt[1] * dh[1][v] + dbt[2] * dh[2][v]) +
-                     (C.beta[0] * dtd[0][v] + C.beta[1] * dtd[1][v] + C.beta[2] * dtd[2][v]);
-          const double* dd[NC] = {dtt, dtd[0], dtd[1], dtd[2], ddh[0], ddh[1], ddh[2], ddh[3], ddh[4], ddh[5]};
-          double dg[4][4][4], ddg[4][4][4][4];
-          dg4(dth, dh, dg);
-          for (int m = 0; m < 4; ++m)
-            for (int n = 0; n < 4; ++n)
-              for (int a = 0; a < 4; ++a)
-                for (int e = 0; e < 4; ++e) ddg[m][n][a][e] = dd[pairindex(m, n)][pairindex(a, e)];
-          double ham, mom[3];
-          adm_constraints_at_node(C.g4, C.gu4, C.alpha, C.beta, dg, ddg, ham, mom);
-          if (matter) {
-            const double c8 = 8.0 * M_PI;
-            ham = ham - 2.0 * (c8 * rho);
-            for (int a = 0; a < 3; ++a) mom[a] = mom[a] - c8 * S3[a];
-          }
-          diag[o + DG_HAM * S] = ham;
-          for (int a = 0; a < 3; ++a) diag[o + (DG_MOM + a) * S] = mom[a];
-          diag[o + DG_MASK * S] = 1.0;
+          const bool keep = all || is_evolved(P, t, x);
+          if (keep) adm_constraint_point<double>(P, c, b, I, x, t, matter, out);
+          diag[o + DG_HAM * S] = out[0];
+          for (int a = 0; a < 3; ++a) diag[o + (DG_MOM + a) * S] = out[1 + a];
+          diag[o + DG_MASK * S] = keep ? 1.0 : 0.0;
         }
 }
 
@@ -1222,6 +1230,24 @@ int orc_count_flops(void* p, double t, long* out) {
     P.err = e.what();
     return TGH_ERR_ARG;
   }
+  out[0] = Cnt::nadd;
+  out[1] = Cnt::nmul;
+  out[2] = Cnt::ndiv;
+  out[3] = Cnt::nsqrt;
+  return TGH_OK;
+}
+
+// The same count for a constraint monitor at that point (which = 0: the gauge constraint,
+// 1: the ADM constraints, vacuum), on a prepared problem.
+int orc_count_monitor_flops(void* p, double t, int which, long* out) {
+  Problem& P = *(Problem*)p;
+  const int I[3] = {P.N / 2, P.N / 2, P.N / 2};
+  double x[3];
+  PointCtx c = point_ctx(P, 0, I, x);
+  Cnt::nadd = Cnt::nmul = Cnt::ndiv = Cnt::nsqrt = 0;
+  Cnt r[4];
+  if (which == 0) gh_constraint_point<Cnt>(P, c, 0, I, r);
+  else adm_constraint_point<Cnt>(P, c, 0, I, x, t, nullptr, r);
   out[0] = Cnt::nadd;
   out[1] = Cnt::nmul;
   out[2] = Cnt::ndiv;

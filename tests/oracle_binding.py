@@ -66,6 +66,8 @@ class Oracle:
             "orc_adm_at_node": (None, [_DP, _DP, _DP, _DP]),
             "orc_metric_derivatives_along": (None, [_DP, _DP, _DP]),
             "orc_metric_derivatives": (None, [_DP, _DP, _DP]),
+            "orc_count_flops": (ctypes.c_int, [_VP, _D, ctypes.POINTER(ctypes.c_long)]),
+            "orc_count_monitor_flops": (ctypes.c_int, [_VP, _D, ctypes.c_int, ctypes.POINTER(ctypes.c_long)]),
         }
         for name, (res, args) in sig.items():
             fn = getattr(lib, name)
@@ -244,6 +246,17 @@ class OracleProblem:
         self.lib.orc_adm_constraint(self.h, _dp(u), t, int(allpoints), _dp(matter) if matter is not None else None,
                                     _dp(diag))
         return diag
+
+    def count_flops(self, t, monitor=None):
+        """Algorithmic FP64 operations at the centre of block 0 of the prepared problem: the
+        right-hand side, or monitor "gauge" / "adm" (adds + multiplies + divides + roots)."""
+        out = (ctypes.c_long * 4)()
+        if monitor is None:
+            st = self.lib.orc_count_flops(self.h, t, out)
+        else:
+            st = self.lib.orc_count_monitor_flops(self.h, t, {"gauge": 0, "adm": 1}[monitor], out)
+        assert st == 0
+        return sum(out)
 
     def constraint_norms(self, diag, weighting="volume", at_level=None):
         out = np.zeros(16)

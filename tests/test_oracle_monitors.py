@@ -132,6 +132,52 @@ def test_both_monitors_converge_at_order_q_on_a_curved_background(tgh, oracle):
         assert vals == sorted(vals, reverse=True)
 
 
+def _bench_constants():
+    import importlib.util
+    from pathlib import Path
+    spec = importlib.util.spec_from_file_location("bench_constants", Path(__file__).resolve().parent.parent / "bench.py")
+    mod = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mod)
+    return mod
+
+
+def _first_block(tgh, case, level, h):
+    """A one-block problem whose block is the workload's first: same point, same spacing."""
+    lo = tuple(case.box[d][0] for d in range(3))
+    box = tuple((lo[d], lo[d] + 32 * h) for d in range(3))
+    c = tgh.cases.Case(case.background, box, (False,) * 3, case.eps_ko, case.gamma0, case.gamma2, case.interior,
+                       case.gauge, case.ks_source, case.M)
+    return c, tgh.gh_forest(c, 32, 1)
+
+
+def test_flop_constants_are_the_oracle_counts(tgh, oracle):
+    # the numerators of the bench's rooflines, counted by the oracle at the centre of each
+    # workload's first block (the static hole, the Fourier modes, the hierarchy's level-1 corner)
+    bench = _bench_constants()
+    ks = tgh.kerr_schild_case(M=1.0, a=0.7, halfwidth=8.0, r0=0.8, r1=1.3, rho_max=4.0, variant="damped",
+                              gauge="sampled", eps_ko=0.5)
+    c, f = _first_block(tgh, ks, 0, 0.125)
+    O = oracle.problem(c, f, 4)
+    O.prepare(O.initial_state(O.statevector(), 0.0), 0.0)
+    assert O.count_flops(0.0) == bench.FLOP_PER_POINT_RHS["sampled"]
+    assert O.count_flops(0.0, "gauge") == bench.FLOP_PER_POINT_MONITORS["gauge"]["sampled"]
+    assert O.count_flops(0.0, "adm") == bench.FLOP_PER_POINT_MONITORS["adm"]["sampled"]
+    fm = tgh.perturbed_minkowski_case()
+    f = tgh.gh_forest(fm, 32, 2)
+    O = oracle.problem(fm, f, 4)
+    O.prepare(O.initial_state(O.statevector(), 0.0) + tgh.perturbation(f, amplitude=1e-4), 0.0)
+    assert O.count_flops(0.0) == bench.FLOP_PER_POINT_RHS["none"]
+    assert O.count_flops(0.0, "gauge") == bench.FLOP_PER_POINT_MONITORS["gauge"]["none"]
+    assert O.count_flops(0.0, "adm") == bench.FLOP_PER_POINT_MONITORS["adm"]["none"]
+    hk = tgh.kerr_schild_case(M=1.0, a=0.7, v=0.1, halfwidth=40.0, r0=0.8, r1=1.3, rho_max=4.0, variant="damped",
+                              gauge="algebraic", eps_ko=0.5)
+    c, f = _first_block(tgh, hk, 1, 80.0 / 128 / 2)
+    O = oracle.problem(c, f, 4)
+    O.prepare(O.initial_state(O.statevector(), 0.0), 0.0)
+    assert O.count_flops(0.0, "gauge") == bench.FLOP_PER_POINT_MONITORS["gauge"]["algebraic"]
+    assert O.count_flops(0.0, "adm") == bench.FLOP_PER_POINT_MONITORS["adm"]["algebraic"]
+
+
 @pytest.mark.parametrize("periodic", [True, False])
 def test_the_norms_count_each_lattice_point_once(tgh, oracle, periodic):
     # A block holds both face planes; the fold reads every point at its primary copy, the

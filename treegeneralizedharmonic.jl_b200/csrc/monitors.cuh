@@ -353,7 +353,7 @@ __device__ __forceinline__ double nan_max(double a, double b) { return (a != a |
 // CTA the evolved volume (mask x weight), per slot the sum of squares x weight and the largest
 // magnitude; weight h^3 (volume) or 1 (points); with hsel > 0 only the blocks of spacing hsel
 // (one refinement level: every spacing is h0 2^-l, exactly).
-// part: per CTA 17 values (volume, 8 sums, 8 maxima), folded in CTA order on the host.
+// part: 17 rows (volume, 8 sums, 8 maxima) of one value per CTA, folded in a fixed order.
 static __global__ void __launch_bounds__(128) diag_norms_kernel(const double* __restrict__ diag,
                                                                 const uint8_t* __restrict__ primary,
                                                                 const double* __restrict__ blk, long S, long npts,
@@ -391,22 +391,26 @@ static __global__ void __launch_bounds__(128) diag_norms_kernel(const double* __
     }
     __syncthreads();
   }
-  if (threadIdx.x == 0) {
-#pragma unroll
-    for (int n = 0; n < 17; ++n) part[17 * blockIdx.x + n] = sh[n][0];
-  }
+  if (threadIdx.x < 17) part[(long)threadIdx.x * gridDim.x + blockIdx.x] = sh[threadIdx.x][0];
 }
 
-// the CTA partials folded in CTA order, one thread per quantity (deterministic)
-static __global__ void diag_norms_fold_kernel(const double* __restrict__ part, int npart, double* out) {
-  const int n = threadIdx.x;
-  if (n >= 17) return;
+// the CTA partials folded, one CTA per quantity: each thread a strided run, then a tree, in the
+// same order every time (deterministic)
+static __global__ void __launch_bounds__(256) diag_norms_fold_kernel(const double* __restrict__ part, int npart,
+                                                                     double* out) {
+  __shared__ double sh[256];
+  const int n = blockIdx.x;
+  const bool sum = n < 9;
+  const double* q = part + (long)n * npart;
   double acc = 0.0;
-  for (int c = 0; c < npart; ++c) {
-    const double v = part[17 * (long)c + n];
-    acc = n < 9 ? acc + v : nan_max(acc, v);
+  for (int c = threadIdx.x; c < npart; c += 256) acc = sum ? acc + q[c] : nan_max(acc, q[c]);
+  sh[threadIdx.x] = acc;
+  __syncthreads();
+  for (int o = 128; o > 0; o >>= 1) {
+    if (threadIdx.x < o) sh[threadIdx.x] = sum ? sh[threadIdx.x] + sh[threadIdx.x + o] : nan_max(sh[threadIdx.x], sh[threadIdx.x + o]);
+    __syncthreads();
   }
-  out[n] = acc;
+  if (threadIdx.x == 0) out[n] = sh[0];
 }
 
 cudaError_t launch_gauge_constraint(int q, cudaStream_t s, const Case& cs, const MonArgs& a);

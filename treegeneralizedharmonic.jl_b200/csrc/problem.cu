@@ -781,7 +781,7 @@ int tgh_constraint_norms(tgh_problem* p, int weighting, int at_level, double* ou
                                                       hsel, p->dpart);
   CK(cudaGetLastError());
   double* fold = p->dpart + 17 * (size_t)p->npart;
-  diag_norms_fold_kernel<<<1, 32, 0, p->stream>>>(p->dpart, p->npart, fold);
+  diag_norms_fold_kernel<<<17, 256, 0, p->stream>>>(p->dpart, p->npart, fold);
   CK(cudaGetLastError());
   double r[17];
   CK(cudaMemcpyAsync(r, fold, sizeof(r), cudaMemcpyDeviceToHost, p->stream));
