@@ -173,7 +173,8 @@ int tgh_error_norm(tgh_problem* p, const double* u, double t, double* l2, double
  * The monitors write the problem's diag field set: per block TGH_NDIAG slots of (N+1)^3
  * points, slot-major like the state vector. Slots 0..3 hold the gauge constraint C_a
  * (the reference's DIAG_CGH), 4 the ADM Hamiltonian constraint (DIAG_HAM), 5..7 the
- * momentum constraint M_i (DIAG_MOM), 8 the mask indicator (DIAG_MASK). Each monitor
+ * momentum constraint M_i (DIAG_MOM), 8 the mask indicator (DIAG_MASK), 9 the refinement
+ * indicator tau (DIAG_TAU, written by tgh_tau below). Each monitor
  * first runs prepare at t (scatter and fill, as _prepare_monitor! does), so the working
  * array is overwritten, and writes only its own slots and the mask.
  *   mask: TGH_MASK_INTERIOR (the interior's r >= r_1; every point without an interior) or
@@ -190,11 +191,27 @@ int tgh_error_norm(tgh_problem* p, const double* u, double t, double* l2, double
  *                        mom_linf[3]; L2 = sqrt(sum u^2 w / evolved volume), 0 when nothing
  *                        is evolved; L-infinity keeps NaN.
  * Problems of one rank only (TGH_ERR_ARG for a shard). */
-#define TGH_NDIAG 9
+#define TGH_NDIAG 10
 enum { TGH_MASK_INTERIOR = 0, TGH_MASK_ALL = 1 };
 int tgh_gh_constraint(tgh_problem* p, const double* u, double t, int mask);
 int tgh_adm_constraint(tgh_problem* p, const double* u, double t, int mask, const double* matter);
 int tgh_constraint_norms(tgh_problem* p, int weighting, int at_level, double* out);
+
+/* --- the refinement indicator (src/refinement.jl:170-400, 738-796) ---
+ * tgh_tau: prepare at t, then field_scales (the largest |h_v| over the evolved owned points,
+ *   one per component), then the masked Loehner indicator at every owned point into diag
+ *   slot 9: the worst over the ten components of h and the three axes of
+ *     |u+ - 2 u0 + u-| / (|u+ - u0| + |u0 - u-| + 4 eps scale)   (0 where the denominator is),
+ *   zero where the mask leaves the point out; and its maximum over the mesh (tau_max).
+ *   scale > 0 is the reference amplitude to use, else the largest of the ten maxima.
+ *   out[12] = the ten maxima, the scale used, tau_max.
+ * tgh_firing: the firing sweeps of refine_flags over slot 9, ntol (1..4) thresholds at once:
+ *   per block b and threshold n the number of owned points with tau > tol[n] in
+ *   counts[b * ntol + n] and the bounding box of their node indices (0-based, i j k low then
+ *   i j k high; low N+1 and high -1 where none fired) in boxes[6 (b * ntol + n) + 0..5].
+ *   counts and boxes are host arrays. */
+int tgh_tau(tgh_problem* p, const double* u, double t, int mask, double eps, double scale, double* out);
+int tgh_firing(tgh_problem* p, int ntol, const double* tol, int* counts, int* boxes);
 /* the diag field set: its length in doubles, and a copy of it into a device buffer */
 size_t tgh_diag_length(const tgh_problem* p);
 int tgh_copy_diag(tgh_problem* p, double* out);

@@ -575,8 +575,8 @@ static void error_norm(Problem& P, const double* u, double t, double* l2, double
 
 // ---- the constraint monitors (src/constraints.jl:211-271, 432-532) into a diag field set:
 // per block NDIAG slots of (N+1)^3 points, C_a (4), H, M_i (3), the mask indicator ----
-static const int NDIAG = 9;
-enum { DG_CGH = 0, DG_HAM = 4, DG_MOM = 5, DG_MASK = 8 };
+static const int NDIAG = 10;
+enum { DG_CGH = 0, DG_HAM = 4, DG_MOM = 5, DG_MASK = 8, DG_TAU = 9 };
 
 static PointCtx point_ctx(const Problem& P, int b, const int I[3], double x[3]) {
   PointCtx c;
@@ -763,6 +763,89 @@ static void adm_constraint(Problem& P, const double* u, double t, bool all, cons
 
 static inline double nanmax(double a, double b) { return (a != a || b != b) ? NAN : (a > b ? a : b); }
 
+// ---- the masked Loehner indicator (src/refinement.jl:170-218, 280-330, 390-391) ----
+// lohner: the second difference over the two first differences and the noise floor
+static inline double lohner(double um, double u0, double up, double scale, double eps) {
+  const double num = std::fabs(up - 2.0 * u0 + um);
+  const double den = std::fabs(up - u0) + std::fabs(u0 - um) + 4.0 * eps * std::fabs(scale);
+  return den == 0.0 ? 0.0 : num / den;
+}
+
+// field_scales (the largest |h_v| over the evolved owned points), then tau at every owned point
+// (cell_tau: the worst over the ten components of h and the three axes; zero where the mask
+// leaves the point out) into the diag slot DG_TAU, then tau_max over the mesh.
+// out: the ten maxima, the scale used (scale_in if positive, else their largest), tau_max
+static void tau(Problem& P, const double* u, double t, bool all, double eps, double scale_in, double* diag,
+                double out[12]) {
+  prepare(P, u, t);
+  const size_t S = P.npt_state();
+  double sc[NC];
+  for (int v = 0; v < NC; ++v) sc[v] = 0.0;
+  for (int b = 0; b < P.nb; ++b)
+    for (int k = 0; k < P.N1; ++k)
+      for (int j = 0; j < P.N1; ++j)
+        for (int i = 0; i < P.N1; ++i) {
+          int I[3] = {i, j, k};
+          double x[3];
+          PointCtx c = point_ctx(P, b, I, x);
+          if (!all && !is_evolved(P, t, x)) continue;
+          for (int v = 0; v < NC; ++v) sc[v] = nanmax(sc[v], std::fabs(c.wk[c.var + v * c.sv]));
+        }
+  double scale = 0.0;
+  for (int v = 0; v < NC; ++v) {
+    out[v] = sc[v];
+    scale = nanmax(scale, sc[v]);
+  }
+  if (scale_in > 0.0) scale = scale_in;
+  double tmax = 0.0;
+  for (int b = 0; b < P.nb; ++b)
+    for (int k = 0; k < P.N1; ++k)
+      for (int j = 0; j < P.N1; ++j)
+        for (int i = 0; i < P.N1; ++i) {
+          int I[3] = {i, j, k};
+          double x[3];
+          PointCtx c = point_ctx(P, b, I, x);
+          double tv = 0.0;
+          if (all || is_evolved(P, t, x))
+            for (int v = 0; v < NC; ++v) {
+              const size_t q = c.var + v * c.sv;
+              for (int d = 0; d < 3; ++d)
+                tv = nanmax(tv, lohner(c.wk[q - c.st[d]], c.wk[q], c.wk[q + c.st[d]], scale, eps));
+            }
+          diag[(size_t)b * NDIAG * S + DG_TAU * S + i + P.N1 * (j + (size_t)P.N1 * k)] = tv;
+          tmax = nanmax(tmax, tv);
+        }
+  out[10] = scale;
+  out[11] = tmax;
+}
+
+// firing_boxes over the diag slot DG_TAU: per block and threshold the number of owned points
+// with tau > tol and the bounding box of their node indices (low N+1 and high -1 where none)
+static void firing(const Problem& P, const double* diag, int ntol, const double* tol, int* counts, int* boxes) {
+  const size_t S = P.npt_state();
+  for (int b = 0; b < P.nb; ++b)
+    for (int n = 0; n < ntol; ++n) {
+      const size_t o = (size_t)b * ntol + n;
+      counts[o] = 0;
+      for (int d = 0; d < 3; ++d) {
+        boxes[6 * o + d] = P.N1;
+        boxes[6 * o + 3 + d] = -1;
+      }
+      for (int k = 0; k < P.N1; ++k)
+        for (int j = 0; j < P.N1; ++j)
+          for (int i = 0; i < P.N1; ++i) {
+            const double tv = diag[(size_t)b * NDIAG * S + DG_TAU * S + i + P.N1 * (j + (size_t)P.N1 * k)];
+            if (!(tv > tol[n])) continue;
+            const int I[3] = {i, j, k};
+            ++counts[o];
+            for (int d = 0; d < 3; ++d) {
+              boxes[6 * o + d] = std::min(boxes[6 * o + d], I[d]);
+              boxes[6 * o + 3 + d] = std::max(boxes[6 * o + 3 + d], I[d]);
+            }
+          }
+    }
+}
+
 // diag_norms over the slots C_a .. mask (src/constraints.jl:716-778, 825-865): each lattice point
 // once, at its primary copy; weight h^3 (volume) or 1 (points), blocks of level at_level only
 // when at_level >= 0; L2 = sqrt(sum u^2 w / evolved volume), Linf the largest |u| (NaN kept).
@@ -947,6 +1030,14 @@ int orc_adm_constraint(void* p, const double* u, double t, int allpoints, const 
 }
 int orc_constraint_norms(void* p, const double* diag, int weighting, int at_level, double* out16) {
   constraint_norms(*(Problem*)p, diag, weighting == 0, at_level, out16);
+  return TGH_OK;
+}
+int orc_tau(void* p, const double* u, double t, int allpoints, double eps, double scale, double* diag, double* out12) {
+  tau(*(Problem*)p, u, t, allpoints != 0, eps, scale, diag, out12);
+  return TGH_OK;
+}
+int orc_firing(void* p, const double* diag, int ntol, const double* tol, int* counts, int* boxes) {
+  firing(*(Problem*)p, diag, ntol, tol, counts, boxes);
   return TGH_OK;
 }
 // the pointwise pieces alone, for the pins of test/constraints_tests.jl:63-158

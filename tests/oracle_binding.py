@@ -67,6 +67,9 @@ class Oracle:
             "orc_metric_derivatives_along": (None, [_DP, _DP, _DP]),
             "orc_metric_derivatives": (None, [_DP, _DP, _DP]),
             "orc_count_flops": (ctypes.c_int, [_VP, _D, ctypes.POINTER(ctypes.c_long)]),
+            "orc_tau": (ctypes.c_int, [_VP, _DP, _D, ctypes.c_int, _D, _D, _DP, _DP]),
+            "orc_firing": (ctypes.c_int, [_VP, _DP, ctypes.c_int, _DP, ctypes.POINTER(ctypes.c_int),
+                                          ctypes.POINTER(ctypes.c_int)]),
             "orc_count_monitor_flops": (ctypes.c_int, [_VP, _D, ctypes.c_int, ctypes.POINTER(ctypes.c_long)]),
         }
         for name, (res, args) in sig.items():
@@ -246,6 +249,23 @@ class OracleProblem:
         self.lib.orc_adm_constraint(self.h, _dp(u), t, int(allpoints), _dp(matter) if matter is not None else None,
                                     _dp(diag))
         return diag
+
+    def tau(self, diag, u, t, eps=1 / 100, scale=None, allpoints=False):
+        """The masked Loehner indicator into diag slot 9; returns (the ten maxima, scale, tau_max)."""
+        out = np.zeros(12)
+        self.lib.orc_tau(self.h, _dp(u), t, int(allpoints), eps, -1.0 if scale is None else scale, _dp(diag),
+                         _dp(out))
+        return {"scales": list(out[:10]), "scale": out[10], "tau_max": out[11]}
+
+    def firing(self, diag, tols):
+        n = len(tols)
+        nb = len(self.forest.level)
+        counts = np.zeros(nb * n, dtype=np.int32)
+        boxes = np.zeros(6 * nb * n, dtype=np.int32)
+        t = np.ascontiguousarray(tols, dtype=float)
+        self.lib.orc_firing(self.h, _dp(diag), n, _dp(t), counts.ctypes.data_as(ctypes.POINTER(ctypes.c_int)),
+                            boxes.ctypes.data_as(ctypes.POINTER(ctypes.c_int)))
+        return counts.reshape(nb, n), boxes.reshape(nb, n, 6)
 
     def count_flops(self, t, monitor=None):
         """Algorithmic FP64 operations at the centre of block 0 of the prepared problem: the

@@ -16,6 +16,7 @@ pytestmark = pytest.mark.gpu
 
 TOL = 1e-12
 ROWS = [0, 1, 2, 3, 4, 6, 7, 8, 10, 11, 12, 17, 19]
+ND = 10  # diag slots per block: C_a, H, M_i, mask, tau
 
 
 def _monitor_rows(tgh):
@@ -42,8 +43,8 @@ def _compare(tgh, oracle, name, case, forest, q, t, mask):
     assert torch.equal(ug, _to_gpu(u)), "u was written"
     d = d.cpu().numpy()
     N1 = forest.N + 1
-    a = d.reshape(forest.nblocks, 9, N1, N1, N1)
-    b = d_ref.reshape(forest.nblocks, 9, N1, N1, N1)
+    a = d.reshape(forest.nblocks, ND, N1, N1, N1)[:, :9]
+    b = d_ref.reshape(forest.nblocks, ND, N1, N1, N1)[:, :9]
     assert np.array_equal(a[:, 8], b[:, 8]), f"{name}: mask"
     off = b[:, 8] == 0.0
     assert np.all(a[:, :8][np.broadcast_to(off[:, None], a[:, :8].shape)] == 0.0), f"{name}: masked points"
@@ -98,14 +99,14 @@ def test_adm_monitor_with_matter_matches_oracle(tgh, oracle):
     P.adm_constraint(_to_gpu(u), 0.25, matter=_to_gpu(matter))
     d = P.diag().cpu().numpy()
     N1 = forest.N + 1
-    a = d.reshape(forest.nblocks, 9, N1, N1, N1)[:, 4:9]
-    b = d_ref.reshape(forest.nblocks, 9, N1, N1, N1)[:, 4:9]
+    a = d.reshape(forest.nblocks, ND, N1, N1, N1)[:, 4:9]
+    b = d_ref.reshape(forest.nblocks, ND, N1, N1, N1)[:, 4:9]
     scale = rhs_scale(O.work(), forest, 4)
     assert float(np.max(np.max(np.abs(a - b), axis=1) / scale)) < TOL
     # the matter moved the constraints by its 16 pi rho and 8 pi S_i (and its source)
     d0 = O.diag()
     O.adm_constraint(d0, u, 0.25)
-    assert np.abs(d0.reshape(forest.nblocks, 9, -1)[:, 4] - d_ref.reshape(forest.nblocks, 9, -1)[:, 4]).max() > 1e-3
+    assert np.abs(d0.reshape(forest.nblocks, ND, -1)[:, 4] - d_ref.reshape(forest.nblocks, ND, -1)[:, 4]).max() > 1e-3
 
 
 def test_norms_per_level_match_oracle(tgh, oracle):

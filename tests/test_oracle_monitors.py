@@ -190,7 +190,7 @@ def test_the_norms_count_each_lattice_point_once(tgh, oracle, periodic):
         case = tgh.cases.Case({"kind": "minkowski"}, ((0.0, 1.0),) * 3, (False, False, False), 0.0, 0.0, 0.0)
     f = tgh.gh_forest(case, 8, 2)
     O = oracle.problem(case, f, 4)
-    d = O.diag().reshape(len(f.level), 9, 9, 9, 9)
+    d = O.diag().reshape(len(f.level), 10, 9, 9, 9)
     d[:, 8] = 1.0
     d[:, 0, :, :, 8] = 1.0
     n = O.constraint_norms(d.ravel(), weighting="points")
@@ -211,7 +211,7 @@ def test_the_mask_writes_exact_zeros_and_the_norms_divide_by_the_evolved_volume(
     O.gh_constraint(d, u, 0.0)
     O.adm_constraint(d, u, 0.0)
     S = 9 ** 3
-    dd = d.reshape(len(f.level), 9, S)
+    dd = d.reshape(len(f.level), 10, S)[:, :9]
     h = f.h0
     idx = np.arange(S)
     i, j, k = idx % 9, (idx // 9) % 9, idx // 81

@@ -11,11 +11,15 @@ Public surface, named after the reference's:
   cases      minkowski_case, gauge_wave_case, shifted_minkowski_case, kerr_schild_case, ...
   forests    gh_forest, hole_forest
   problem    GHProblem with prepare, rhs, gh_rhs, settle, stage_limit, step_limit, max_speed,
-             initial_state, gh_dt, rk4_step, step_batched, gh_solve, error_norm
+             initial_state, gh_dt, rk4_step, step_batched, gh_solve, error_norm,
+             gh_constraint, adm_constraint, constraint_norms, tau, firing
+  refinement Refinement, level_bounds, refine_flags, indicator_flags: the masked Loehner verdict
   shard      partition, exchange_plan, ShardedGHProblem (one rank per GPU)
   gradient   MaskedErrorStudy, MaskedError: the masked error's gradient by forward-mode tangents
 """
 from . import _abi
+from . import refinement
+from .refinement import Refinement, indicator_flags, level_bounds, refine_flags
 from .cases import (Case, gauge_wave_case, horizon_min_radius, kerr_schild_case, minkowski_case,
                     perturbed_minkowski_case, shifted_minkowski_case)
 from .forest import Forest, gh_forest, hole_forest
@@ -27,6 +31,7 @@ from .gradient import MaskedError, MaskedErrorStudy
 __all__ = ["Case", "Forest", "GHProblem", "gauge_wave_case", "gh_forest", "hole_forest", "kerr_schild_case",
            "minkowski_case", "perturbed_minkowski_case", "shifted_minkowski_case", "horizon_min_radius",
            "fourier_modes", "perturbation", "fp64_peak_tflops", "load_library", "ShardedGHProblem",
-           "exchange_plan", "partition", "MaskedError", "MaskedErrorStudy"]
+           "exchange_plan", "partition", "MaskedError", "MaskedErrorStudy", "Refinement", "indicator_flags",
+           "level_bounds", "refine_flags", "refinement"]
 
 load_library = _abi.load_library

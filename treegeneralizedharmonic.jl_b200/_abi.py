@@ -18,7 +18,7 @@ DISS_CONSTANT, DISS_HORIZON = range(2)
 INT_NONE, INT_DAMPED, INT_FROZEN, INT_PASTED = range(4)
 PREC_FP64, PREC_MIXED = range(2)
 MASK_INTERIOR, MASK_ALL = range(2)
-NDIAG = 9  # diag slots per block: C_a (0..3), H (4), M_i (5..7), mask (8)
+NDIAG = 10  # diag slots per block: C_a (0..3), H (4), M_i (5..7), mask (8), tau (9)
 
 D3 = ctypes.c_double * 3
 D4 = ctypes.c_double * 4
@@ -75,6 +75,9 @@ SIGNATURES = {
     "tgh_gh_constraint": (ctypes.c_int, [_VP, _VP, _D, ctypes.c_int]),
     "tgh_adm_constraint": (ctypes.c_int, [_VP, _VP, _D, ctypes.c_int, _VP]),
     "tgh_constraint_norms": (ctypes.c_int, [_VP, ctypes.c_int, ctypes.c_int, ctypes.POINTER(_D)]),
+    "tgh_tau": (ctypes.c_int, [_VP, _VP, _D, ctypes.c_int, _D, _D, ctypes.POINTER(_D)]),
+    "tgh_firing": (ctypes.c_int, [_VP, ctypes.c_int, ctypes.POINTER(_D), ctypes.POINTER(ctypes.c_int),
+                                  ctypes.POINTER(ctypes.c_int)]),
     "tgh_diag_length": (ctypes.c_size_t, [_VP]),
     "tgh_copy_diag": (ctypes.c_int, [_VP, _VP]),
     "tgh_max_speed_noalloc": (ctypes.c_int, [ctypes.POINTER(Config), ctypes.POINTER(Mesh), _VP, _D, _VP,

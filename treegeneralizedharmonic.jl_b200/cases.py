@@ -108,7 +108,7 @@ def perturbed_minkowski_case(halfwidth=1.0, eps_ko=0.5, gamma0=1.0, gamma2=0.0):
 
 def kerr_schild_case(M=1.0, a=0.0, v=0.0, x0=0.0, halfwidth=8.0, r0=0.8, r1=1.3, rho_max=None,
                      variant="damped", gauge="sampled", eps_ko=0.5, gamma0=None, gamma2=0.0, w_ramp=0.5,
-                     rho_ramp=0.5):
+                     rho_ramp=0.5, margin=8):
     """A Kerr-Schild hole in a Dirichlet box with the damping layer (hole_case /
     kerr_schild_case, src/initialdata.jl:1044-1300). The hole sits at (x0 + v t, 0, 0): the
     background is translate(boost(KerrSchild(M, a), (-v, 0, 0)), (0, x0, 0, 0)). A moving hole
@@ -124,7 +124,8 @@ def kerr_schild_case(M=1.0, a=0.0, v=0.0, x0=0.0, halfwidth=8.0, r0=0.8, r1=1.3,
     interior = None
     if variant is not None:
         interior = {"variant": variant, "c0": centre, "v": vel, "r0": r0, "r1": r1,
-                    "rho_max": 4.0 / M if rho_max is None else rho_max, "w_ramp": w_ramp, "rho_ramp": rho_ramp}
+                    "rho_max": 4.0 / M if rho_max is None else rho_max, "w_ramp": w_ramp, "rho_ramp": rho_ramp,
+                    "margin": margin}
     ks = {"M": M, "spin": (0.0, 0.0, a), "velocity": vel}
     return Case(bg, ((-halfwidth, halfwidth),) * 3, (False, False, False), eps_ko, gamma0, gamma2, interior,
                 gauge, ks, M)

@@ -12,7 +12,7 @@
 
 namespace tgh {
 
-enum { NDIAG = 9, DG_CGH = 0, DG_HAM = 4, DG_MOM = 5, DG_MASK = 8 };
+enum { NDIAG = 10, DG_CGH = 0, DG_HAM = 4, DG_MOM = 5, DG_MASK = 8, DG_TAU = 9 };
 
 struct MonArgs {
   const double* work;    // the filled working array
@@ -411,6 +411,106 @@ static __global__ void __launch_bounds__(256) diag_norms_fold_kernel(const doubl
     __syncthreads();
   }
   if (threadIdx.x == 0) out[n] = sh[0];
+}
+
+// ---- the masked Loehner indicator (src/refinement.jl:170-400) ----
+// A non-negative double's bit pattern orders as the double does (and a positive NaN above +inf),
+// so integer atomics give an order-independent maximum that keeps NaN.
+__device__ __forceinline__ void atomic_max_nonneg(unsigned long long* a, double v) {
+  atomicMax(a, (unsigned long long)__double_as_longlong(v));
+}
+
+// field_scales: the largest |h_v| over the evolved owned points, per component (the
+// reference amplitude of the indicator's noise floor); out[v] as bit patterns, zeroed before
+static __global__ void __launch_bounds__(128) field_scales_kernel(const MonArgs A, const Case cs,
+                                                                  unsigned long long* out) {
+  __shared__ unsigned long long sh[NC];
+  if (threadIdx.x < NC) sh[threadIdx.x] = 0ull;
+  __syncthreads();
+  const long p = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (p < A.npts) {
+    const MonPoint m = mon_point(A, p);
+    if (A.all || evolved(cs, A.t, m.x)) {
+#pragma unroll
+      for (int v = 0; v < NC; ++v) atomicMax(&sh[v], (unsigned long long)__double_as_longlong(fabs(m.wk[v * A.Wv])));
+    }
+  }
+  __syncthreads();
+  if (threadIdx.x < NC) atomicMax(&out[threadIdx.x], sh[threadIdx.x]);
+}
+
+// lohner: |u+ - 2 u0 + u-| / (|u+ - u0| + |u0 - u-| + 4 eps scale), 0 where the denominator
+// is; every operation rounded on its own, in the reference's order
+__device__ __forceinline__ double lohner(double um, double u0, double up, double floor4) {
+  const double num = fabs(__dadd_rn(__dsub_rn(up, __dmul_rn(2.0, u0)), um));
+  const double den = __dadd_rn(__dadd_rn(fabs(__dsub_rn(up, u0)), fabs(__dsub_rn(u0, um))), floor4);
+  return den == 0.0 ? 0.0 : __ddiv_rn(num, den);
+}
+
+// gh_tau_kernel!: tau at every owned point into the diag slot DG_TAU, the worst lohner over the
+// ten components of h and the three axes, zero where the mask leaves the point out (asked
+// before any value is read); its maximum over the mesh into *tmax (bit pattern)
+static __global__ void __launch_bounds__(128) tau_kernel(const MonArgs A, const Case cs, double floor4,
+                                                         unsigned long long* tmax) {
+  __shared__ unsigned long long sh;
+  if (threadIdx.x == 0) sh = 0ull;
+  __syncthreads();
+  const long p = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (p < A.npts) {
+    const MonPoint m = mon_point(A, p);
+    double tau = 0.0;
+    if (A.all || evolved(cs, A.t, m.x)) {
+      const long s[3] = {1, A.Wd, (long)A.Wd * A.Wd};
+#pragma unroll
+      for (int v = 0; v < NC; ++v) {
+        const double* q = m.wk + v * A.Wv;
+        const double u0 = q[0];
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+          const double t = lohner(q[-s[d]], u0, q[s[d]], floor4);
+          tau = (t != t || tau != tau) ? __longlong_as_double(0x7ff8000000000000LL) : fmax(tau, t);
+        }
+      }
+    }
+    A.diag[(long)m.b * NDIAG * A.S + DG_TAU * A.S + m.ip] = tau;
+    atomicMax(&sh, (unsigned long long)__double_as_longlong(tau));
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) atomicMax(tmax, sh);
+}
+
+// firing_boxes over the diag slot DG_TAU, for ntol thresholds at once: per block and threshold
+// the number of owned points with tau > tol and the bounding box of their node indices.
+// counts: nb x ntol (zeroed before); boxes: nb x ntol x 6 (lo i, j, k set to N1, hi to -1 before)
+static __global__ void __launch_bounds__(128) firing_kernel(const MonArgs A, int ntol, const double* __restrict__ tol,
+                                                            int* counts, int* boxes) {
+  const long p = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= A.npts) return;
+  const int b = (int)(p / A.S);
+  const long ip = p - (long)b * A.S;
+  const int ijk[3] = {(int)(ip % A.N1), (int)((ip / A.N1) % A.N1), (int)(ip / ((long)A.N1 * A.N1))};
+  const double tau = A.diag[(long)b * NDIAG * A.S + DG_TAU * A.S + ip];
+  for (int n = 0; n < ntol; ++n) {
+    if (!(tau > tol[n])) continue;
+    const long o = (long)b * ntol + n;
+    atomicAdd(&counts[o], 1);
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+      atomicMin(&boxes[6 * o + d], ijk[d]);
+      atomicMax(&boxes[6 * o + 3 + d], ijk[d]);
+    }
+  }
+}
+
+static __global__ void firing_init_kernel(int n, int N1, int* counts, int* boxes) {
+  const int id = blockIdx.x * blockDim.x + threadIdx.x;
+  if (id >= n) return;
+  counts[id] = 0;
+#pragma unroll
+  for (int d = 0; d < 3; ++d) {
+    boxes[6 * id + d] = N1;
+    boxes[6 * id + 3 + d] = -1;
+  }
 }
 
 cudaError_t launch_gauge_constraint(int q, cudaStream_t s, const Case& cs, const MonArgs& a);

@@ -74,6 +74,10 @@ struct tgh_problem {
   double* part = nullptr;                 // error-norm partials + result
   double* diag = nullptr;                 // the monitors' diag field set (NDIAG slots per block)
   double* dpart = nullptr;                // constraint-norm partials (17 per CTA) + the fold
+  unsigned long long* ind = nullptr;      // the indicator's maxima (10 scales, tau_max) as bit patterns
+  double* ind_tol = nullptr;              // the firing thresholds (at most 4)
+  int* ind_counts = nullptr;              // per block and threshold: firing count
+  int* ind_boxes = nullptr;               // ... and the bounding box of the firing nodes
   double* coef = nullptr;                 // per-point coefficients between the two RHS kernels
   int npart = 0;
   // plain-form RK4 buffers (state layout)
@@ -681,6 +685,10 @@ static int setup_device(tgh_problem* p) {
   CK(cudaMalloc(&p->diag, (size_t)NDIAG * p->npts * sizeof(double)));
   CK(cudaMemsetAsync(p->diag, 0, (size_t)NDIAG * p->npts * sizeof(double), p->stream));
   CK(cudaMalloc(&p->dpart, (17 * (size_t)p->npart + 17) * sizeof(double)));
+  CK(cudaMalloc(&p->ind, 16 * sizeof(unsigned long long)));
+  CK(cudaMalloc(&p->ind_tol, 4 * sizeof(double)));
+  CK(cudaMalloc(&p->ind_counts, 4 * (size_t)p->nb * sizeof(int)));
+  CK(cudaMalloc(&p->ind_boxes, 24 * (size_t)p->nb * sizeof(int)));
   double wp[10] = {0};
   prolong_weights(p->q + 2, wp);
   CK(cudaMemcpyToSymbol(c_wprol, wp, sizeof(wp)));
@@ -712,7 +720,7 @@ void tgh_problem_destroy(tgh_problem* p) {
     if (x.recv) cudaFree(x.recv);
   }
   void* bufs[] = {p->work, p->Hsrc, p->blk, p->primary, p->runs, p->gpts, p->hooks, p->hook_cache, p->scratch,
-                  p->part, p->coef, p->diag, p->dpart,
+                  p->part, p->coef, p->diag, p->dpart, p->ind, p->ind_tol, p->ind_counts, p->ind_boxes,
                   p->k, p->acc, p->y, p->u0, p->W1, p->W2, p->bacc, p->twork, p->kt, p->acct, p->yt};
   for (void* b : bufs)
     if (b) cudaFree(b);
@@ -799,6 +807,59 @@ int tgh_constraint_norms(tgh_problem* p, int weighting, int at_level, double* ou
     out[10 + a] = l2[DG_MOM + a];
     out[13 + a] = r[9 + DG_MOM + a];
   }
+  return TGH_OK;
+}
+
+// ---- the masked Loehner indicator (src/refinement.jl:280-400) ----
+int tgh_tau(tgh_problem* p, const double* u, double t, int mask, double eps, double scale, double* out) {
+  if (!(eps > 0.0)) return fail(p, TGH_ERR_ARG, "the noise floor's coefficient eps must be positive");
+  MonArgs a;
+  int s = monitor_prepare(p, u, t, mask, a);
+  if (s) return s;
+  CK(cudaMemsetAsync(p->ind, 0, 11 * sizeof(unsigned long long), p->stream));
+  const unsigned nb = (unsigned)grid_for(p->npts, 128);
+  field_scales_kernel<<<nb, 128, 0, p->stream>>>(a, p->cs, p->ind);
+  CK(cudaGetLastError());
+  unsigned long long bits[11];
+  CK(cudaMemcpyAsync(bits, p->ind, 10 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, p->stream));
+  CK(cudaStreamSynchronize(p->stream));
+  double sc = 0.0;
+  for (int v = 0; v < NC; ++v) {
+    double x;
+    std::memcpy(&x, &bits[v], sizeof(x));
+    out[v] = x;
+    sc = (x != x || sc != sc) ? x + sc : std::max(sc, x);
+  }
+  if (scale > 0.0) sc = scale;
+  const double floor4 = (4.0 * eps) * std::fabs(sc);
+  tau_kernel<<<nb, 128, 0, p->stream>>>(a, p->cs, floor4, p->ind + 10);
+  CK(cudaGetLastError());
+  CK(cudaMemcpyAsync(&bits[10], p->ind + 10, sizeof(unsigned long long), cudaMemcpyDeviceToHost, p->stream));
+  CK(cudaStreamSynchronize(p->stream));
+  out[10] = sc;
+  std::memcpy(&out[11], &bits[10], sizeof(double));
+  return TGH_OK;
+}
+
+int tgh_firing(tgh_problem* p, int ntol, const double* tol, int* counts, int* boxes) {
+  if (p->nranks > 1) return fail(p, TGH_ERR_ARG, "the indicator runs on a problem of one rank");
+  if (ntol < 1 || ntol > 4) return fail(p, TGH_ERR_ARG, "between 1 and 4 thresholds");
+  MonArgs a;
+  std::memset(&a, 0, sizeof(a));
+  a.diag = p->diag;
+  a.N1 = p->N1;
+  a.S = p->S;
+  a.npts = p->npts;
+  CK(cudaMemcpyAsync(p->ind_tol, tol, ntol * sizeof(double), cudaMemcpyHostToDevice, p->stream));
+  const int n = p->nb * ntol;
+  firing_init_kernel<<<(unsigned)grid_for(n, 128), 128, 0, p->stream>>>(n, p->N1, p->ind_counts, p->ind_boxes);
+  CK(cudaGetLastError());
+  firing_kernel<<<(unsigned)grid_for(p->npts, 128), 128, 0, p->stream>>>(a, ntol, p->ind_tol, p->ind_counts,
+                                                                          p->ind_boxes);
+  CK(cudaGetLastError());
+  CK(cudaMemcpyAsync(counts, p->ind_counts, n * sizeof(int), cudaMemcpyDeviceToHost, p->stream));
+  CK(cudaMemcpyAsync(boxes, p->ind_boxes, 6 * (size_t)n * sizeof(int), cudaMemcpyDeviceToHost, p->stream));
+  CK(cudaStreamSynchronize(p->stream));
   return TGH_OK;
 }
 

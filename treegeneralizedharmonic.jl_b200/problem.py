@@ -141,8 +141,30 @@ class GHProblem:
         return {"gauge_l2": o[0:4], "gauge_linf": o[4:8], "ham_l2": o[8], "ham_linf": o[9],
                 "mom_l2": o[10:13], "mom_linf": o[13:16]}
 
+    # ---- the refinement indicator (src/refinement.jl:280-400, include/tgh.h) ----
+    def tau(self, u, t, eps=1 / 100, scale=None, mask="interior"):
+        """The masked Loehner indicator of u at t into the diag field set (slot 9): returns the ten
+        masked maxima of |h_v| (field_scales), the scale used and tau_max."""
+        out = (ctypes.c_double * 12)()
+        self._check(self.lib.tgh_tau(self._h, _ptr(u), float(t), self.MASKS[mask], float(eps),
+                                     -1.0 if scale is None else float(scale), out))
+        o = list(out)
+        return {"scales": o[:10], "scale": o[10], "tau_max": o[11]}
+
+    def firing(self, tols):
+        """The firing sweeps over the indicator the last tau wrote: per block and threshold the
+        count of points above it and the bounding box (0-based nodes, low then high)."""
+        tols = [float(x) for x in tols]
+        n = len(tols)
+        nb = self.forest.nblocks
+        counts = (ctypes.c_int * (nb * n))()
+        boxes = (ctypes.c_int * (6 * nb * n))()
+        self._check(self.lib.tgh_firing(self._h, n, (ctypes.c_double * n)(*tols), counts, boxes))
+        import numpy as np
+        return np.array(counts).reshape(nb, n), np.array(boxes).reshape(nb, n, 6)
+
     def diag(self):
-        """A copy of the diag field set: per block 9 slots of (N+1)^3 points (C_a, H, M_i, mask)."""
+        """A copy of the diag field set: per block 10 slots of (N+1)^3 points (C_a, H, M_i, mask, tau)."""
         d = torch.empty(int(self.lib.tgh_diag_length(self._h)), dtype=torch.float64, device="cuda")
         self._check(self.lib.tgh_copy_diag(self._h, _ptr(d)))
         return d
