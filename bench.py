@@ -334,6 +334,18 @@ def time_monitors(P, u, stream, gauge, n1pts, peak, reps=5):
     t0 = time.perf_counter()
     n = P.constraint_norms()
     out["norms_ms_host"] = (time.perf_counter() - t0) * 1e3
+    # the refinement indicator (prepare, masked amplitudes, tau, tau_max) and the two firing sweeps,
+    # each a host call that returns its numbers
+    P.tau(u, 0.0)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    r = P.tau(u, 0.0)
+    t1 = time.perf_counter()
+    P.firing([0.4, 0.1])
+    t2 = time.perf_counter()
+    out["indicator_ms_host"] = (t1 - t0) * 1e3
+    out["firing_ms_host"] = (t2 - t1) * 1e3
+    out["tau_max"] = r["tau_max"]
     out["gauge_l2"] = n["gauge_l2"]
     out["ham_l2"] = n["ham_l2"]
     out["mom_l2"] = n["mom_l2"]
