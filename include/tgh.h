@@ -212,6 +212,16 @@ int tgh_constraint_norms(tgh_problem* p, int weighting, int at_level, double* ou
  *   counts and boxes are host arrays. */
 int tgh_tau(tgh_problem* p, const double* u, double t, int mask, double eps, double scale, double* out);
 int tgh_firing(tgh_problem* p, int ntol, const double* tol, int* counts, int* boxes);
+
+/* --- the regrid's state transfer (TreeAMR's regrid!, driver src/driver.jl:1660-1695) ---
+ * The state u_src of problem src at t onto the forest of problem dst (same case, order, block
+ * size and root grid; the caller builds dst on the regridded forest): src is prepared at t
+ * (its ghosts filled with this t's hook), then every owned point of every dst leaf takes its
+ * lattice point's value there, copied from the finest src leaf holding it at its level or
+ * finer, else prolonged (order q + 2) from the src leaf one level coarser covering it. u_dst is
+ * a device state vector of dst. The transfer plans on the host and allocates (and frees) its
+ * point lists on the device: it runs once per regrid. Problems of one rank only. */
+int tgh_transfer(tgh_problem* dst, tgh_problem* src, const double* u_src, double t, double* u_dst);
 /* the diag field set: its length in doubles, and a copy of it into a device buffer */
 size_t tgh_diag_length(const tgh_problem* p);
 int tgh_copy_diag(tgh_problem* p, double* out);

@@ -1032,6 +1032,31 @@ int orc_constraint_norms(void* p, const double* diag, int weighting, int at_leve
   constraint_norms(*(Problem*)p, diag, weighting == 0, at_level, out16);
   return TGH_OK;
 }
+// the regrid's transfer: every owned point of every leaf of `pd` takes the value its lattice
+// point has in `ps`'s state at t (value20: the primary copy, injection from a finer leaf, else the
+// prolongation of the next coarser level; the hook outside the domain)
+int orc_transfer(void* pd, void* ps, const double* u_src, double t, double* u_dst) {
+  Problem& D = *(Problem*)pd;
+  const Problem& Sr = *(Problem*)ps;
+  const std::vector<double> u(u_src, u_src + Sr.npt_state() * NV * Sr.nb);
+  const size_t S = D.npt_state();
+  try {
+    for (int b = 0; b < D.nb; ++b)
+      for (int k = 0; k < D.N1; ++k)
+        for (int j = 0; j < D.N1; ++j)
+          for (int i = 0; i < D.N1; ++i) {
+            int64_t n[3] = {(int64_t)D.corner[3 * b] + i, (int64_t)D.corner[3 * b + 1] + j,
+                            (int64_t)D.corner[3 * b + 2] + k};
+            double out[NV];
+            value20(Sr, u, t, D.level[b], n, out);
+            for (int v = 0; v < NV; ++v) u_dst[(size_t)b * NV * S + v * S + i + D.N1 * (j + (size_t)D.N1 * k)] = out[v];
+          }
+  } catch (const std::exception& e) {
+    D.err = e.what();
+    return TGH_ERR_ARG;
+  }
+  return TGH_OK;
+}
 int orc_tau(void* p, const double* u, double t, int allpoints, double eps, double scale, double* diag, double* out12) {
   tau(*(Problem*)p, u, t, allpoints != 0, eps, scale, diag, out12);
   return TGH_OK;

@@ -68,6 +68,7 @@ class Oracle:
             "orc_metric_derivatives": (None, [_DP, _DP, _DP]),
             "orc_count_flops": (ctypes.c_int, [_VP, _D, ctypes.POINTER(ctypes.c_long)]),
             "orc_tau": (ctypes.c_int, [_VP, _DP, _D, ctypes.c_int, _D, _D, _DP, _DP]),
+            "orc_transfer": (ctypes.c_int, [_VP, _VP, _DP, _D, _DP]),
             "orc_firing": (ctypes.c_int, [_VP, _DP, ctypes.c_int, _DP, ctypes.POINTER(ctypes.c_int),
                                           ctypes.POINTER(ctypes.c_int)]),
             "orc_count_monitor_flops": (ctypes.c_int, [_VP, _D, ctypes.c_int, ctypes.POINTER(ctypes.c_long)]),
@@ -249,6 +250,13 @@ class OracleProblem:
         self.lib.orc_adm_constraint(self.h, _dp(u), t, int(allpoints), _dp(matter) if matter is not None else None,
                                     _dp(diag))
         return diag
+
+    def transfer_from(self, src, u_src, t):
+        """The regrid's transfer of src's state at t onto this problem's forest."""
+        u = self.statevector()
+        st = self.lib.orc_transfer(self.h, src.h, _dp(np.ascontiguousarray(u_src)), t, _dp(u))
+        assert st == 0, self.lib.orc_last_error(self.h)
+        return u
 
     def tau(self, diag, u, t, eps=1 / 100, scale=None, allpoints=False):
         """The masked Loehner indicator into diag slot 9; returns (the ten maxima, scale, tau_max)."""

@@ -77,3 +77,45 @@ def test_indicator_flags_match_the_oracle_pipeline(tgh, oracle):
     # around a static hole at the origin the refined region is centred near it
     assert out["centroid"] is not None and np.linalg.norm(out["centroid"]) < 3 * R.spacing(forest, 0)
     assert any(m == R.REFINE for m in out["flags"])
+
+
+def _regrid_rows(tgh):
+    """(name, case, forest, q, t, marks): a hole refined where its indicator asks, a two-level
+    gauge wave coarsened back, and the moving-hole hierarchy with its finest level coarsened and
+    root blocks refined (rebalanced)."""
+    R = tgh.refinement
+    rows = []
+    hole = _hole(tgh)
+    f = tgh.gh_forest(hole, 8, 4)
+    rows.append(("hole_fixture_indicator", hole, f, 2, 0.0, None))
+    c = tgh.gauge_wave_case(A=1 / 20, d=1.0, eps_ko=0.0, gamma0=1.0, gamma2=0.0)
+    f = two_level_forest(tgh, c, 8)
+    rows.append(("gauge_wave_coarsened", c, f, 4, 0.125, [R.COARSEN if lv == 1 else R.KEEP for lv in f.level]))
+    name, c, f, q, t = cases(tgh)[19]
+    top = int(f.level.max())
+    marks = [R.COARSEN if lv == top else (R.REFINE if lv == 0 and i % 5 == 0 else R.KEEP)
+             for i, lv in enumerate(f.level)]
+    rows.append((name, c, f, q, t, marks))
+    return rows
+
+
+@pytest.mark.parametrize("row", range(3))
+def test_regrid_transfer_matches_oracle_bit_for_bit(tgh, oracle, row):
+    name, case, forest, q, t, marks = _regrid_rows(tgh)[row]
+    R = tgh.refinement
+    P = tgh.GHProblem(case, forest, q, margin_check=False)
+    O = oracle.problem(case, forest, q)
+    u = _initial(tgh, P, O, case, forest, name, t)
+    if marks is None:
+        marks = tgh.indicator_flags(P, case, _to_gpu(u), t, _ref(tgh), buffer=1)["flags"]
+    f2 = R.regrid_forest(forest, marks)
+    assert f2.nblocks != forest.nblocks or not np.array_equal(f2.corner, forest.corner)
+    P2, u2 = R.regrid(P, _to_gpu(u), t, marks)
+    O2 = oracle.problem(case, f2, q)
+    ref = O2.transfer_from(O, u, t)
+    O2.stage_limit(ref, t)
+    got = u2.cpu().numpy()
+    assert np.array_equal(got, ref), f"{name}: {np.abs(got - ref).max()}"
+    # the new problem steps on the transferred state
+    lam = P2.max_speed(u2, t)
+    assert np.isfinite(lam) and lam > 0

@@ -231,3 +231,70 @@ def test_the_margin_promotes_the_neighbours_of_a_box(tgh, oracle):
     buffered = R.refine_flags(forest, lb, ref, c, bx, buffer=1)
     assert buffered[b] == R.REFINE and buffered[nbr] == R.REFINE
     assert sum(1 for m in buffered if m == R.REFINE) < nb
+
+
+# ---- the regrid: the new forest and the state transfer (TreeAMR's regrid!, src/driver.jl:1660-1695) ----
+def _marks_for(forest, R, refine=(), coarsen_level=None):
+    out = []
+    for b in range(len(forest.level)):
+        c = tuple(int(x) for x in forest.corner[b])
+        lev = int(forest.level[b])
+        if (lev, c) in refine:
+            out.append(R.REFINE)
+        elif coarsen_level is not None and lev == coarsen_level:
+            out.append(R.COARSEN)
+        else:
+            out.append(R.KEEP)
+    return out
+
+
+def test_regrid_forest_refines_coarsens_and_balances(tgh):
+    R = tgh.refinement
+    case = tgh.gauge_wave_case()
+    f = tgh.gh_forest(case, 8, 2)
+    f1 = R.regrid_forest(f, _marks_for(f, R, refine={(0, (0, 0, 0))}))
+    assert len(f1.level) == 15 and sorted(set(int(x) for x in f1.level)) == [0, 1]
+    # the eight children all marked Coarsen become their parent again
+    f0 = R.regrid_forest(f1, _marks_for(f1, R, coarsen_level=1))
+    assert len(f0.level) == 8 and np.array_equal(np.sort(f0.corner, axis=0), np.sort(f.corner, axis=0))
+    # seven of eight siblings marked Coarsen: nothing coarsens
+    m = _marks_for(f1, R, coarsen_level=1)
+    m[[i for i, lv in enumerate(f1.level) if lv == 1][0]] = R.KEEP
+    assert len(R.regrid_forest(f1, m).level) == 15
+    # refining a level-1 leaf in the corner block's far corner forces its level-0 neighbours to refine
+    corner = max(tuple(int(x) for x in c) for c, lv in zip(f1.corner, f1.level) if lv == 1)
+    f2 = R.regrid_forest(f1, _marks_for(f1, R, refine={(1, corner)}))
+    levels = [int(x) for x in f2.level]
+    assert max(levels) == 2 and levels.count(0) < 7
+
+
+def test_transfer_is_exact_where_points_coincide(tgh, oracle):
+    # onto the same forest, and refined then coarsened back: the identity, bit for bit
+    R = tgh.refinement
+    case = tgh.kerr_schild_case(M=1.0, a=0.7, halfwidth=2.0, r0=0.8, r1=1.3, gauge="sampled")
+    f = tgh.gh_forest(case, 8, 2)
+    O = oracle.problem(case, f, 4)
+    u = O.initial_state(O.statevector(), 0.0)
+    Os = oracle.problem(case, f, 4)
+    assert np.array_equal(Os.transfer_from(O, u, 0.0), u)
+    f1 = R.regrid_forest(f, _marks_for(f, R, refine={(0, (0, 0, 0))}))
+    O1 = oracle.problem(case, f1, 4)
+    u1 = O1.transfer_from(O, u, 0.0)
+    O0 = oracle.problem(case, R.regrid_forest(f1, _marks_for(f1, R, coarsen_level=1)), 4)
+    assert np.array_equal(O0.transfer_from(O1, u1, 0.0), u)
+
+
+def test_transfer_prolongs_at_the_operator_order(tgh, oracle):
+    # smooth periodic data onto a refined mesh: the new points' error against the exact state
+    # falls at the prolongation's order as the mesh is refined
+    R = tgh.refinement
+    case = tgh.gauge_wave_case(A=0.05)
+    errs = []
+    for N in (8, 16):
+        f = tgh.gh_forest(case, N, 2)
+        O = oracle.problem(case, f, 4)
+        u = O.initial_state(O.statevector(), 0.0)
+        f1 = R.regrid_forest(f, _marks_for(f, R, refine={(0, (0, 0, 0))}))
+        O1 = oracle.problem(case, f1, 4)
+        errs.append(float(np.abs(O1.transfer_from(O, u, 0.0) - O1.initial_state(O1.statevector(), 0.0)).max()))
+    assert errs[0] > 0 and errs[0] / errs[1] > 2 ** 5.5  # order q + 2 = 6 prolongation

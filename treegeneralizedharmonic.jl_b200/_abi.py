@@ -78,6 +78,7 @@ SIGNATURES = {
     "tgh_tau": (ctypes.c_int, [_VP, _VP, _D, ctypes.c_int, _D, _D, ctypes.POINTER(_D)]),
     "tgh_firing": (ctypes.c_int, [_VP, ctypes.c_int, ctypes.POINTER(_D), ctypes.POINTER(ctypes.c_int),
                                   ctypes.POINTER(ctypes.c_int)]),
+    "tgh_transfer": (ctypes.c_int, [_VP, _VP, _VP, _D, _VP]),
     "tgh_diag_length": (ctypes.c_size_t, [_VP]),
     "tgh_copy_diag": (ctypes.c_int, [_VP, _VP]),
     "tgh_max_speed_noalloc": (ctypes.c_int, [ctypes.POINTER(Config), ctypes.POINTER(Mesh), _VP, _D, _VP,

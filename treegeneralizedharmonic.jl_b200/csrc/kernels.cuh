@@ -119,14 +119,10 @@ __global__ void hook_copy_kernel(const HookPt* __restrict__ pts, int n, const do
 // array, summed with x innermost, then y, then z; products and sums rounded one by one
 __constant__ double c_wprol[10];
 
-template <int P>
-__global__ void fill_prolong_kernel(const ProlongPt* __restrict__ pts, int n, double* __restrict__ work, Geo g) {
-  const int id = blockIdx.x * blockDim.x + threadIdx.x;
-  if (id >= n * NV) return;
-  const int pi = id / NV, v = id % NV;
-  const ProlongPt p = pts[pi];
-  const int cx = (p.odd & 1) ? P : 1, cy = (p.odd & 2) ? P : 1, cz = (p.odd & 4) ? P : 1;
-  const double* src = work + (long)p.src_b * NV * g.Wv + (long)v * g.Wv + p.src_w;
+// one variable's prolonged value from its coarse stencil base `src`, x summed innermost, each
+// product and sum rounded on its own
+template <int P> __device__ __forceinline__ double prolong_value(const double* src, int odd, Geo g) {
+  const int cx = (odd & 1) ? P : 1, cy = (odd & 2) ? P : 1, cz = (odd & 4) ? P : 1;
   const long sy = g.Wd, sz = (long)g.Wd * g.Wd;
   double szv = 0.0;
   for (int kz = 0; kz < cz; ++kz) {
@@ -147,7 +143,41 @@ __global__ void fill_prolong_kernel(const ProlongPt* __restrict__ pts, int n, do
     const double tz = __dmul_rn(wz, syv);
     szv = kz == 0 ? tz : __dadd_rn(szv, tz);
   }
-  work[(long)p.dst_b * NV * g.Wv + (long)v * g.Wv + p.dst_w] = szv;
+  return szv;
+}
+
+// The regrid's transfer (the fill's operators between two forests): the value of every owned
+// point of the new forest, copied from the old filled working array or prolonged from it,
+// into a state vector (S points per block and variable)
+__global__ void transfer_copy_kernel(const CopyPt* __restrict__ pts, long n, const double* __restrict__ work,
+                                     Geo g, double* __restrict__ u, long S) {
+  const long id = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (id >= n) return;
+  const CopyPt c = pts[id];
+  const double* src = work + (long)c.src_b * NV * g.Wv + c.src_w;
+  double* dst = u + (long)c.dst_b * NV * S + c.dst_w;
+#pragma unroll
+  for (int v = 0; v < NV; ++v) dst[v * S] = src[v * g.Wv];
+}
+template <int P>
+__global__ void transfer_prolong_kernel(const ProlongPt* __restrict__ pts, int n, const double* __restrict__ work,
+                                        Geo g, double* __restrict__ u, long S) {
+  const int id = blockIdx.x * blockDim.x + threadIdx.x;
+  if (id >= n * NV) return;
+  const int pi = id / NV, v = id % NV;
+  const ProlongPt p = pts[pi];
+  u[(long)p.dst_b * NV * S + (long)v * S + p.dst_w] =
+      prolong_value<P>(work + (long)p.src_b * NV * g.Wv + (long)v * g.Wv + p.src_w, p.odd, g);
+}
+
+template <int P>
+__global__ void fill_prolong_kernel(const ProlongPt* __restrict__ pts, int n, double* __restrict__ work, Geo g) {
+  const int id = blockIdx.x * blockDim.x + threadIdx.x;
+  if (id >= n * NV) return;
+  const int pi = id / NV, v = id % NV;
+  const ProlongPt p = pts[pi];
+  work[(long)p.dst_b * NV * g.Wv + (long)v * g.Wv + p.dst_w] =
+      prolong_value<P>(work + (long)p.src_b * NV * g.Wv + (long)v * g.Wv + p.src_w, p.odd, g);
 }
 
 // plain-form RK4 stage updates over the whole state vector (each one fused multiply-add):

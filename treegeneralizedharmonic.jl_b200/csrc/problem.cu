@@ -74,6 +74,7 @@ struct tgh_problem {
   double* part = nullptr;                 // error-norm partials + result
   double* diag = nullptr;                 // the monitors' diag field set (NDIAG slots per block)
   double* dpart = nullptr;                // constraint-norm partials (17 per CTA) + the fold
+  double* dwprol = nullptr;               // this order's prolongation weights (10), for the constant bank
   unsigned long long* ind = nullptr;      // the indicator's maxima (10 scales, tau_max) as bit patterns
   double* ind_tol = nullptr;              // the firing thresholds (at most 4)
   int* ind_counts = nullptr;              // per block and threshold: firing count
@@ -452,6 +453,24 @@ static void prolong_weights(int P, double* w) {
   }
 }
 
+// Level l's prolongation into `work`. The weights of this problem's order go into the constant
+// bank first, from the problem's own device copy and on its stream (a copy a graph captures),
+// since problems of other orders in the process use the same bank.
+static cudaError_t launch_prolong(tgh_problem* p, int l, double* work) {
+  cudaError_t e = cudaMemcpyToSymbolAsync(c_wprol, p->dwprol, 10 * sizeof(double), 0, cudaMemcpyDeviceToDevice,
+                                          p->stream);
+  if (e != cudaSuccess) return e;
+  const int T = 256;
+  const long n = (long)p->nprol[l] * NV;
+  switch (p->q + 2) {
+    case 4: fill_prolong_kernel<4><<<grid_for(n, T), T, 0, p->stream>>>(p->prol[l], p->nprol[l], work, p->geo); break;
+    case 6: fill_prolong_kernel<6><<<grid_for(n, T), T, 0, p->stream>>>(p->prol[l], p->nprol[l], work, p->geo); break;
+    case 8: fill_prolong_kernel<8><<<grid_for(n, T), T, 0, p->stream>>>(p->prol[l], p->nprol[l], work, p->geo); break;
+    default: fill_prolong_kernel<10><<<grid_for(n, T), T, 0, p->stream>>>(p->prol[l], p->nprol[l], work, p->geo); break;
+  }
+  return cudaGetLastError();
+}
+
 // The Dirichlet ghosts of `work` at time t. A stationary case (its analytic state does not
 // depend on t) evaluates them once and copies the kept values afterwards.
 static int launch_hooks(tgh_problem* p, double* work, double t) {
@@ -486,14 +505,7 @@ static int launch_fill(tgh_problem* p, const double* src, bool from_work, double
   if (s) return s;
   for (int l = 1; l <= p->maxlevel; ++l) {
     if (!p->nprol[l]) continue;
-    const long n = (long)p->nprol[l] * NV;
-    switch (p->q + 2) {
-      case 4: fill_prolong_kernel<4><<<grid_for(n, T), T, 0, p->stream>>>(p->prol[l], p->nprol[l], work, p->geo); break;
-      case 6: fill_prolong_kernel<6><<<grid_for(n, T), T, 0, p->stream>>>(p->prol[l], p->nprol[l], work, p->geo); break;
-      case 8: fill_prolong_kernel<8><<<grid_for(n, T), T, 0, p->stream>>>(p->prol[l], p->nprol[l], work, p->geo); break;
-      default: fill_prolong_kernel<10><<<grid_for(n, T), T, 0, p->stream>>>(p->prol[l], p->nprol[l], work, p->geo); break;
-    }
-    CK(cudaGetLastError());
+    CK(launch_prolong(p, l, work));
   }
   return TGH_OK;
 }
@@ -691,7 +703,8 @@ static int setup_device(tgh_problem* p) {
   CK(cudaMalloc(&p->ind_boxes, 24 * (size_t)p->nb * sizeof(int)));
   double wp[10] = {0};
   prolong_weights(p->q + 2, wp);
-  CK(cudaMemcpyToSymbol(c_wprol, wp, sizeof(wp)));
+  CK(cudaMalloc(&p->dwprol, sizeof(wp)));
+  CK(cudaMemcpy(p->dwprol, wp, sizeof(wp), cudaMemcpyHostToDevice));
   if (cfg->gauge == TGH_GAUGE_SAMPLED) {
     CK(cudaMalloc(&p->Hsrc, (size_t)p->S * NV * p->nb * sizeof(double)));
     sample_gauge_kernel<<<grid_for(p->npts, 64), 64, 0, p->stream>>>(p->Hsrc, p->blk, p->geo, p->npts, p->cs, 0.0);
@@ -720,7 +733,7 @@ void tgh_problem_destroy(tgh_problem* p) {
     if (x.recv) cudaFree(x.recv);
   }
   void* bufs[] = {p->work, p->Hsrc, p->blk, p->primary, p->runs, p->gpts, p->hooks, p->hook_cache, p->scratch,
-                  p->part, p->coef, p->diag, p->dpart, p->ind, p->ind_tol, p->ind_counts, p->ind_boxes,
+                  p->part, p->coef, p->diag, p->dpart, p->ind, p->ind_tol, p->ind_counts, p->ind_boxes, p->dwprol,
                   p->k, p->acc, p->y, p->u0, p->W1, p->W2, p->bacc, p->twork, p->kt, p->acct, p->yt};
   for (void* b : bufs)
     if (b) cudaFree(b);
@@ -864,6 +877,96 @@ int tgh_firing(tgh_problem* p, int ntol, const double* tol, int* counts, int* bo
 }
 
 size_t tgh_diag_length(const tgh_problem* p) { return (size_t)NDIAG * p->npts; }
+
+// ---- the regrid's state transfer (TreeAMR's regrid! with the fill's operators) ----
+// Every owned point of every leaf of `dst` takes the value its lattice point has in the filled
+// working array of `src` at t: copied from the finest src leaf holding it at its level or finer
+// (the primary copy; injection from a finer leaf), else prolonged (order q + 2) from the src leaf
+// one level coarser that covers it. The plan is built here on the host and released after: a
+// regrid runs once per chunk of steps.
+int tgh_transfer(tgh_problem* dst, tgh_problem* src, const double* u_src, double t, double* u_dst) {
+  if (dst->nranks > 1 || src->nranks > 1) return fail(dst, TGH_ERR_ARG, "the transfer runs on problems of one rank");
+  bool same = dst->q == src->q && dst->N == src->N && dst->h0 == src->h0;
+  for (int d = 0; d < 3; ++d)
+    same = same && dst->lo[d] == src->lo[d] && dst->cells0[d] == src->cells0[d] && dst->periodic[d] == src->periodic[d];
+  if (!same) return fail(dst, TGH_ERR_ARG, "the two problems differ in order, block size or root grid");
+  int s = tgh_prepare(src, u_src, t);
+  if (s) return s;
+  const int G = src->G, Wd = src->Wd, P = src->q + 2;
+  std::vector<CopyPt> cp;
+  std::vector<ProlongPt> pp;
+  for (int b = 0; b < dst->nb; ++b) {
+    const int gb = dst->i2g[b], l = dst->level[gb];
+    for (int k = 0; k < dst->N1; ++k)
+      for (int j = 0; j < dst->N1; ++j)
+        for (int i = 0; i < dst->N1; ++i) {
+          const int ip = i + dst->N1 * (j + dst->N1 * k);
+          int64_t n[3] = {(int64_t)dst->corner[3 * gb] + i, (int64_t)dst->corner[3 * gb + 1] + j,
+                          (int64_t)dst->corner[3 * gb + 2] + k};
+          for (int d = 0; d < 3; ++d)
+            if (dst->periodic[d]) {
+              const int64_t per = (int64_t)dst->cells0[d] << l;
+              n[d] %= per;
+              if (n[d] < 0) n[d] += per;
+            }
+          int leaf, loc[3], lev;
+          if (find_owner(src, l, n, leaf, loc, lev)) {
+            const int sw = (loc[0] + G) + Wd * ((loc[1] + G) + Wd * (loc[2] + G));
+            cp.push_back(CopyPt{b, ip, src->g2i[leaf], sw});
+            continue;
+          }
+          const int c = l > 0 ? coarse_cover(src, l - 1, n) : -1;
+          if (c < 0) return fail(dst, TGH_ERR_ARG, "a point of the new forest is covered by no leaf of the old one "
+                                                   "at its level or one coarser (a leaf refined twice at once?)");
+          int odd = 0;
+          int64_t base[3];
+          for (int d = 0; d < 3; ++d) {
+            base[d] = (n[d] & 1) ? (n[d] >> 1) - (P / 2 - 1) : n[d] >> 1;
+            if (n[d] & 1) odd |= 1 << d;
+            const int64_t rel = base[d] - src->corner[3 * c + d] + G;
+            if (rel < 0 || rel + ((n[d] & 1) ? P : 1) > Wd)
+              return fail(dst, TGH_ERR_ARG, "a prolongation stencil of the transfer leaves the old block's ghost zone");
+          }
+          const int sw = (int)((base[0] - src->corner[3 * c] + G) +
+                               Wd * ((base[1] - src->corner[3 * c + 1] + G) + (int64_t)Wd * (base[2] - src->corner[3 * c + 2] + G)));
+          pp.push_back(ProlongPt{b, ip, src->g2i[c], sw, odd});
+        }
+  }
+  tgh_problem* p = dst;  // where a CUDA failure is reported
+  struct Plan {
+    CopyPt* cp = nullptr;
+    ProlongPt* pp = nullptr;
+    ~Plan() {
+      cudaFree(cp);
+      cudaFree(pp);
+    }
+  } plan;
+  CopyPt*& dcp = plan.cp;
+  ProlongPt*& dpp = plan.pp;
+  CK(cudaMalloc(&dcp, std::max<size_t>(1, cp.size()) * sizeof(CopyPt)));
+  CK(cudaMalloc(&dpp, std::max<size_t>(1, pp.size()) * sizeof(ProlongPt)));
+  CK(cudaMemcpy(dcp, cp.data(), cp.size() * sizeof(CopyPt), cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(dpp, pp.data(), pp.size() * sizeof(ProlongPt), cudaMemcpyHostToDevice));
+  const int T = 256;
+  if (!cp.empty())
+    transfer_copy_kernel<<<grid_for((long)cp.size(), T), T, 0, src->stream>>>(dcp, (long)cp.size(), src->work,
+                                                                               src->geo, u_dst, dst->S);
+  CK(cudaGetLastError());
+  if (!pp.empty()) {
+    CK(cudaMemcpyToSymbolAsync(c_wprol, src->dwprol, 10 * sizeof(double), 0, cudaMemcpyDeviceToDevice, src->stream));
+    const int np = (int)pp.size();
+    const long n = (long)np * NV;
+    switch (P) {
+      case 4: transfer_prolong_kernel<4><<<grid_for(n, T), T, 0, src->stream>>>(dpp, np, src->work, src->geo, u_dst, dst->S); break;
+      case 6: transfer_prolong_kernel<6><<<grid_for(n, T), T, 0, src->stream>>>(dpp, np, src->work, src->geo, u_dst, dst->S); break;
+      case 8: transfer_prolong_kernel<8><<<grid_for(n, T), T, 0, src->stream>>>(dpp, np, src->work, src->geo, u_dst, dst->S); break;
+      default: transfer_prolong_kernel<10><<<grid_for(n, T), T, 0, src->stream>>>(dpp, np, src->work, src->geo, u_dst, dst->S); break;
+    }
+    CK(cudaGetLastError());
+  }
+  CK(cudaStreamSynchronize(src->stream));
+  return TGH_OK;
+}
 
 int tgh_copy_diag(tgh_problem* p, double* out) {
   CK(cudaMemcpyAsync(out, p->diag, (size_t)NDIAG * p->npts * sizeof(double), cudaMemcpyDeviceToDevice, p->stream));
@@ -1014,14 +1117,7 @@ static int launch_fill_phase(tgh_problem* p, double* work, int phase, double t) 
   }
   const int l = phase;
   if (!p->nprol[l]) return TGH_OK;
-  const long n = (long)p->nprol[l] * NV;
-  switch (p->q + 2) {
-    case 4: fill_prolong_kernel<4><<<grid_for(n, T), T, 0, p->stream>>>(p->prol[l], p->nprol[l], work, p->geo); break;
-    case 6: fill_prolong_kernel<6><<<grid_for(n, T), T, 0, p->stream>>>(p->prol[l], p->nprol[l], work, p->geo); break;
-    case 8: fill_prolong_kernel<8><<<grid_for(n, T), T, 0, p->stream>>>(p->prol[l], p->nprol[l], work, p->geo); break;
-    default: fill_prolong_kernel<10><<<grid_for(n, T), T, 0, p->stream>>>(p->prol[l], p->nprol[l], work, p->geo); break;
-  }
-  CK(cudaGetLastError());
+  CK(launch_prolong(p, l, work));
   return TGH_OK;
 }
 
@@ -1325,14 +1421,7 @@ static int launch_fill_tangent(tgh_problem* p, const double* ut) {
   }
   for (int l = 1; l <= p->maxlevel; ++l) {
     if (!p->nprol[l]) continue;
-    const long n = (long)p->nprol[l] * NV;
-    switch (p->q + 2) {
-      case 4: fill_prolong_kernel<4><<<grid_for(n, T), T, 0, p->stream>>>(p->prol[l], p->nprol[l], p->twork, p->geo); break;
-      case 6: fill_prolong_kernel<6><<<grid_for(n, T), T, 0, p->stream>>>(p->prol[l], p->nprol[l], p->twork, p->geo); break;
-      case 8: fill_prolong_kernel<8><<<grid_for(n, T), T, 0, p->stream>>>(p->prol[l], p->nprol[l], p->twork, p->geo); break;
-      default: fill_prolong_kernel<10><<<grid_for(n, T), T, 0, p->stream>>>(p->prol[l], p->nprol[l], p->twork, p->geo); break;
-    }
-    CK(cudaGetLastError());
+    CK(launch_prolong(p, l, p->twork));
   }
   return TGH_OK;
 }

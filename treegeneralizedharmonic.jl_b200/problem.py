@@ -29,6 +29,7 @@ class GHProblem:
             raise RuntimeError("GHProblem runs on a CUDA device; none is available")
         self.lib = _abi.load_library()
         self.case, self.forest, self.q = case, forest, int(q)
+        self.margin_check, self.precision = margin_check, precision
         self.stream = stream if stream is not None else torch.cuda.current_stream()
         self._cfg = case.config(q, precision)
         self._mesh = forest.mesh()
@@ -162,6 +163,13 @@ class GHProblem:
         self._check(self.lib.tgh_firing(self._h, n, (ctypes.c_double * n)(*tols), counts, boxes))
         import numpy as np
         return np.array(counts).reshape(nb, n), np.array(boxes).reshape(nb, n, 6)
+
+    def transfer_from(self, src, u_src, t, u):
+        """The state u_src of problem `src` at t onto this problem's forest, into u (the regrid's
+        transfer: copies where the old forest holds the point at its level or finer, else the
+        order q + 2 prolongation from the old leaf one level coarser)."""
+        self._check(self.lib.tgh_transfer(self._h, src._h, _ptr(u_src), float(t), _ptr(u)))
+        return u
 
     def diag(self):
         """A copy of the diag field set: per block 10 slots of (N+1)^3 points (C_a, H, M_i, mask, tau)."""

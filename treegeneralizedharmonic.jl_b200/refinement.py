@@ -301,6 +301,61 @@ def refinement_buffer(forest, maxlevel_cap, travel):
     return cells
 
 
+def regrid_forest(forest, flags):
+    """The leaves after one regrid on bare or boxed marks (TreeAMR's regrid! with buffer = 0, as
+    the reference's driver calls it): a Refine leaf becomes its eight children; eight siblings
+    that are all marked Coarsen become their parent; then the forest is made 2:1 balanced by
+    refining (a coarsened parent next to a leaf two levels finer is refined back). Returns a new
+    Forest with the leaves sorted by level, then corner with x fastest (gh_forest's order, so
+    that a forest that did not change keeps its block numbering)."""
+    from .forest import Forest, _balance
+    N = forest.N
+    leaves = [(int(l), tuple(int(x) for x in c)) for l, c in zip(forest.level, forest.corner)]
+    if len(flags) != len(leaves):
+        raise ValueError(f"{len(flags)} marks for {len(leaves)} leaves")
+    kind = [m[0] if isinstance(m, tuple) else m for m in flags]
+
+    def parent(l, c):
+        return l - 1, tuple((ci // N) // 2 * N for ci in c)
+
+    groups = {}
+    for (l, c), k in zip(leaves, kind):
+        if k == COARSEN and l > 0:
+            groups.setdefault(parent(l, c), []).append((l, c))
+    whole = {pk for pk, ch in groups.items() if len(ch) == 8}
+    new, done = [], set()
+    for (l, c), k in zip(leaves, kind):
+        if k == REFINE:
+            for dz in (0, 1):
+                for dy in (0, 1):
+                    for dx in (0, 1):
+                        new.append((l + 1, (2 * c[0] + dx * N, 2 * c[1] + dy * N, 2 * c[2] + dz * N)))
+        elif k == COARSEN and l > 0 and parent(l, c) in whole:
+            pk = parent(l, c)
+            if pk not in done:
+                done.add(pk)
+                new.append(pk)
+        else:
+            new.append((l, c))
+    new = sorted(_balance(new, N, forest.cells0), key=lambda lc: (lc[0], lc[1][2], lc[1][1], lc[1][0]))
+    return Forest(N, forest.lo, forest.h0, forest.cells0, forest.periodic,
+                  np.array([l for l, _ in new], dtype=np.int32), np.array([c for _, c in new], dtype=np.int32))
+
+
+def regrid(P, u, t, flags):
+    """regrid! and the rebuild after it (src/driver.jl:1660-1695): the regridded forest, a new
+    problem on it (same case and order; the gauge source is sampled anew), the state transferred
+    with this t's hook, and the stage limiter applied to it (the pasted variant's paste; the
+    prolongation into a fresh block is unlimited). Returns (problem, state)."""
+    from .problem import GHProblem
+    f2 = regrid_forest(P.forest, flags)
+    P2 = GHProblem(P.case, f2, P.q, margin_check=P.margin_check, precision=P.precision, stream=P.stream)
+    u2 = P2.statevector()
+    P2.transfer_from(P, u, t, u2)
+    P2.stage_limit(u2, t)
+    return P2, u2
+
+
 def indicator_flags(P, case, u, t, ref, G=None, buffer=0, travel=0.0, mask="interior"):
     """indicator_flags / gh_indicator! (src/refinement.jl:973-1025) on a problem's own mesh: the
     masked reference amplitude, tau into the diag field set, then the marks with the level
