@@ -18,7 +18,8 @@ Public surface, named after the reference's:
   gradient   MaskedErrorStudy, MaskedError: the masked error's gradient by forward-mode tangents
 """
 from . import _abi
-from . import refinement
+from . import checkpoint, refinement
+from .checkpoint import latest_checkpoint, load_checkpoint, save_checkpoint
 from .refinement import Refinement, indicator_flags, level_bounds, refine_flags
 from .cases import (Case, gauge_wave_case, horizon_min_radius, kerr_schild_case, minkowski_case,
                     perturbed_minkowski_case, shifted_minkowski_case)
@@ -32,6 +33,7 @@ __all__ = ["Case", "Forest", "GHProblem", "gauge_wave_case", "gh_forest", "hole_
            "minkowski_case", "perturbed_minkowski_case", "shifted_minkowski_case", "horizon_min_radius",
            "fourier_modes", "perturbation", "fp64_peak_tflops", "load_library", "ShardedGHProblem",
            "exchange_plan", "partition", "MaskedError", "MaskedErrorStudy", "Refinement", "indicator_flags",
-           "level_bounds", "refine_flags", "refinement"]
+           "level_bounds", "refine_flags", "refinement", "checkpoint", "latest_checkpoint", "load_checkpoint",
+           "save_checkpoint"]
 
 load_library = _abi.load_library
