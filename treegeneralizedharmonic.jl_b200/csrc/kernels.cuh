@@ -159,12 +159,15 @@ __global__ void transfer_copy_kernel(const CopyPt* __restrict__ pts, long n, con
 #pragma unroll
   for (int v = 0; v < NV; ++v) dst[v * S] = src[v * g.Wv];
 }
+// one thread per (point, variable), consecutive threads on consecutive points of one variable:
+// their coarse stencils are neighbours in memory (the lists are grouped by odd-axis mask, so a
+// warp's points do the same amount of work)
 template <int P>
 __global__ void transfer_prolong_kernel(const ProlongPt* __restrict__ pts, int n, const double* __restrict__ work,
                                         Geo g, double* __restrict__ u, long S) {
   const int id = blockIdx.x * blockDim.x + threadIdx.x;
   if (id >= n * NV) return;
-  const int pi = id / NV, v = id % NV;
+  const int pi = id % n, v = id / n;
   const ProlongPt p = pts[pi];
   u[(long)p.dst_b * NV * S + (long)v * S + p.dst_w] =
       prolong_value<P>(work + (long)p.src_b * NV * g.Wv + (long)v * g.Wv + p.src_w, p.odd, g);
@@ -174,7 +177,7 @@ template <int P>
 __global__ void fill_prolong_kernel(const ProlongPt* __restrict__ pts, int n, double* __restrict__ work, Geo g) {
   const int id = blockIdx.x * blockDim.x + threadIdx.x;
   if (id >= n * NV) return;
-  const int pi = id / NV, v = id % NV;
+  const int pi = id % n, v = id / n;
   const ProlongPt p = pts[pi];
   work[(long)p.dst_b * NV * g.Wv + (long)v * g.Wv + p.dst_w] =
       prolong_value<P>(work + (long)p.src_b * NV * g.Wv + (long)v * g.Wv + p.src_w, p.odd, g);

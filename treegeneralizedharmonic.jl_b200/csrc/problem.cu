@@ -379,7 +379,7 @@ static int build_plan(tgh_problem* p) {
   const auto& runs = hp.runs;
   const auto& gpts = hp.gpts;
   const auto& hooks = hp.hooks;
-  const auto& prol = hp.prol;
+  auto& prol = hp.prol;
   const auto& prim = hp.prim;
   const int nph = p->maxlevel + 1;
   p->xch.assign(nph, ExchangeList{});
@@ -424,6 +424,10 @@ static int build_plan(tgh_problem* p) {
   p->prol.assign(p->maxlevel + 1, nullptr);
   p->nprol.assign(p->maxlevel + 1, 0);
   for (int l = 1; l <= p->maxlevel; ++l) {
+    // grouped by odd-axis mask (a point prolonged along k axes sums 6^k terms), in plan order
+    // within a group, so that a warp's points do the same work
+    std::stable_sort(prol[l].begin(), prol[l].end(),
+                     [](const ProlongPt& a, const ProlongPt& b) { return a.odd < b.odd; });
     p->nprol[l] = (int)prol[l].size();
     CK(cudaMalloc(&p->prol[l], std::max<size_t>(1, prol[l].size()) * sizeof(ProlongPt)));
     if (!prol[l].empty())
@@ -932,6 +936,7 @@ int tgh_transfer(tgh_problem* dst, tgh_problem* src, const double* u_src, double
           pp.push_back(ProlongPt{b, ip, src->g2i[c], sw, odd});
         }
   }
+  std::stable_sort(pp.begin(), pp.end(), [](const ProlongPt& a, const ProlongPt& b) { return a.odd < b.odd; });
   tgh_problem* p = dst;  // where a CUDA failure is reported
   struct Plan {
     CopyPt* cp = nullptr;
