@@ -68,6 +68,10 @@ struct tgh_problem {
   int nhooks = 0;
   double* hook_cache = nullptr;  // stationary cases: the Dirichlet ghosts' values, 20 per point
   bool hook_cache_valid = false;
+  // the batched form's stage buffers whose Dirichlet ghosts already hold a stationary case's
+  // hook: written once, and by nothing else after (the stage epilogue writes owned points, the
+  // copies and the prolongation write ghosts inside the domain)
+  double* hooks_held[2] = {nullptr, nullptr};
   std::vector<ProlongPt*> prol;  // per level 1..maxlevel
   std::vector<int> nprol;
   unsigned long long* scratch = nullptr;  // speed reduction: max bits, non-finite count
@@ -480,6 +484,7 @@ static cudaError_t launch_prolong(tgh_problem* p, int l, double* work) {
 static int launch_hooks(tgh_problem* p, double* work, double t) {
   if (!p->nhooks) return TGH_OK;
   if (p->hook_cache && p->hook_cache_valid) {
+    if (work == p->hooks_held[0] || work == p->hooks_held[1]) return TGH_OK;
     hook_copy_kernel<<<grid_for(p->nhooks, 256), 256, 0, p->stream>>>(p->hooks, p->nhooks, p->hook_cache, work,
                                                                        p->geo);
   } else {
@@ -1145,6 +1150,13 @@ int tgh_step_batched(tgh_problem* p, double* u, double t, double dt, int nsteps)
   if (s) return s;
   // the state into W0's owned points (and ghosts), outside the graph
   if ((s = launch_fill(p, u, false, p->work, t))) return s;
+  // a stationary hook into the two stage buffers once, also outside the graph; the graph's
+  // stage fills of those buffers then skip it
+  if (p->hook_cache && p->hook_cache_valid && !p->hooks_held[0]) {
+    if ((s = launch_hooks(p, p->W1, t)) || (s = launch_hooks(p, p->W2, t))) return s;
+    p->hooks_held[0] = p->W1;
+    p->hooks_held[1] = p->W2;
+  }
   const bool reuse = p->gexec && p->gkey.t == t && p->gkey.dt == dt && p->gkey.nsteps == nsteps;
   if (!reuse) {
     if (p->gexec) {
