@@ -31,6 +31,7 @@
 #include <unordered_map>
 #include <vector>
 
+#include "adm_streamed.hpp"
 #include "physics.hpp"
 #include "pointwise.hpp"
 #include "spacetime.hpp"
@@ -633,7 +634,9 @@ static void gh_constraint_point(const Problem& P, const PointCtx& c, int b, cons
 // d_t d_t blocks from the evolution equations (d_t Pi from gh_node_rhs_expanded, source and
 // damping included, no dissipation), then the Ricci assembly; with matter, H - 16 pi rho and
 // M_i - 8 pi S_i. out: H, M_x, M_y, M_z
-template <class T>
+// STREAMED: the Ricci contraction in the GPU kernel's order (adm_streamed.hpp), for its flop
+// count; the monitors' values use the reference's assembly.
+template <class T, bool STREAMED = false>
 static void adm_constraint_point(const Problem& P, const PointCtx& c, int b, const int I[3], const double x[3],
                                  double t, const double* matter, T out[4]) {
   static const int P3[3][3] = {{0, 1, 2}, {1, 3, 4}, {2, 4, 5}};
@@ -711,7 +714,8 @@ static void adm_constraint_point(const Problem& P, const PointCtx& c, int b, con
       for (int a = 0; a < 4; ++a)
         for (int e = 0; e < 4; ++e) ddg[m][n][a][e] = dd[pairindex(m, n)][pairindex(a, e)];
   T ham, mom[3];
-  adm_constraints_at_node(C.g4, C.gu4, C.alpha, C.beta, dg, ddg, ham, mom);
+  if constexpr (STREAMED) adm_constraints_streamed(C.g4, C.gu4, C.alpha, C.beta, dg, ddg, ham, mom);
+  else adm_constraints_at_node(C.g4, C.gu4, C.alpha, C.beta, dg, ddg, ham, mom);
   if constexpr (std::is_same<T, double>::value) if (matter) {
     const double c8 = 8.0 * M_PI;
     ham = ham - 2.0 * (c8 * rho);
@@ -1083,6 +1087,17 @@ void orc_adm_at_node(const double* h10, const double* dg64, const double* ddg256
   out4[0] = ham;
   for (int a = 0; a < 3; ++a) out4[1 + a] = mom[a];
 }
+// the same with the Ricci tensor contracted in the GPU kernel's order
+void orc_adm_at_node_streamed(const double* h10, const double* dg64, const double* ddg256, double* out4) {
+  Coef<double> C;
+  metric_quantities(h10, C);
+  double dg[4][4][4], ddg[4][4][4][4], ham, mom[3];
+  std::memcpy(dg, dg64, sizeof(dg));
+  std::memcpy(ddg, ddg256, sizeof(ddg));
+  adm_constraints_streamed(C.g4, C.gu4, C.alpha, C.beta, dg, ddg, ham, mom);
+  out4[0] = ham;
+  for (int a = 0; a < 3; ++a) out4[1 + a] = mom[a];
+}
 // out: d alpha, d beta (3), d sqrt(gamma), d gamma^{jk} (9) along the direction of dg10
 void orc_metric_derivatives_along(const double* h10, const double* dg10, double* out14) {
   Coef<double> C;
@@ -1354,7 +1369,8 @@ int orc_count_flops(void* p, double t, long* out) {
 }
 
 // The same count for a constraint monitor at that point (which = 0: the gauge constraint,
-// 1: the ADM constraints, vacuum), on a prepared problem.
+// 1: the ADM constraints, vacuum, the reference's Ricci assembly; 2: the same with the Ricci
+// tensor contracted in the GPU kernel's order), on a prepared problem.
 int orc_count_monitor_flops(void* p, double t, int which, long* out) {
   Problem& P = *(Problem*)p;
   const int I[3] = {P.N / 2, P.N / 2, P.N / 2};
@@ -1363,7 +1379,8 @@ int orc_count_monitor_flops(void* p, double t, int which, long* out) {
   Cnt::nadd = Cnt::nmul = Cnt::ndiv = Cnt::nsqrt = 0;
   Cnt r[4];
   if (which == 0) gh_constraint_point<Cnt>(P, c, 0, I, r);
-  else adm_constraint_point<Cnt>(P, c, 0, I, x, t, nullptr, r);
+  else if (which == 1) adm_constraint_point<Cnt>(P, c, 0, I, x, t, nullptr, r);
+  else adm_constraint_point<Cnt, true>(P, c, 0, I, x, t, nullptr, r);
   out[0] = Cnt::nadd;
   out[1] = Cnt::nmul;
   out[2] = Cnt::ndiv;

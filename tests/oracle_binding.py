@@ -64,6 +64,7 @@ class Oracle:
             "orc_constraint_norms": (ctypes.c_int, [_VP, _DP, ctypes.c_int, ctypes.c_int, _DP]),
             "orc_ddmetric": (None, [ctypes.POINTER(abi.Background), _DP, _DP, _DP, _DP]),
             "orc_adm_at_node": (None, [_DP, _DP, _DP, _DP]),
+            "orc_adm_at_node_streamed": (None, [_DP, _DP, _DP, _DP]),
             "orc_metric_derivatives_along": (None, [_DP, _DP, _DP]),
             "orc_metric_derivatives": (None, [_DP, _DP, _DP]),
             "orc_count_flops": (ctypes.c_int, [_VP, _D, ctypes.POINTER(ctypes.c_long)]),
@@ -153,11 +154,13 @@ class Oracle:
                               _dp(ddg))
         return g.reshape(4, 4), dg.reshape(4, 4, 4), ddg.reshape(4, 4, 4, 4)
 
-    def adm_at_node(self, h, dg, ddg):
-        """(H, M_x, M_y, M_z) of the Ricci assembly at one point of offset h."""
+    def adm_at_node(self, h, dg, ddg, streamed=False):
+        """(H, M_x, M_y, M_z) of the Ricci assembly at one point of offset h (streamed: the
+        contraction in the GPU monitor kernel's order)."""
         out = np.zeros(4)
         a = [np.ascontiguousarray(x, dtype=float).ravel() for x in (h, dg, ddg)]
-        self.lib.orc_adm_at_node(*[_dp(x) for x in a], _dp(out))
+        fn = self.lib.orc_adm_at_node_streamed if streamed else self.lib.orc_adm_at_node
+        fn(*[_dp(x) for x in a], _dp(out))
         return out
 
     def metric_derivatives_along(self, h, dg10):
@@ -277,12 +280,14 @@ class OracleProblem:
 
     def count_flops(self, t, monitor=None):
         """Algorithmic FP64 operations at the centre of block 0 of the prepared problem: the
-        right-hand side, or monitor "gauge" / "adm" (adds + multiplies + divides + roots)."""
+        right-hand side, or monitor "gauge" / "adm" (the Ricci tensor contracted in the GPU
+        kernel's order) / "adm_reference" (the reference's assembly); adds + multiplies +
+        divides + roots."""
         out = (ctypes.c_long * 4)()
         if monitor is None:
             st = self.lib.orc_count_flops(self.h, t, out)
         else:
-            st = self.lib.orc_count_monitor_flops(self.h, t, {"gauge": 0, "adm": 1}[monitor], out)
+            st = self.lib.orc_count_monitor_flops(self.h, t, {"gauge": 0, "adm_reference": 1, "adm": 2}[monitor], out)
         assert st == 0
         return sum(out)
 

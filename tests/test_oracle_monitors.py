@@ -44,6 +44,31 @@ def test_adm_constraints_vanish_on_exact_vacuum_solutions(tgh, oracle):
             assert np.abs(out).max() < 16 * EPS * scale, (name, x, out)
 
 
+def test_the_kernels_ricci_contraction_is_the_references(tgh, oracle):
+    # the GPU monitor contracts the Ricci tensor in another order (first-derivative terms, then
+    # one metric component's second derivatives at a time): the same numbers to roundoff, on the
+    # vacuum solutions and on arbitrary (non-solution) derivatives alike
+    for name, bg in _backgrounds(tgh):
+        for x in POINTS:
+            g, dg, ddg = oracle.ddmetric(bg, np.array([0.3, *x]))
+            scale = max(1.0, np.abs(ddg).max(), np.abs(dg).max() ** 2)
+            a = oracle.adm_at_node(_offset(g), dg, ddg)
+            b = oracle.adm_at_node(_offset(g), dg, ddg, streamed=True)
+            assert np.abs(a - b).max() < 64 * EPS * scale, (name, x, a, b)
+    rng = np.random.default_rng(7)
+    for _ in range(20):
+        m = rng.normal(size=(4, 4))
+        g = ETA + 0.05 * (m + m.T)  # Lorentzian: g^tt < 0, spatial part positive definite
+        assert np.linalg.inv(g)[0, 0] < 0 and np.linalg.eigvalsh(g[1:, 1:]).min() > 0
+        dg = rng.normal(size=(4, 4, 4))
+        dg = 0.5 * (dg + dg.transpose(0, 2, 1))
+        ddg = rng.normal(size=(4, 4, 4, 4))
+        ddg = 0.25 * (ddg + ddg.transpose(1, 0, 2, 3) + ddg.transpose(0, 1, 3, 2) + ddg.transpose(1, 0, 3, 2))
+        a = oracle.adm_at_node(_offset(g), dg, ddg)
+        b = oracle.adm_at_node(_offset(g), dg, ddg, streamed=True)
+        assert np.abs(a - b).max() < 1e-12 * max(1.0, np.abs(a).max()), (a, b)
+
+
 def test_adm_constraints_are_not_vacuous_off_the_solution(tgh, oracle):
     bg = _backgrounds(tgh)[0][1]
     g, dg, ddg = oracle.ddmetric(bg, np.array([0.3, *POINTS[0]]))

@@ -149,14 +149,162 @@ __device__ __forceinline__ void mon_along(const Coef<double>& C, const double* d
   dsq = C.sqrtg * s * 0.5;
 }
 
-// The ADM Hamiltonian and momentum constraints at one owned point: every second derivative of
-// g (the spatial ones from the right-hand side's stencils, d_t d_i g and d_t d_t g from the
-// first evolution equation differentiated once and twice, with d_t Pi from the reduced equation,
-// source and damping included, no dissipation), then the four-dimensional Ricci tensor
+// The first-derivative terms of the four-dimensional Ricci tensor, R_ab for the packed a <= b:
+//   (d_c g^{cd}) Gamma_{d,ab} - (d_b g^{cd}) Gamma_{d,ca} + Gamma^c_cd Gamma^d_ab - Gamma^c_bd Gamma^d_ca
+// with d g^{-1} = -g^{-1} (d g) g^{-1} folded into the contractions: per b, U = g^{-1} d_b g
+// (16 values); the first term is -w_f Gamma^f_ab with w_f = sum_c U_c[c][f]. R_ab is symmetric
+// as a whole (not term by term), so each packed entry is formed once, with b its larger index.
+__device__ __forceinline__ void ricci_first_order(const Coef<double>& C, const double* const D[4], double R[NC]) {
+  double G4[4][NC];  // Gamma^a_bc
+#pragma unroll
+  for (int a = 0; a < 4; ++a)
+#pragma unroll
+    for (int n = 0; n < NC; ++n) {
+      const int b = prow(n), c = pcol(n);
+      double s = 0.0;
+#pragma unroll
+      for (int x = 0; x < 4; ++x) s = fma(C.gu[pidx(a, x)], 0.5 * (D[b][pidx(x, c)] + D[c][pidx(x, b)] - D[x][n]), s);
+      G4[a][n] = s;
+    }
+  double w[4] = {0.0, 0.0, 0.0, 0.0};
+#pragma unroll
+  for (int b = 0; b < 4; ++b) {
+    double U[4][4];  // U[c][f] = g^{ce} d_b g_ef
+#pragma unroll
+    for (int c = 0; c < 4; ++c)
+#pragma unroll
+      for (int f = 0; f < 4; ++f) {
+        double s = 0.0;
+#pragma unroll
+        for (int e = 0; e < 4; ++e) s = fma(C.gu[pidx(c, e)], D[b][pidx(e, f)], s);
+        U[c][f] = s;
+      }
+#pragma unroll
+    for (int f = 0; f < 4; ++f) w[f] += U[b][f];
+#pragma unroll
+    for (int a = 0; a <= b; ++a) {
+      double r = 0.0;
+#pragma unroll
+      for (int c = 0; c < 4; ++c)
+#pragma unroll
+        for (int f = 0; f < 4; ++f) r = fma(U[c][f], G4[f][pidx(c, a)], r);
+#pragma unroll
+      for (int c = 0; c < 4; ++c)
+#pragma unroll
+        for (int d = 0; d < 4; ++d) r = fma(-G4[c][pidx(b, d)], G4[d][pidx(c, a)], r);
+      R[pidx(a, b)] = r;
+    }
+  }
+  double tw[4];  // Gamma^c_cf - w_f
+#pragma unroll
+  for (int f = 0; f < 4; ++f)
+    tw[f] = G4[0][pidx(0, f)] + G4[1][pidx(1, f)] + G4[2][pidx(2, f)] + G4[3][pidx(3, f)] - w[f];
+#pragma unroll
+  for (int n = 0; n < NC; ++n)
+#pragma unroll
+    for (int f = 0; f < 4; ++f) R[n] = fma(tw[f], G4[f][n], R[n]);
+}
+
+// The second-derivative terms of R_ab from the ten second derivatives dv[m] = d_mu d_nu g_v
+// (m the packed (mu nu)) of one metric component v = (al be), added to the packed R:
+//   R_ab += X_ab + X_ba - (1/2) g^{cd} d_c d_d g_ab - (1/2) g^{cd} d_a d_b g_cd,
+//   X_ab = (1/2) g^{cd} d_c d_a g_db,
+// the terms -(1/2) g^{cd} (d_c d_b g_da - d_b d_c g_da) of the full expansion cancelling.
+template <int V>
+__device__ __forceinline__ void ricci_second_order(const Coef<double>& C, const double dv[NC], double R[NC]) {
+  constexpr int al = prow(V), be = pcol(V);
+  const double c3 = (al == be ? -0.5 : -1.0) * C.gu[V];
+  double tr = 0.0;
+#pragma unroll
+  for (int m = 0; m < NC; ++m) {
+    R[m] = fma(c3, dv[m], R[m]);
+    tr = fma(prow(m) == pcol(m) ? C.gu[m] : 2.0 * C.gu[m], dv[m], tr);
+  }
+  R[V] = fma(-0.5, tr, R[V]);
+#pragma unroll
+  for (int a = 0; a < 4; ++a) {
+    double y = 0.0;
+#pragma unroll
+    for (int c = 0; c < 4; ++c) y = fma(C.gu[pidx(c, al)], dv[pidx(c, a)], y);
+    R[pidx(a, be)] = fma(a == be ? 1.0 : 0.5, y, R[pidx(a, be)]);
+    if (al != be) {
+      double z = 0.0;
+#pragma unroll
+      for (int c = 0; c < 4; ++c) z = fma(C.gu[pidx(c, be)], dv[pidx(c, a)], z);
+      R[pidx(a, al)] = fma(a == al ? 1.0 : 0.5, z, R[pidx(a, al)]);
+    }
+  }
+}
+
+// What the ten second derivatives of one component need besides its own stencils: the
+// metric, the shift's and lapse's derivatives along x_i (i = 0..2) and t (3), the divergences
+// and the d_t Pi terms that carry no second derivative.
+struct AdmPoint {
+  Coef<double> C;
+  double phi, am, divb, divA[3];
+  double dphi[4], db[4][3];
+  const double* wk;
+  long Wv, s[3];
+  double ih, ih2;
+};
+
+// Component V's second derivatives d_mu d_nu g_V in packed (mu nu) order: the six spatial ones
+// from the stencils; d_t d_i g and d_t d_t g from the first evolution equation differentiated
+// once and twice, with d_t Pi_V from the reduced equation (src + the principal part).
+template <int Q, int V>
+__device__ __forceinline__ void adm_component(const AdmPoint& P, double src, double dv[NC]) {
+  const double* ph = P.wk + V * P.Wv;
+  const double* pp = ph + NC * P.Wv;
+  const double hc = ph[0], pc = pp[0];
+  // the component's first derivatives are formed again here (the same stencils) rather than
+  // held for all ten components
+  double dh[3], dP[3];
+#pragma unroll
+  for (int d = 0; d < 3; ++d) {
+    dh[d] = P.ih * st_d1<Q, double>(ph, P.s[d]);
+    dP[d] = P.ih * st_d1<Q, double>(pp, P.s[d]);
+  }
+  dv[4] = P.ih2 * st_d2<Q, double>(ph, P.s[0], hc);
+  dv[5] = P.ih2 * st_mixed<Q, double>(ph, P.s[0], P.s[1]);
+  dv[6] = P.ih2 * st_mixed<Q, double>(ph, P.s[0], P.s[2]);
+  dv[7] = P.ih2 * st_d2<Q, double>(ph, P.s[1], hc);
+  dv[8] = P.ih2 * st_mixed<Q, double>(ph, P.s[1], P.s[2]);
+  dv[9] = P.ih2 * st_d2<Q, double>(ph, P.s[2], hc);
+  const Coef<double>& C = P.C;
+  double t0 = C.beta[0] * dP[0] + C.beta[1] * dP[1] + C.beta[2] * dP[2] + P.divb * pc;
+  t0 += P.am * (C.gamu[0] * dv[4] + 2.0 * C.gamu[1] * dv[5] + 2.0 * C.gamu[2] * dv[6] + C.gamu[3] * dv[7] +
+                2.0 * C.gamu[4] * dv[8] + C.gamu[5] * dv[9]);
+  t0 += P.divA[0] * dh[0] + P.divA[1] * dh[1] + P.divA[2] * dh[2];
+  const double dtP = src + t0;
+#pragma unroll
+  for (int i = 0; i < 3; ++i)
+    dv[1 + i] = P.dphi[i] * pc + P.phi * dP[i] +
+                (P.db[i][0] * dh[0] + P.db[i][1] * dh[1] + P.db[i][2] * dh[2]) +
+                (C.beta[0] * dv[pidx(i + 1, 1)] + C.beta[1] * dv[pidx(i + 1, 2)] + C.beta[2] * dv[pidx(i + 1, 3)]);
+  dv[0] = P.dphi[3] * pc + P.phi * dtP + (P.db[3][0] * dh[0] + P.db[3][1] * dh[1] + P.db[3][2] * dh[2]) +
+          (C.beta[0] * dv[1] + C.beta[1] * dv[2] + C.beta[2] * dv[3]);
+}
+
+template <int Q, int V>
+__device__ __forceinline__ void adm_components(const AdmPoint& P, const double src[NC], double R[NC]) {
+  if constexpr (V < NC) {
+    double dv[NC];
+    adm_component<Q, V>(P, src[V], dv);
+    ricci_second_order<V>(P.C, dv, R);
+    adm_components<Q, V + 1>(P, src, R);
+  }
+}
+
+// The ADM Hamiltonian and momentum constraints at one owned point: the four-dimensional Ricci
+// tensor
 //   R_ab = d_c Gamma^c_ab - d_b Gamma^c_ca + Gamma^c_cd Gamma^d_ab - Gamma^c_bd Gamma^d_ca
-// and H = 2 R_nn + R, M_i = -n^a (R_ai - g_ai R / 2), n = (1, -beta) / alpha. With matter, H - 16 pi
-// rho and M_i - 8 pi S_i. A diagnostic: it holds the hundred second derivatives at once and
-// spills, which is the reference's trade as well.
+// from every second derivative of g (the spatial ones from the right-hand side's stencils,
+// d_t d_i g and d_t d_t g from the first evolution equation differentiated once and twice, with
+// d_t Pi from the reduced equation, source and damping included, no dissipation), then
+// H = 2 R_nn + R, M_i = -n^a (R_ai - g_ai R / 2), n = (1, -beta) / alpha. With matter, H - 16 pi
+// rho and M_i - 8 pi S_i. The first-derivative terms are formed first; the hundred second
+// derivatives are then formed component by component and folded into the ten packed R_ab at
+// once, so that no more than ten of them are held (the reference's kernel holds them all).
 template <int Q>
 __global__ void __launch_bounds__(128) adm_constraint_kernel(const Case cs, const MonArgs A) {
   const long p = (long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -170,55 +318,52 @@ __global__ void __launch_bounds__(128) adm_constraint_kernel(const Case cs, cons
     dgo[DG_MASK * A.S] = 0.0;
     return;
   }
-  const long s[3] = {1, A.Wd, (long)A.Wd * A.Wd};
-  const double ih = 1.0 / m.h, ih2 = ih * ih;
-  double hv[NC], Pv[NC], dh[3][NC], dP[3][NC], dd[NC][NC];  // dd[(mu nu)][(ab)] = d_mu d_nu g_ab
+  AdmPoint P;
+  P.wk = m.wk;
+  P.Wv = A.Wv;
+  P.s[0] = 1;
+  P.s[1] = A.Wd;
+  P.s[2] = (long)A.Wd * A.Wd;
+  P.ih = 1.0 / m.h;
+  P.ih2 = P.ih * P.ih;
+  double hv[NC], dh[3][NC];
 #pragma unroll
   for (int v = 0; v < NC; ++v) {
     const double* ph = m.wk + v * A.Wv;
-    const double* pp = ph + NC * A.Wv;
     hv[v] = ph[0];
-    Pv[v] = pp[0];
 #pragma unroll
-    for (int d = 0; d < 3; ++d) {
-      dh[d][v] = ih * st_d1<Q, double>(ph, s[d]);
-      dP[d][v] = ih * st_d1<Q, double>(pp, s[d]);
-    }
-    dd[4][v] = ih2 * st_d2<Q, double>(ph, s[0], hv[v]);
-    dd[5][v] = ih2 * st_mixed<Q, double>(ph, s[0], s[1]);
-    dd[6][v] = ih2 * st_mixed<Q, double>(ph, s[0], s[2]);
-    dd[7][v] = ih2 * st_d2<Q, double>(ph, s[1], hv[v]);
-    dd[8][v] = ih2 * st_mixed<Q, double>(ph, s[1], s[2]);
-    dd[9][v] = ih2 * st_d2<Q, double>(ph, s[2], hv[v]);
+    for (int d = 0; d < 3; ++d) dh[d][v] = P.ih * st_d1<Q, double>(ph, P.s[d]);
   }
-  Coef<double> C;
-  metric_quantities(hv, C);
-  const double phi = C.alpha / C.sqrtg;
-  double dth[NC];
-#pragma unroll
-  for (int v = 0; v < NC; ++v)
-    dth[v] = C.beta[0] * dh[0][v] + C.beta[1] * dh[1][v] + C.beta[2] * dh[2][v] + phi * Pv[v];
-  const double* D[4] = {dth, dh[0], dh[1], dh[2]};
-  // d_t Pi: gh_node_rhs_expanded (src/pointwise.jl:818-850) without the dissipation
-  double dtP[NC];
+  metric_quantities(hv, P.C);
+  const Coef<double>& C = P.C;
+  P.phi = C.alpha / C.sqrtg;
+  P.am = C.alpha * C.sqrtg;
+  double R[NC], src[NC];
   {
-    double Hl[4], dHl[4][4], dHs[NC];
-    mon_gauge(cs, A, m, hv, D, Hl, dHl);
+    double dth[NC];
 #pragma unroll
-    for (int n = 0; n < NC; ++n) dHs[n] = dHl[prow(n)][pcol(n)] + dHl[pcol(n)][prow(n)];
-    gh_source<double, true>(C, D, Hl, dHs, damping_rate(cs, A.t, m.x), cs.g2, dtP);
-    const double* dhp[3] = {dh[0], dh[1], dh[2]};
-    double divb, divA[3];
-    metric_divergences(C, dhp, divb, divA);
-    const double am = C.alpha * C.sqrtg;
+    for (int v = 0; v < NC; ++v)
+      dth[v] = C.beta[0] * dh[0][v] + C.beta[1] * dh[1][v] + C.beta[2] * dh[2][v] + P.phi * m.wk[(NC + v) * A.Wv];
+    const double* D[4] = {dth, dh[0], dh[1], dh[2]};
+    // d_t Pi without its second-derivative terms: gh_node_rhs_expanded (src/pointwise.jl:818-850)
+    // without the dissipation, the source and damping first
+    {
+      double Hl[4], dHl[4][4], dHs[NC];
+      mon_gauge(cs, A, m, hv, D, Hl, dHl);
 #pragma unroll
-    for (int v = 0; v < NC; ++v) {
-      double t0 = C.beta[0] * dP[0][v] + C.beta[1] * dP[1][v] + C.beta[2] * dP[2][v] + divb * Pv[v];
-      t0 += am * (C.gamu[0] * dd[4][v] + 2.0 * C.gamu[1] * dd[5][v] + 2.0 * C.gamu[2] * dd[6][v] +
-                  C.gamu[3] * dd[7][v] + 2.0 * C.gamu[4] * dd[8][v] + C.gamu[5] * dd[9][v]);
-      t0 += divA[0] * dh[0][v] + divA[1] * dh[1][v] + divA[2] * dh[2][v];
-      dtP[v] += t0;
+      for (int n = 0; n < NC; ++n) dHs[n] = dHl[prow(n)][pcol(n)] + dHl[pcol(n)][prow(n)];
+      gh_source<double, true>(C, D, Hl, dHs, damping_rate(cs, A.t, m.x), cs.g2, src);
     }
+    // d alpha, d beta, d sqrt(gamma) along x_i and t
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+      double dal, dsq;
+      mon_along(C, i < 3 ? dh[i] : dth, dal, P.db[i], dsq);
+      P.dphi[i] = (dal - P.phi * dsq) / C.sqrtg;
+    }
+    const double* dhp[3] = {dh[0], dh[1], dh[2]};
+    metric_divergences(C, dhp, P.divb, P.divA);
+    ricci_first_order(C, D, R);
   }
   double rho = 0.0, Sm[3] = {0.0, 0.0, 0.0};
   if (A.matter) {
@@ -228,110 +373,35 @@ __global__ void __launch_bounds__(128) adm_constraint_kernel(const Case cs, cons
     for (int n = 0; n < NC; ++n) mm[n] = q[n * A.S];
     matter_source<double>(C, mm, ms);
 #pragma unroll
-    for (int v = 0; v < NC; ++v) dtP[v] += ms[v];
+    for (int v = 0; v < NC; ++v) src[v] += ms[v];
     rho = mm[0];
     Sm[0] = mm[1];
     Sm[1] = mm[2];
     Sm[2] = mm[3];
   }
-  // d_t d_i g (slots tx, ty, tz) and d_t d_t g (slot tt)
-#pragma unroll
-  for (int i = 0; i < 3; ++i) {
-    double dal, db[3], dsq;
-    mon_along(C, dh[i], dal, db, dsq);
-    const double dphi = (dal - phi * dsq) / C.sqrtg;
-#pragma unroll
-    for (int v = 0; v < NC; ++v)
-      dd[1 + i][v] = dphi * Pv[v] + phi * dP[i][v] + (db[0] * dh[0][v] + db[1] * dh[1][v] + db[2] * dh[2][v]) +
-                     (C.beta[0] * dd[pidx(i + 1, 1)][v] + C.beta[1] * dd[pidx(i + 1, 2)][v] +
-                      C.beta[2] * dd[pidx(i + 1, 3)][v]);
-  }
-  {
-    double dal, db[3], dsq;
-    mon_along(C, dth, dal, db, dsq);
-    const double dphi = (dal - phi * dsq) / C.sqrtg;
-#pragma unroll
-    for (int v = 0; v < NC; ++v)
-      dd[0][v] = dphi * Pv[v] + phi * dtP[v] + (db[0] * dh[0][v] + db[1] * dh[1][v] + db[2] * dh[2][v]) +
-                 (C.beta[0] * dd[1][v] + C.beta[1] * dd[2][v] + C.beta[2] * dd[3][v]);
-  }
-  // the Ricci assembly (adm_constraints_at_node), dg[e][(ab)] = D[e][(ab)]
-  double dgu[4][NC], Gl[4][NC], G4[4][NC], Gtr[4];
-#pragma unroll
-  for (int e = 0; e < 4; ++e)
-#pragma unroll
-    for (int n = 0; n < NC; ++n) {
-      const int a = prow(n), b = pcol(n);
-      double sa = 0.0;
-#pragma unroll
-      for (int c = 0; c < 4; ++c) {
-        double r = 0.0;
-#pragma unroll
-        for (int d = 0; d < 4; ++d) r = fma(D[e][pidx(c, d)], C.gu[pidx(d, b)], r);
-        sa = fma(C.gu[pidx(a, c)], r, sa);
-      }
-      dgu[e][n] = -sa;
-    }
-#pragma unroll
-  for (int a = 0; a < 4; ++a)
-#pragma unroll
-    for (int n = 0; n < NC; ++n) {
-      const int b = prow(n), c = pcol(n);
-      Gl[a][n] = 0.5 * (D[b][pidx(a, c)] + D[c][pidx(a, b)] - D[a][n]);
-    }
-#pragma unroll
-  for (int a = 0; a < 4; ++a)
-#pragma unroll
-    for (int n = 0; n < NC; ++n) {
-      double sa = 0.0;
-#pragma unroll
-      for (int x = 0; x < 4; ++x) sa = fma(C.gu[pidx(a, x)], Gl[x][n], sa);
-      G4[a][n] = sa;
-    }
-#pragma unroll
-  for (int d = 0; d < 4; ++d) Gtr[d] = G4[0][pidx(0, d)] + G4[1][pidx(1, d)] + G4[2][pidx(2, d)] + G4[3][pidx(3, d)];
-  double R[4][4];
-#pragma unroll
-  for (int a = 0; a < 4; ++a)
-#pragma unroll
-    for (int b = 0; b < 4; ++b) {
-      double r = 0.0;
-#pragma unroll
-      for (int c = 0; c < 4; ++c)
-#pragma unroll
-        for (int d = 0; d < 4; ++d) {
-          const double gcd = C.gu[pidx(c, d)];
-          // d_c Gamma^c_ab
-          r = fma(dgu[c][pidx(c, d)], Gl[d][pidx(a, b)], r);
-          r = fma(0.5 * gcd, dd[pidx(c, a)][pidx(d, b)] + dd[pidx(c, b)][pidx(d, a)] - dd[pidx(c, d)][pidx(a, b)], r);
-          // - d_b Gamma^c_ca
-          r = fma(-dgu[b][pidx(c, d)], Gl[d][pidx(c, a)], r);
-          r = fma(-0.5 * gcd, dd[pidx(b, c)][pidx(d, a)] + dd[pidx(b, a)][pidx(d, c)] - dd[pidx(b, d)][pidx(c, a)], r);
-          // - Gamma^c_bd Gamma^d_ca
-          r = fma(-G4[c][pidx(b, d)], G4[d][pidx(c, a)], r);
-        }
-#pragma unroll
-      for (int d = 0; d < 4; ++d) r = fma(Gtr[d], G4[d][pidx(a, b)], r);
-      R[a][b] = r;
-    }
+  adm_components<Q, 0>(P, src, R);
   double Rs = 0.0;
 #pragma unroll
   for (int a = 0; a < 4; ++a)
 #pragma unroll
-    for (int b = 0; b < 4; ++b) Rs = fma(C.gu[pidx(a, b)], R[a][b], Rs);
+    for (int b = 0; b < 4; ++b) Rs = fma(C.gu[pidx(a, b)], R[pidx(a, b)], Rs);
   const double nv[4] = {1.0 / C.alpha, -C.beta[0] / C.alpha, -C.beta[1] / C.alpha, -C.beta[2] / C.alpha};
   double Rnn = 0.0;
 #pragma unroll
   for (int a = 0; a < 4; ++a)
 #pragma unroll
-    for (int b = 0; b < 4; ++b) Rnn = fma(R[a][b] * nv[a], nv[b], Rnn);
+    for (int b = 0; b < 4; ++b) Rnn = fma(R[pidx(a, b)] * nv[a], nv[b], Rnn);
   double ham = 2.0 * Rnn + Rs;
   double mom[3];
 #pragma unroll
   for (int i = 0; i < 3; ++i) {
     double sm = 0.0;
 #pragma unroll
-    for (int a = 0; a < 4; ++a) sm = fma(nv[a], R[a][i + 1] - C.g[pidx(a, i + 1)] * Rs * 0.5, sm);
+    for (int a = 0; a < 4; ++a) {
+      // g_a(i+1) = eta + h, read again
+      const double g = m.wk[pidx(a, i + 1) * A.Wv] + (a == i + 1 ? 1.0 : 0.0);
+      sm = fma(nv[a], R[pidx(a, i + 1)] - g * Rs * 0.5, sm);
+    }
     mom[i] = -sm;
   }
   if (A.matter) {
