@@ -103,6 +103,7 @@ SIGNATURES = {
 EXTRA_SIGNATURES = {
     "tgh_fp64_probe": (ctypes.c_double, [_VP, ctypes.c_int]),
     "tgh_time_rhs": (ctypes.c_int, [_VP, _VP, _D, ctypes.c_int, ctypes.c_int, ctypes.POINTER(_D)]),
+    "tgh_time_monitor": (ctypes.c_int, [_VP, _VP, _D, ctypes.c_int, ctypes.c_int, ctypes.POINTER(_D)]),
     "tgh_copy_hsrc": (ctypes.c_int, [_VP, _VP]),
     "tgh_point_physics": (ctypes.c_int, [_VP, _D, ctypes.POINTER(_D), ctypes.POINTER(_D)]),
     "tgh_last_launch_count": (ctypes.c_int, [_VP, ctypes.POINTER(ctypes.c_long)]),

@@ -1402,6 +1402,35 @@ int tgh_time_rhs(tgh_problem* p, const double* u, double t, int mode, int nlaunc
   return TGH_OK;
 }
 
+// Benchmark aid: the average duration of a constraint monitor's kernel alone (which 0: the
+// gauge constraint, 1: the ADM constraints; interior mask, no matter), timed with CUDA events on
+// the problem's stream over nlaunch launches after one prepare of u at t.
+int tgh_time_monitor(tgh_problem* p, const double* u, double t, int which, int nlaunch, double* ms_per_launch) {
+  if (which != 0 && which != 1) return fail(p, TGH_ERR_ARG, "which must be 0 (gauge) or 1 (ADM)");
+  if (nlaunch < 1) return fail(p, TGH_ERR_ARG, "nlaunch must be positive");
+  MonArgs a;
+  int s = monitor_prepare(p, u, t, TGH_MASK_INTERIOR, a);
+  if (s) return s;
+  auto launch = [&]() {
+    return which == 0 ? launch_gauge_constraint(p->q, p->stream, p->cs, a)
+                      : launch_adm_constraint(p->q, p->stream, p->cs, a);
+  };
+  CK(launch());  // warm
+  cudaEvent_t e0, e1;
+  CK(cudaEventCreate(&e0));
+  CK(cudaEventCreate(&e1));
+  CK(cudaEventRecord(e0, p->stream));
+  for (int i = 0; i < nlaunch; ++i) CK(launch());
+  CK(cudaEventRecord(e1, p->stream));
+  CK(cudaEventSynchronize(e1));
+  float ms = 0;
+  CK(cudaEventElapsedTime(&ms, e0, e1));
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  *ms_per_launch = ms / nlaunch;
+  return TGH_OK;
+}
+
 // ---- the tangent-linear plain form: derivatives of the right-hand side, an RK4 step and the
 // masked error along one direction (the state's tangent and, optionally, one parameter) ----
 

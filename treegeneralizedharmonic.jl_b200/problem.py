@@ -218,6 +218,14 @@ class GHProblem:
         self._check(self.lib.tgh_time_rhs(self._h, _ptr(u), float(t), int(mode), int(nlaunch), ctypes.byref(ms)))
         return ms.value
 
+    def time_monitor(self, u, t, which="adm", nlaunch=5):
+        """Average duration (ms) of a constraint monitor's kernel alone ("gauge" or "adm", the
+        interior mask), CUDA events on this problem's stream after one prepare of u at t."""
+        ms = ctypes.c_double()
+        w = {"gauge": 0, "adm": 1}[which]
+        self._check(self.lib.tgh_time_monitor(self._h, _ptr(u), float(t), w, int(nlaunch), ctypes.byref(ms)))
+        return ms.value
+
     def last_launch_count(self):
         """Kernels the last step_batched call launched: the fill of u, the captured graph's
         kernel nodes and the gather."""
