@@ -72,6 +72,9 @@ struct tgh_problem {
   // hook: written once, and by nothing else after (the stage epilogue writes owned points, the
   // copies and the prolongation write ghosts inside the domain)
   double* hooks_held[2] = {nullptr, nullptr};
+  // set while the batched form's graph is captured: W0's Dirichlet ghosts are written by the
+  // fill that precedes every launch of that graph, and nothing inside the graph overwrites them
+  bool capturing = false;
   std::vector<ProlongPt*> prol;  // per level 1..maxlevel
   std::vector<int> nprol;
   unsigned long long* scratch = nullptr;  // speed reduction: max bits, non-finite count
@@ -484,7 +487,7 @@ static cudaError_t launch_prolong(tgh_problem* p, int l, double* work) {
 static int launch_hooks(tgh_problem* p, double* work, double t) {
   if (!p->nhooks) return TGH_OK;
   if (p->hook_cache && p->hook_cache_valid) {
-    if (work == p->hooks_held[0] || work == p->hooks_held[1]) return TGH_OK;
+    if (work == p->hooks_held[0] || work == p->hooks_held[1] || (p->capturing && work == p->work)) return TGH_OK;
     hook_copy_kernel<<<grid_for(p->nhooks, 256), 256, 0, p->stream>>>(p->hooks, p->nhooks, p->hook_cache, work,
                                                                        p->geo);
   } else {
@@ -1171,8 +1174,10 @@ int tgh_step_batched(tgh_problem* p, double* u, double t, double dt, int nsteps)
     p->stream = p->cap;
     cudaError_t eb = cudaStreamBeginCapture(p->cap, cudaStreamCaptureModeThreadLocal);
     int st = TGH_OK;
+    p->capturing = true;
     if (eb == cudaSuccess)
       for (int n = 0; n < nsteps && st == TGH_OK; ++n) st = batched_step(p, t + n * dt, dt);
+    p->capturing = false;
     cudaError_t ee = eb == cudaSuccess ? cudaStreamEndCapture(p->cap, &graph) : eb;
     p->stream = user;
     if (st) return st;
