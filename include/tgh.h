@@ -20,6 +20,8 @@
  *                                                          tgh_step_batched (fused, graph-captured form)
  *   error_norms / gh_error_kernel! src/constraints.jl:311-396, 716-792
  *                                                          tgh_error_norm
+ *   apply_bounds! / gh_stage_limiter!, StateBounds         tgh_apply_bounds, tgh_set_bounds,
+ *     src/bounds.jl:81-175, 458-663, 686-825              tgh_bounds_check, tgh_bounds_accounting
  *   gh_constraint!, adm_constraint!, constraint_norms     tgh_gh_constraint,
  *     src/constraints.jl:211-271, 432-532, 559-609, 848    tgh_adm_constraint,
  *                                                          tgh_constraint_norms
@@ -225,6 +227,33 @@ int tgh_transfer(tgh_problem* dst, tgh_problem* src, const double* u_src, double
 /* the diag field set: its length in doubles, and a copy of it into a device buffer */
 size_t tgh_diag_length(const tgh_problem* p);
 int tgh_copy_diag(tgh_problem* p, double* out);
+
+/* --- the range projection of the stage limiter (src/bounds.jl:81-175, 458-663, 686-825) ---
+ * tgh_bounds is StateBounds: alpha_min <= alpha <= alpha_max (the lapse, alpha^2 =
+ *   beta_i beta^i - g_tt), lambda_min <= every eigenvalue of gamma_ij <= lambda_max,
+ *   |beta| = sqrt(beta_i gamma^ij beta_j) <= beta_max, max_ab |(alpha/sqrt(gamma)) Pi_ab| <= K_max,
+ *   held at the points r < r_gate from the interior's centre.
+ * tgh_bounds_check: StateBounds' own checks (every bound finite, 0 < alpha_min < 1 < alpha_max,
+ *   0 < lambda_min < 1 < lambda_max, beta_max, K_max and r_gate positive). Host only; errbuf
+ *   (nullable) receives the reason.
+ * tgh_apply_bounds: apply_bounds!: bounds_project at every owned point of the device state
+ *   vector u with r < r_gate, written back only where it fired (a point it leaves alone keeps
+ *   its bits), and over the primary copies the number of points it fired at, of those with a
+ *   non-finite component, and the largest r it fired at (0 when none). Needs an interior.
+ * tgh_set_bounds: the problem's bounds (NULL: none). The stage and step limiters (and so
+ *   tgh_rk4_step and tgh_initial_state) then apply the projection before the :pasted paste and
+ *   add its counts to the problem's accounting, reset here; the batched form refuses a
+ *   problem with bounds.
+ * tgh_bounds_accounting: BoundsAccounting's totals: counts3 = calls, hits, non-finite hits;
+ *   vals3 = the largest r fired at, the t and r of the first call that fired (NaN before). */
+typedef struct {
+  double alpha_min, alpha_max, lambda_min, lambda_max, beta_max, K_max, r_gate;
+} tgh_bounds;
+int tgh_bounds_check(const tgh_bounds* b, char* errbuf, int errlen);
+int tgh_apply_bounds(tgh_problem* p, double* u, double t, const tgh_bounds* b, long* fired, long* nonfinite,
+                     double* r_max);
+int tgh_set_bounds(tgh_problem* p, const tgh_bounds* b);
+int tgh_bounds_accounting(const tgh_problem* p, long* counts3, double* vals3);
 
 /* --- allocation-free speed (no counterpart in the reference) ---
  * tgh_max_speed without a problem handle, for callers that cannot allocate device memory

@@ -11,6 +11,7 @@
 //   gh_error_kernel!, masked volume-weighted L2                       src/constraints.jl:311-396, 716-792
 //   sample_gauge_source!, gauge_at                                    src/gauge.jl:156-212
 //   initial_state!, stage_limit!, gh_paste_kernel!                    src/stepping.jl:91-115, src/evolution.jl:888-905
+//   bounds_project, gh_bounds_kernel! (bounds.hpp)                    src/bounds.jl:256-663
 // and of the un-vendored packages under it (no exact pin; compat bounds only):
 //   TreeAMR 0.3: closed vertex-centered blocks, scatter!, fill_ghosts! (same-level copies
 //     from the primary copy, restriction by injection, the Dirichlet CellBoundary hook,
@@ -32,6 +33,7 @@
 #include <vector>
 
 #include "adm_streamed.hpp"
+#include "bounds.hpp"
 #include "physics.hpp"
 #include "pointwise.hpp"
 #include "spacetime.hpp"
@@ -1365,6 +1367,68 @@ int orc_count_flops(void* p, double t, long* out) {
   out[1] = Cnt::nmul;
   out[2] = Cnt::ndiv;
   out[3] = Cnt::nsqrt;
+  return TGH_OK;
+}
+
+// bounds_project (src/bounds.jl:458-527) at one point: h10, P10 in; the projected state out,
+// flags2 = (hit, nonfinite). bd7: alpha_min, alpha_max, lambda_min, lambda_max, beta_max, K_max,
+// r_gate.
+void orc_bounds_project(const double* h10, const double* P10, const double* bd7, double* hout, double* Pout,
+                        int* flags2) {
+  Bounds bd{bd7[0], bd7[1], bd7[2], bd7[3], bd7[4], bd7[5], bd7[6]};
+  for (int v = 0; v < 10; ++v) {
+    hout[v] = h10[v];
+    Pout[v] = P10[v];
+  }
+  bool nf = false;
+  flags2[0] = bounds_project(hout, Pout, bd, nf) ? 1 : 0;
+  flags2[1] = nf ? 1 : 0;
+}
+
+// gh_bounds_kernel! (src/bounds.jl:635-663) over a state vector u in place: every owned point
+// at interior radius r < r_gate is projected and written back only where it fired. Counted
+// over the primary copies (each lattice point once): fired, non-finite, and the largest r at
+// which it fired (0 when none).
+int orc_apply_bounds(void* p, double* u, double t, const double* bd7, long* fired, long* nonfinite, double* rmax) {
+  Problem& P = *(Problem*)p;
+  Bounds bd{bd7[0], bd7[1], bd7[2], bd7[3], bd7[4], bd7[5], bd7[6]};
+  const size_t S = P.npt_state();
+  long nf = 0, nn = 0;
+  double rm = 0.0;
+  for (int b = 0; b < P.nb; ++b)
+    for (int k = 0; k < P.N1; ++k)
+      for (int j = 0; j < P.N1; ++j)
+        for (int i = 0; i < P.N1; ++i) {
+          double x[3];
+          int64_t n[3] = {(int64_t)P.corner[3 * b] + i, (int64_t)P.corner[3 * b + 1] + j,
+                          (int64_t)P.corner[3 * b + 2] + k};
+          P.position(P.level[b], n, x);
+          const double r = P.in.radius(t, x);
+          if (!(r < bd.r_gate)) continue;
+          const size_t o = (size_t)b * NV * S + i + P.N1 * (j + (size_t)P.N1 * k);
+          double h[10], Pi[10];
+          for (int v = 0; v < 10; ++v) {
+            h[v] = u[o + v * S];
+            Pi[v] = u[o + (10 + v) * S];
+          }
+          bool nfin = false;
+          const bool hit = bounds_project(h, Pi, bd, nfin);
+          if (hit)
+            for (int v = 0; v < 10; ++v) {
+              u[o + v * S] = h[v];
+              u[o + (10 + v) * S] = Pi[v];
+            }
+          if (is_primary(P, b, i, j, k)) {
+            if (hit) {
+              ++nf;
+              rm = std::fmax(rm, r);
+            }
+            if (nfin) ++nn;
+          }
+        }
+  *fired = nf;
+  *nonfinite = nn;
+  *rmax = rm;
   return TGH_OK;
 }
 

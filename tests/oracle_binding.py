@@ -73,6 +73,9 @@ class Oracle:
             "orc_firing": (ctypes.c_int, [_VP, _DP, ctypes.c_int, _DP, ctypes.POINTER(ctypes.c_int),
                                           ctypes.POINTER(ctypes.c_int)]),
             "orc_count_monitor_flops": (ctypes.c_int, [_VP, _D, ctypes.c_int, ctypes.POINTER(ctypes.c_long)]),
+            "orc_bounds_project": (None, [_DP, _DP, _DP, _DP, _DP, ctypes.POINTER(ctypes.c_int)]),
+            "orc_apply_bounds": (ctypes.c_int, [_VP, _DP, _D, _DP, ctypes.POINTER(ctypes.c_long),
+                                                ctypes.POINTER(ctypes.c_long), ctypes.POINTER(_D)]),
         }
         for name, (res, args) in sig.items():
             fn = getattr(lib, name)
@@ -134,6 +137,14 @@ class Oracle:
         self.lib.orc_background_state(ctypes.byref(bg), t, _dp(np.ascontiguousarray(x, dtype=float)), _dp(h),
                                       _dp(Pi), _dp(dh), _dp(dtg))
         return h, Pi, dh.reshape(3, 10), dtg
+
+    def bounds_project(self, h, Pi, bounds):
+        """bounds_project(h, Pi, bounds) at one point: (h', Pi', hit, nonfinite); bounds is the
+        7-tuple (alpha_min, alpha_max, lambda_min, lambda_max, beta_max, K_max, r_gate)."""
+        ho, Po, fl = np.zeros(10), np.zeros(10), (ctypes.c_int * 2)()
+        a = [np.ascontiguousarray(x, dtype=float) for x in (h, Pi, bounds)]
+        self.lib.orc_bounds_project(*[_dp(x) for x in a], _dp(ho), _dp(Po), fl)
+        return ho, Po, bool(fl[0]), bool(fl[1])
 
     def gauge_source_grad(self, bg, p):
         Hl, dHl = np.zeros(4), np.zeros(16)
@@ -290,6 +301,14 @@ class OracleProblem:
             st = self.lib.orc_count_monitor_flops(self.h, t, {"gauge": 0, "adm_reference": 1, "adm": 2}[monitor], out)
         assert st == 0
         return sum(out)
+
+    def apply_bounds(self, u, t, bounds):
+        """gh_bounds_kernel! over the state vector u in place; counts over the primaries."""
+        fired, nonfin, rmax = ctypes.c_long(), ctypes.c_long(), ctypes.c_double()
+        b = np.ascontiguousarray(bounds, dtype=float)
+        assert self.lib.orc_apply_bounds(self.h, _dp(u), t, _dp(b), ctypes.byref(fired), ctypes.byref(nonfin),
+                                         ctypes.byref(rmax)) == 0
+        return {"fired": fired.value, "nonfinite": nonfin.value, "r_max": rmax.value}
 
     def constraint_norms(self, diag, weighting="volume", at_level=None):
         out = np.zeros(16)

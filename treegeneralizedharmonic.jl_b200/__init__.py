@@ -18,7 +18,8 @@ Public surface, named after the reference's:
   gradient   MaskedErrorStudy, MaskedError: the masked error's gradient by forward-mode tangents
 """
 from . import _abi
-from . import checkpoint, refinement
+from . import bounds, checkpoint, refinement
+from .bounds import StateBounds, check_bounds_gate, default_bounds, default_gate, layer_spacing
 from .checkpoint import latest_checkpoint, load_checkpoint, save_checkpoint
 from .refinement import Refinement, indicator_flags, level_bounds, refine_flags
 from .cases import (Case, gauge_wave_case, horizon_min_radius, kerr_schild_case, minkowski_case,
@@ -29,7 +30,7 @@ from .problem import GHProblem, fp64_peak_tflops
 from .shard import ShardedGHProblem, exchange_plan, partition
 from .gradient import MaskedError, MaskedErrorStudy
 
-__all__ = ["Case", "Forest", "GHProblem", "gauge_wave_case", "gh_forest", "hole_forest", "kerr_schild_case",
+__all__ = ["StateBounds", "check_bounds_gate", "default_bounds", "default_gate", "layer_spacing", "Case", "Forest", "GHProblem", "gauge_wave_case", "gh_forest", "hole_forest", "kerr_schild_case",
            "minkowski_case", "perturbed_minkowski_case", "shifted_minkowski_case", "horizon_min_radius",
            "fourier_modes", "perturbation", "fp64_peak_tflops", "load_library", "ShardedGHProblem",
            "exchange_plan", "partition", "MaskedError", "MaskedErrorStudy", "Refinement", "indicator_flags",

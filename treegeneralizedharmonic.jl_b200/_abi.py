@@ -53,6 +53,12 @@ class Mesh(ctypes.Structure):
 # every entry point include/tgh.h declares, with its ctypes signature
 _VP = ctypes.c_void_p
 _D = ctypes.c_double
+class BoundsC(ctypes.Structure):
+    """tgh_bounds: StateBounds (src/bounds.jl:81-147)."""
+    _fields_ = [(n, ctypes.c_double) for n in ("alpha_min", "alpha_max", "lambda_min", "lambda_max", "beta_max",
+                                               "K_max", "r_gate")]
+
+
 SIGNATURES = {
     "tgh_problem_create": (ctypes.c_int, [ctypes.POINTER(Config), ctypes.POINTER(Mesh), _VP, ctypes.c_int,
                                           ctypes.POINTER(_VP)]),
@@ -81,6 +87,11 @@ SIGNATURES = {
     "tgh_transfer": (ctypes.c_int, [_VP, _VP, _VP, _D, _VP]),
     "tgh_diag_length": (ctypes.c_size_t, [_VP]),
     "tgh_copy_diag": (ctypes.c_int, [_VP, _VP]),
+    "tgh_bounds_check": (ctypes.c_int, [ctypes.POINTER(BoundsC), ctypes.c_char_p, ctypes.c_int]),
+    "tgh_apply_bounds": (ctypes.c_int, [_VP, _VP, _D, ctypes.POINTER(BoundsC), ctypes.POINTER(ctypes.c_long),
+                                        ctypes.POINTER(ctypes.c_long), ctypes.POINTER(_D)]),
+    "tgh_set_bounds": (ctypes.c_int, [_VP, ctypes.POINTER(BoundsC)]),
+    "tgh_bounds_accounting": (ctypes.c_int, [_VP, ctypes.POINTER(ctypes.c_long), ctypes.POINTER(_D)]),
     "tgh_max_speed_noalloc": (ctypes.c_int, [ctypes.POINTER(Config), ctypes.POINTER(Mesh), _VP, _D, _VP,
                                              ctypes.POINTER(_D), ctypes.c_char_p, ctypes.c_int]),
     "tgh_tangent_rhs": (ctypes.c_int, [_VP, _VP, _VP, _VP, _VP, _D, ctypes.c_int]),

@@ -13,6 +13,7 @@
 #include <vector>
 
 #include "../../include/tgh.h"
+#include "bounds.cuh"
 #include "kernels.cuh"
 #include "monitors.cuh"
 #include "rhs_inst.cuh"
@@ -78,6 +79,12 @@ struct tgh_problem {
   std::vector<ProlongPt*> prol;  // per level 1..maxlevel
   std::vector<int> nprol;
   unsigned long long* scratch = nullptr;  // speed reduction: max bits, non-finite count
+  unsigned long long* bcounts = nullptr;  // the range projection's counts: fired, non-finite, max r bits
+  // the range projection the limiters apply (set by tgh_set_bounds), and its accounting
+  bool has_bounds = false;
+  tgh_bounds bounds{};
+  long acc_calls = 0, acc_hits = 0, acc_nonfinite = 0;
+  double acc_rmax = 0.0, acc_first_t = NAN, acc_first_r = NAN;
   double* part = nullptr;                 // error-norm partials + result
   double* diag = nullptr;                 // the monitors' diag field set (NDIAG slots per block)
   double* dpart = nullptr;                // constraint-norm partials (17 per CTA) + the fold
@@ -573,7 +580,83 @@ static RhsArgs base_args(tgh_problem* p, const double* work, double t) {
   return a;
 }
 
+// StateBounds' checks (src/bounds.jl:81-147): "" when the ranges are acceptable
+static std::string bounds_problem(const tgh_bounds& b) {
+  const double v[7] = {b.alpha_min, b.alpha_max, b.lambda_min, b.lambda_max, b.beta_max, b.K_max, b.r_gate};
+  for (double x : v)
+    if (!std::isfinite(x))
+      return "every bound must be finite: a bound at infinity is no bound, and it is spelled by setting "
+             "no bounds";
+  if (!(0 < b.alpha_min && b.alpha_min < 1 && 1 < b.alpha_max))
+    return "the lapse range needs 0 < alpha_min < 1 < alpha_max, got alpha_min = " + std::to_string(b.alpha_min) +
+           " and alpha_max = " + std::to_string(b.alpha_max) +
+           ": flat space's alpha = 1 must lie inside, since a non-finite component is repaired to its "
+           "Minkowski value";
+  if (!(0 < b.lambda_min && b.lambda_min < 1 && 1 < b.lambda_max))
+    return "the spatial metric's eigenvalue range needs 0 < lambda_min < 1 < lambda_max, got lambda_min = " +
+           std::to_string(b.lambda_min) + " and lambda_max = " + std::to_string(b.lambda_max);
+  if (!(b.beta_max > 0)) return "the shift's norm bound must be positive, got beta_max = " + std::to_string(b.beta_max);
+  if (!(b.K_max > 0)) return "the momentum's scale bound must be positive, got K_max = " + std::to_string(b.K_max);
+  if (!(b.r_gate > 0))
+    return "the gate radius must be positive, got r_gate = " + std::to_string(b.r_gate) +
+           ": a projection that never runs is spelled by setting no bounds";
+  return "";
+}
+
+// apply_bounds! (src/bounds.jl:749-779): the projection over u, its counts over the primaries
+static int apply_bounds_impl(tgh_problem* p, double* u, double t, const tgh_bounds& b, long* fired, long* nonfinite,
+                             double* rmax) {
+  const std::string why = bounds_problem(b);
+  if (!why.empty()) return fail(p, TGH_ERR_ARG, why);
+  if (!p->intr) return fail(p, TGH_ERR_ARG, "the range projection's gate is a radius from the interior's centre; "
+                                            "this problem has no interior");
+  BoundsArgs a;
+  a.u = u;
+  a.blk = p->blk;
+  a.primary = p->primary;
+  a.counts = p->bcounts;
+  a.amin = b.alpha_min;
+  a.amax = b.alpha_max;
+  a.lmin = b.lambda_min;
+  a.lmax = b.lambda_max;
+  a.bmax = b.beta_max;
+  a.kmax = b.K_max;
+  a.rgate = b.r_gate;
+  a.t = t;
+  a.S = p->S;
+  a.npts = p->npts;
+  a.N1 = p->N1;
+  CK(launch_bounds_projection(p->stream, p->cs, a));
+  unsigned long long h[3];
+  CK(cudaMemcpyAsync(h, p->bcounts, sizeof(h), cudaMemcpyDeviceToHost, p->stream));
+  CK(cudaStreamSynchronize(p->stream));
+  *fired = (long)h[0];
+  *nonfinite = (long)h[1];
+  double r;
+  std::memcpy(&r, &h[2], sizeof(r));
+  *rmax = r;
+  return TGH_OK;
+}
+
+// gh_stage_limiter! then gh_step_limiter! (src/stepping.jl:91-95): the range projection, when
+// the problem has bounds, with its accounting (src/bounds.jl:757-776); then the :pasted paste
 static int stage_limit_impl(tgh_problem* p, double* u, double t) {
+  if (p->has_bounds) {
+    long n = 0, nf = 0;
+    double rm = 0.0;
+    int s = apply_bounds_impl(p, u, t, p->bounds, &n, &nf, &rm);
+    if (s) return s;
+    ++p->acc_calls;
+    if (n > 0) {
+      p->acc_hits += n;
+      p->acc_nonfinite += nf;
+      p->acc_rmax = std::max(p->acc_rmax, rm);
+      if (std::isnan(p->acc_first_t)) {
+        p->acc_first_t = t;
+        p->acc_first_r = rm;
+      }
+    }
+  }
   if (p->cfg.interior != TGH_INT_PASTED) return TGH_OK;
   exact_state_kernel<<<grid_for(p->npts, 128), 128, 0, p->stream>>>(u, p->blk, p->geo, p->npts, p->cs, t, 1);
   CK(cudaGetLastError());
@@ -703,6 +786,7 @@ static int setup_device(tgh_problem* p) {
   CK(cudaMalloc(&p->work, (size_t)p->Wv * NV * p->nwb * sizeof(double)));
   CK(cudaMemsetAsync(p->work, 0, (size_t)p->Wv * NV * p->nwb * sizeof(double), p->stream));
   CK(cudaMalloc(&p->scratch, 2 * sizeof(unsigned long long)));
+  CK(cudaMalloc(&p->bcounts, 3 * sizeof(unsigned long long)));
   CK(cudaMalloc(&p->coef, (size_t)NCOEF * p->npts * sizeof(double)));
   p->npart = (int)grid_for(p->npts, 128);
   CK(cudaMalloc(&p->part, (3 * (size_t)p->npart + 2) * sizeof(double)));
@@ -745,6 +829,7 @@ void tgh_problem_destroy(tgh_problem* p) {
     if (x.recv) cudaFree(x.recv);
   }
   void* bufs[] = {p->work, p->Hsrc, p->blk, p->primary, p->runs, p->gpts, p->hooks, p->hook_cache, p->scratch,
+                  p->bcounts,
                   p->part, p->coef, p->diag, p->dpart, p->ind, p->ind_tol, p->ind_counts, p->ind_boxes, p->dwprol,
                   p->k, p->acc, p->y, p->u0, p->W1, p->W2, p->bacc, p->twork, p->kt, p->acct, p->yt};
   for (void* b : bufs)
@@ -1007,6 +1092,47 @@ int tgh_settle(tgh_problem* p, double* u, double t) {
 }
 
 int tgh_stage_limit(tgh_problem* p, double* u, double t) { return stage_limit_impl(p, u, t); }
+
+int tgh_bounds_check(const tgh_bounds* b, char* errbuf, int errlen) {
+  const std::string why = b ? bounds_problem(*b) : std::string("no bounds given");
+  if (why.empty()) return TGH_OK;
+  if (errbuf && errlen > 0) {
+    std::strncpy(errbuf, why.c_str(), (size_t)errlen - 1);
+    errbuf[errlen - 1] = 0;
+  }
+  return TGH_ERR_ARG;
+}
+
+int tgh_apply_bounds(tgh_problem* p, double* u, double t, const tgh_bounds* b, long* fired, long* nonfinite,
+                     double* r_max) {
+  if (!b) return fail(p, TGH_ERR_ARG, "no bounds given");
+  return apply_bounds_impl(p, u, t, *b, fired, nonfinite, r_max);
+}
+
+int tgh_set_bounds(tgh_problem* p, const tgh_bounds* b) {
+  if (b) {
+    const std::string why = bounds_problem(*b);
+    if (!why.empty()) return fail(p, TGH_ERR_ARG, why);
+    if (!p->intr) return fail(p, TGH_ERR_ARG, "the range projection's gate is a radius from the interior's centre; "
+                                              "this problem has no interior");
+    p->bounds = *b;
+  }
+  p->has_bounds = b != nullptr;
+  p->acc_calls = p->acc_hits = p->acc_nonfinite = 0;
+  p->acc_rmax = 0.0;
+  p->acc_first_t = p->acc_first_r = NAN;
+  return TGH_OK;
+}
+
+int tgh_bounds_accounting(const tgh_problem* p, long* counts3, double* vals3) {
+  counts3[0] = p->acc_calls;
+  counts3[1] = p->acc_hits;
+  counts3[2] = p->acc_nonfinite;
+  vals3[0] = p->acc_rmax;
+  vals3[1] = p->acc_first_t;
+  vals3[2] = p->acc_first_r;
+  return TGH_OK;
+}
 int tgh_step_limit(tgh_problem* p, double* u, double t) { return stage_limit_impl(p, u, t); }
 
 int tgh_initial_state(tgh_problem* p, double* u, double t) {
@@ -1149,6 +1275,7 @@ int tgh_step_batched(tgh_problem* p, double* u, double t, double dt, int nsteps)
   if (nsteps < 1) return fail(p, TGH_ERR_ARG, "nsteps must be positive");
   if (p->cfg.interior == TGH_INT_PASTED)
     return fail(p, TGH_ERR_ARG, "the batched form has no :pasted limiter; use tgh_rk4_step");
+  if (p->has_bounds) return fail(p, TGH_ERR_ARG, "the batched form has no range projection; use tgh_rk4_step");
   int s = batched_buffers(p);
   if (s) return s;
   // the state into W0's owned points (and ghosts), outside the graph
@@ -1302,6 +1429,7 @@ int tgh_shard_counts(tgh_problem* p, int phase, long* send_count, long* recv_cou
 int tgh_shard_begin(tgh_problem* p, const double* u) {
   if (p->cfg.interior == TGH_INT_PASTED)
     return fail(p, TGH_ERR_ARG, "the batched form has no :pasted limiter; use tgh_rk4_step");
+  if (p->has_bounds) return fail(p, TGH_ERR_ARG, "the batched form has no range projection; use tgh_rk4_step");
   int s = batched_buffers(p);
   if (s) return s;
   scatter_owned_kernel<<<grid_for(p->npts, 256), 256, 0, p->stream>>>(u, p->work, p->geo, p->npts);

@@ -177,6 +177,27 @@ class GHProblem:
         self._check(self.lib.tgh_copy_diag(self._h, _ptr(d)))
         return d
 
+    # ---- the range projection (src/bounds.jl:458-825) ----
+    def apply_bounds(self, u, t, bounds):
+        """apply_bounds!: bounds_project at every owned point of u with r < r_gate, written back
+        only where it fired. Returns the counts over the primary copies: fired, nonfinite, r_max."""
+        fired, nonfin, rmax = ctypes.c_long(), ctypes.c_long(), ctypes.c_double()
+        self._check(self.lib.tgh_apply_bounds(self._h, _ptr(u), float(t), ctypes.byref(bounds.to_c()),
+                                              ctypes.byref(fired), ctypes.byref(nonfin), ctypes.byref(rmax)))
+        return {"fired": fired.value, "nonfinite": nonfin.value, "r_max": rmax.value}
+
+    def set_bounds(self, bounds):
+        """The bounds the stage and step limiters apply (None: none); resets the accounting. The
+        batched form refuses a problem with bounds."""
+        self._check(self.lib.tgh_set_bounds(self._h, ctypes.byref(bounds.to_c()) if bounds is not None else None))
+        return self
+
+    def bounds_accounting(self):
+        """BoundsAccounting's totals since set_bounds: calls, hits, nonfinite, r_max, first_t, first_r."""
+        n, v = (ctypes.c_long * 3)(), (ctypes.c_double * 3)()
+        self._check(self.lib.tgh_bounds_accounting(self._h, n, v))
+        return {"calls": n[0], "hits": n[1], "nonfinite": n[2], "r_max": v[0], "first_t": v[1], "first_r": v[2]}
+
     # ---- derivatives: the tangent-linear plain form (include/tgh.h) ----
     TANGENTS = {"state": 0, "rho_max": 1, "ramp": 2, "damp_near": 3}
 
