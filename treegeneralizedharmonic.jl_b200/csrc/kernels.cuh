@@ -117,33 +117,69 @@ __global__ void hook_copy_kernel(const HookPt* __restrict__ pts, int n, const do
 
 // tensor-product Lagrange prolongation of order P from the coarse block's filled working
 // array, summed with x innermost, then y, then z; products and sums rounded one by one
-__constant__ double c_wprol[10];
 
-// one variable's prolonged value from its coarse stencil base `src`, x summed innermost, each
-// product and sum rounded on its own
-template <int P> __device__ __forceinline__ double prolong_value(const double* src, int odd, Geo g) {
-  const int cx = (odd & 1) ? P : 1, cy = (odd & 2) ? P : 1, cz = (odd & 4) ? P : 1;
+// The Lagrange weights of P points at the midpoint of the middle pair: exact rationals,
+// w_k = prod_{m != k} (0 - x_m) / (x_k - x_m) with x_m = m - (P/2 - 1) - 1/2, numerator and
+// denominator formed in integers (doubled units) and divided once.
+template <int P> struct ProlongWeights {
+  double v[P];
+};
+template <int P> __host__ __device__ constexpr ProlongWeights<P> prolong_weights() {
+  ProlongWeights<P> r{};
+  for (int k = 0; k < P; ++k) {
+    long long num = 1, den = 1;
+    for (int m = 0; m < P; ++m) {
+      if (m == k) continue;
+      const long long xm = 2 * (m - (P / 2 - 1)) - 1, xk = 2 * (k - (P / 2 - 1)) - 1;
+      num *= -xm;
+      den *= xk - xm;
+    }
+    r.v[k] = (double)num / (double)den;
+  }
+  return r;
+}
+
+// one variable's prolonged value from its coarse stencil base `src` along the odd axes ODD (a
+// bit per axis): every loop and weight fixed at compile time. An axis that does not
+// interpolate contributes its one value with weight 1 (the product is the value).
+template <int P, int ODD> __device__ __forceinline__ double prolong_odd(const double* src, Geo g) {
+  constexpr int cx = (ODD & 1) ? P : 1, cy = (ODD & 2) ? P : 1, cz = (ODD & 4) ? P : 1;
+  constexpr ProlongWeights<P> W = prolong_weights<P>();
   const long sy = g.Wd, sz = (long)g.Wd * g.Wd;
   double szv = 0.0;
+#pragma unroll
   for (int kz = 0; kz < cz; ++kz) {
-    const double wz = cz == 1 ? 1.0 : c_wprol[kz];
     double syv = 0.0;
+#pragma unroll
     for (int ky = 0; ky < cy; ++ky) {
-      const double wy = cy == 1 ? 1.0 : c_wprol[ky];
       double sxv = 0.0;
       const double* row = src + kz * sz + ky * sy;
+#pragma unroll
       for (int kx = 0; kx < cx; ++kx) {
-        const double wx = cx == 1 ? 1.0 : c_wprol[kx];
-        const double term = __dmul_rn(wx, row[kx]);
+        const double term = cx == 1 ? row[kx] : __dmul_rn(W.v[kx], row[kx]);
         sxv = kx == 0 ? term : __dadd_rn(sxv, term);
       }
-      const double ty = __dmul_rn(wy, sxv);
+      const double ty = cy == 1 ? sxv : __dmul_rn(W.v[ky], sxv);
       syv = ky == 0 ? ty : __dadd_rn(syv, ty);
     }
-    const double tz = __dmul_rn(wz, syv);
+    const double tz = cz == 1 ? syv : __dmul_rn(W.v[kz], syv);
     szv = kz == 0 ? tz : __dadd_rn(szv, tz);
   }
   return szv;
+}
+
+// the same for a run-time mask (the point lists are grouped by mask, so a warp takes one case)
+template <int P> __device__ __forceinline__ double prolong_value(const double* src, int odd, Geo g) {
+  switch (odd) {
+    case 1: return prolong_odd<P, 1>(src, g);
+    case 2: return prolong_odd<P, 2>(src, g);
+    case 3: return prolong_odd<P, 3>(src, g);
+    case 4: return prolong_odd<P, 4>(src, g);
+    case 5: return prolong_odd<P, 5>(src, g);
+    case 6: return prolong_odd<P, 6>(src, g);
+    case 7: return prolong_odd<P, 7>(src, g);
+    default: return prolong_odd<P, 0>(src, g);
+  }
 }
 
 // The regrid's transfer (the fill's operators between two forests): the value of every owned

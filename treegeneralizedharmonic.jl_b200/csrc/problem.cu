@@ -88,7 +88,6 @@ struct tgh_problem {
   double* part = nullptr;                 // error-norm partials + result
   double* diag = nullptr;                 // the monitors' diag field set (NDIAG slots per block)
   double* dpart = nullptr;                // constraint-norm partials (17 per CTA) + the fold
-  double* dwprol = nullptr;               // this order's prolongation weights (10), for the constant bank
   unsigned long long* ind = nullptr;      // the indicator's maxima (10 scales, tau_max) as bit patterns
   double* ind_tol = nullptr;              // the firing thresholds (at most 4)
   int* ind_counts = nullptr;              // per block and threshold: firing count
@@ -452,32 +451,8 @@ static int build_plan(tgh_problem* p) {
   return TGH_OK;
 }
 
-// Lagrange weights of P points at the midpoint of the middle pair (exact rationals,
-// rounded once): numerators over 2^(2P-3) computed in integers.
-static void prolong_weights(int P, double* w) {
-  // w_k = prod_{m != k} (0 - x_m)/(x_k - x_m), x_m = m - (P/2 - 1) - 1/2, in doubled units
-  for (int k = 0; k < P; ++k) {
-    long double num = 1, den = 1;
-    int64_t inum = 1, iden = 1;
-    for (int m = 0; m < P; ++m) {
-      if (m == k) continue;
-      const int64_t xm = 2 * (m - (P / 2 - 1)) - 1, xk = 2 * (k - (P / 2 - 1)) - 1;
-      inum *= -xm;
-      iden *= (xk - xm);
-    }
-    (void)num;
-    (void)den;
-    w[k] = (double)inum / (double)iden;
-  }
-}
-
-// Level l's prolongation into `work`. The weights of this problem's order go into the constant
-// bank first, from the problem's own device copy and on its stream (a copy a graph captures),
-// since problems of other orders in the process use the same bank.
+// Level l's prolongation into `work` (the weights of order P are compile-time constants).
 static cudaError_t launch_prolong(tgh_problem* p, int l, double* work) {
-  cudaError_t e = cudaMemcpyToSymbolAsync(c_wprol, p->dwprol, 10 * sizeof(double), 0, cudaMemcpyDeviceToDevice,
-                                          p->stream);
-  if (e != cudaSuccess) return e;
   const int T = 256;
   const long n = (long)p->nprol[l] * NV;
   switch (p->q + 2) {
@@ -797,10 +772,6 @@ static int setup_device(tgh_problem* p) {
   CK(cudaMalloc(&p->ind_tol, 4 * sizeof(double)));
   CK(cudaMalloc(&p->ind_counts, 4 * (size_t)p->nb * sizeof(int)));
   CK(cudaMalloc(&p->ind_boxes, 24 * (size_t)p->nb * sizeof(int)));
-  double wp[10] = {0};
-  prolong_weights(p->q + 2, wp);
-  CK(cudaMalloc(&p->dwprol, sizeof(wp)));
-  CK(cudaMemcpy(p->dwprol, wp, sizeof(wp), cudaMemcpyHostToDevice));
   if (cfg->gauge == TGH_GAUGE_SAMPLED) {
     CK(cudaMalloc(&p->Hsrc, (size_t)p->S * NV * p->nb * sizeof(double)));
     sample_gauge_kernel<<<grid_for(p->npts, 64), 64, 0, p->stream>>>(p->Hsrc, p->blk, p->geo, p->npts, p->cs, 0.0);
@@ -830,7 +801,7 @@ void tgh_problem_destroy(tgh_problem* p) {
   }
   void* bufs[] = {p->work, p->Hsrc, p->blk, p->primary, p->runs, p->gpts, p->hooks, p->hook_cache, p->scratch,
                   p->bcounts,
-                  p->part, p->coef, p->diag, p->dpart, p->ind, p->ind_tol, p->ind_counts, p->ind_boxes, p->dwprol,
+                  p->part, p->coef, p->diag, p->dpart, p->ind, p->ind_tol, p->ind_counts, p->ind_boxes,
                   p->k, p->acc, p->y, p->u0, p->W1, p->W2, p->bacc, p->twork, p->kt, p->acct, p->yt};
   for (void* b : bufs)
     if (b) cudaFree(b);
@@ -1051,7 +1022,6 @@ int tgh_transfer(tgh_problem* dst, tgh_problem* src, const double* u_src, double
                                                                                src->geo, u_dst, dst->S);
   CK(cudaGetLastError());
   if (!pp.empty()) {
-    CK(cudaMemcpyToSymbolAsync(c_wprol, src->dwprol, 10 * sizeof(double), 0, cudaMemcpyDeviceToDevice, src->stream));
     const int np = (int)pp.size();
     const long n = (long)np * NV;
     switch (P) {
