@@ -23,6 +23,8 @@ Workloads (seeded synthetic inputs, fully specified by their parameters):
                       refined around its path in 5 levels to 2472 blocks of 32^3 (finest h =
                       5/256), algebraic Kerr-Schild gauge source, moving :damped core; ~117 GB
                       on the device, so the plain-form and host-buffer legs are left out
+  hierarchy_small     the same hole on [-6,6]^3 refined in 2 levels (radii 3.0, 1.6) to 120
+                      blocks of 32^3: one coarse-fine interface, a few GB, for ncu captures
 """
 import argparse
 import ctypes
@@ -81,18 +83,20 @@ def workload(tgh, name):
         cfg = {"workload": "fourier_minkowski", "domain": "[-1,1]^3 periodic", "blocks": 8, "block": "32^3",
                "h": 1 / 32, "q": 4, "modes": 8, "amplitude": 1e-4, "eps_ko": 0.5, "gamma0": 1.0, "cfl": 0.25}
         return case, forest, case, forest, cfg, "none", True
-    if name == "hierarchy":
-        radii = [30.0, 16.0, 8.0, 4.5, 2.6]
-        case = tgh.kerr_schild_case(M=1.0, a=0.7, v=0.1, halfwidth=40.0, r0=0.8, r1=1.3, rho_max=4.0,
-                                    variant="damped", gauge="algebraic", eps_ko=0.5)
+    if name in ("hierarchy", "hierarchy_small"):
+        small = name == "hierarchy_small"
+        radii = [3.0, 1.6] if small else [30.0, 16.0, 8.0, 4.5, 2.6]
+        case = tgh.kerr_schild_case(M=1.0, a=0.7, v=0.1, halfwidth=6.0 if small else 40.0, r0=0.8, r1=1.3,
+                                    rho_max=4.0, variant="damped", gauge="algebraic", eps_ko=0.5)
         # the shells follow the centre over the 200-step run (t_end ~ 0.6, so 0.07 along x)
-        forest = tgh.hole_forest(case, 32, 4, radii, path=((0.0, 0.0, 0.0), (0.07, 0.0, 0.0)))
+        forest = tgh.hole_forest(case, 32, 2 if small else 4, radii, path=((0.0, 0.0, 0.0), (0.07, 0.0, 0.0)))
         sample = tgh.kerr_schild_case(M=1.0, a=0.7, v=0.1, halfwidth=4.0, r0=0.8, r1=1.3, rho_max=4.0,
                                       variant="damped", gauge="algebraic", eps_ko=0.5)
         sample_forest = tgh.gh_forest(sample, 32, 2)
         counts = [int(c) for c in __import__("numpy").bincount(forest.level)]
-        cfg = {"workload": "kerr_schild_hierarchy", "M": 1.0, "a": 0.7, "velocity": [0.1, 0.0, 0.0],
-               "domain": "[-40,40]^3", "blocks": forest.nblocks, "blocks_per_level": counts, "block": "32^3",
+        cfg = {"workload": "kerr_schild_hierarchy" + ("_small" if small else ""), "M": 1.0, "a": 0.7,
+               "velocity": [0.1, 0.0, 0.0], "domain": "[-6,6]^3" if small else "[-40,40]^3",
+               "blocks": forest.nblocks, "blocks_per_level": counts, "block": "32^3",
                "h_min": forest.h0 / 2 ** int(forest.level.max()), "refinement_radii": radii, "q": 4,
                "boundary": "dirichlet", "interior": "damped moving core r0=0.8 r1=1.3",
                "gauge_source": "algebraic", "eps_ko": 0.5, "cfl": 0.25}
@@ -411,7 +415,8 @@ def main():
     ap.add_argument("--steps", type=int, default=30)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="kerr_schild_static", choices=["kerr_schild_static", "fourier", "hierarchy"])
+    ap.add_argument("--workload", default="kerr_schild_static", choices=["kerr_schild_static", "fourier", "hierarchy",
+                                                                                "hierarchy_small"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"],
                     help="mixed: FP32 stencil sums and algebra on the FP64 state (one GPU)")
