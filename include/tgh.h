@@ -35,8 +35,11 @@
  *    (a CuArray, a torch tensor, ...), holding tgh_state_length() doubles.
  *  - The problem owns its ghosted working array, the sampled gauge source and all
  *    scratch; no verb allocates device memory after tgh_problem_create.
- *  - rhs reads the working array as the last prepare left it; max_speed, settle,
- *    initial_state and error_norm overwrite it (src/evolution.jl:1376-1384).
+ *  - rhs reads the working array as the last prepare left it (src/evolution.jl:1376-1384).
+ *    Here every other verb that writes the working array (error_norm, the monitors, tau,
+ *    transfer, the RK4 forms, the tangent-linear form, the sharded step) marks it
+ *    overwritten, and tgh_rhs then refuses with TGH_ERR_STALE until the next tgh_prepare;
+ *    settle is a prepare and keeps it current; max_speed and initial_state do not touch it.
  *  - Every entry point returns a status code and never aborts; tgh_last_error gives
  *    the message of the last failure on that problem.
  *  - A problem is bound to one CUDA stream (given at create) and is not thread-safe.
@@ -63,7 +66,8 @@ enum {
   TGH_ERR_RADII = 4,      /* interior radius checks, src/interior.jl:1104-1153 */
   TGH_ERR_TIMEOUT = 5,    /* a bounded device-side wait gave up */
   TGH_ERR_CUDA = 6,       /* a CUDA runtime call failed */
-  TGH_ERR_NOMEM = 7
+  TGH_ERR_NOMEM = 7,
+  TGH_ERR_STALE = 8       /* tgh_rhs after another verb overwrote what tgh_prepare filled */
 };
 
 /* backgrounds (SpacetimeMetrics metrics named by the reference's cases) */
@@ -147,6 +151,10 @@ int tgh_copy_work(tgh_problem* p, double* dst);
 
 /* --- the verbs (src/evolution.jl:1327-1390, src/stepping.jl:91-125) --- */
 int tgh_prepare(tgh_problem* p, const double* u, double t);
+/* the prepare/rhs contract as a generation counter: the number of tgh_prepare calls so far,
+ * and whether the working array still holds the last one's fill (1) or another verb has
+ * written it since (0, when tgh_rhs answers TGH_ERR_STALE) */
+int tgh_prepare_generation(const tgh_problem* p, long* generation, int* current);
 /* matter: nullable device pointer, 10 values per owned point in state layout
  * (rho, S_x, S_y, S_z, S_xx, S_xy, S_xz, S_yy, S_yz, S_zz); the GH-3 adapter
  * of src/evolution.jl:1288-1316 sampled at the owned points. */

@@ -89,3 +89,35 @@ def test_forests(tgh):
             touch = all(lo1[d] <= hi2[d] and lo2[d] <= hi1[d] for d in range(3))
             if touch:
                 assert abs(l1 - l2) <= 1
+
+
+def test_noalloc_speed_refuses_bad_meshes_before_touching_the_gpu(tgh):
+    """tgh_max_speed_noalloc makes tgh_problem_create's checks on the block table (null tables,
+    N < 1, levels out of range, corners off the block lattice) before any CUDA call, so its
+    refusals are TGH_ERR_ARG with a message even where no GPU is present."""
+    lib = tgh.load_library()
+    c = tgh.minkowski_case(L=1.0)
+    f = tgh.gh_forest(c, 8, 2)
+    cfg = c.config(4)
+    err = ctypes.create_string_buffer(256)
+    lam = ctypes.c_double()
+    dummy = ctypes.c_void_p(1)  # never dereferenced: every case is refused first
+
+    def call(mesh):
+        return lib.tgh_max_speed_noalloc(ctypes.byref(cfg), ctypes.byref(mesh), dummy, 0.0, None,
+                                         ctypes.byref(lam), err, 256)
+
+    m = f.mesh()
+    m.level = ctypes.POINTER(ctypes.c_int32)()
+    assert call(m) == tgh._abi.TGH_ERR_ARG and b"must not be null" in err.value
+    m = f.mesh()
+    m.N = 0
+    assert call(m) == tgh._abi.TGH_ERR_ARG and b"at least 1" in err.value
+    lev = (ctypes.c_int32 * f.nblocks)(*([25] * f.nblocks))
+    m = f.mesh()
+    m.level = ctypes.cast(lev, ctypes.POINTER(ctypes.c_int32))
+    assert call(m) == tgh._abi.TGH_ERR_ARG and b"out of range" in err.value
+    cor = (ctypes.c_int32 * (3 * f.nblocks))(*([3] * (3 * f.nblocks)))
+    m = f.mesh()
+    m.corner = ctypes.cast(cor, ctypes.POINTER(ctypes.c_int32))
+    assert call(m) == tgh._abi.TGH_ERR_ARG and b"multiple of N" in err.value

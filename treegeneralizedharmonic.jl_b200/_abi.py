@@ -10,7 +10,8 @@ from pathlib import Path
 _HERE = Path(__file__).resolve().parent
 LIB_PATH = _HERE / "lib" / "libtgh_b200.so"
 
-TGH_OK, TGH_ERR_ARG, TGH_ERR_NONFINITE, TGH_ERR_SPEED, TGH_ERR_RADII, TGH_ERR_TIMEOUT, TGH_ERR_CUDA, TGH_ERR_NOMEM = range(8)
+(TGH_OK, TGH_ERR_ARG, TGH_ERR_NONFINITE, TGH_ERR_SPEED, TGH_ERR_RADII, TGH_ERR_TIMEOUT, TGH_ERR_CUDA, TGH_ERR_NOMEM,
+ TGH_ERR_STALE) = range(9)
 BG_MINKOWSKI, BG_GAUGE_WAVE, BG_SHIFTED_MINKOWSKI, BG_KERR_SCHILD = range(4)
 GAUGE_NONE, GAUGE_SAMPLED, GAUGE_KERR_SCHILD = range(3)
 DAMP_CONSTANT, DAMP_GAUSSIAN = range(2)
@@ -68,6 +69,7 @@ SIGNATURES = {
     "tgh_work_length": (ctypes.c_size_t, [_VP]),
     "tgh_copy_work": (ctypes.c_int, [_VP, _VP]),
     "tgh_prepare": (ctypes.c_int, [_VP, _VP, _D]),
+    "tgh_prepare_generation": (ctypes.c_int, [_VP, ctypes.POINTER(ctypes.c_long), ctypes.POINTER(ctypes.c_int)]),
     "tgh_rhs": (ctypes.c_int, [_VP, _VP, _D, _VP]),
     "tgh_gh_rhs": (ctypes.c_int, [_VP, _VP, _VP, _D, _VP]),
     "tgh_settle": (ctypes.c_int, [_VP, _VP, _D]),

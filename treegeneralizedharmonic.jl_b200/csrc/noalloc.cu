@@ -15,12 +15,14 @@
 // no cudaMalloc, no cudaFree, no host heap.
 //
 // Limits and sharing: at most TGH_NOALLOC_MAX_BLOCKS blocks. Every GPU that loads the library
-// holds the array (about 0.63 MB) until the process exits. All calls on a device share it and
+// holds the array (256 + 16 x TGH_NOALLOC_MAX_BLOCKS bytes = 131,328 bytes, about 0.13 MB)
+// until the process exits. All calls on a device share it and
 // it keeps the last call's contents; calls that overlap on the GPU (two streams, or two host
 // threads) race on it. The first call on a device looks up the array's device address with
 // that device current; make that first call before any stream capture.
 #include <cuda_runtime.h>
 
+#include <cmath>
 #include <cstdio>
 #include <cstring>
 
@@ -110,11 +112,27 @@ extern "C" int tgh_max_speed_noalloc(const tgh_config* cfg, const tgh_mesh* mesh
   if (!cfg || !mesh || !u || !lambda) return set_error(errbuf, errlen, TGH_ERR_ARG, "a required argument is null");
   if (cfg->q < 2 || cfg->q > 8 || cfg->q % 2) return set_error(errbuf, errlen, TGH_ERR_ARG, "q must be even in 2..8");
   if (mesh->nblocks < 1) return set_error(errbuf, errlen, TGH_ERR_ARG, "the mesh has no blocks");
+  if (!mesh->level || !mesh->corner)
+    return set_error(errbuf, errlen, TGH_ERR_ARG, "the mesh's level and corner tables must not be null");
+  if (mesh->N < 1) return set_error(errbuf, errlen, TGH_ERR_ARG, "the block edge N must be at least 1");
   if (mesh->nblocks > kMaxBlocks) {
     std::snprintf(msg, sizeof(msg),
                   "the mesh has %d blocks; the allocation-free speed holds at most %d (use tgh_max_speed)",
                   mesh->nblocks, kMaxBlocks);
     return set_error(errbuf, errlen, TGH_ERR_ARG, msg);
+  }
+  // the checks tgh_problem_create makes on the block table (levels in range, corners on the
+  // block lattice), on the host copy the caller passed
+  for (int b = 0; b < mesh->nblocks; ++b) {
+    if (mesh->level[b] < 0 || mesh->level[b] > 20) {
+      std::snprintf(msg, sizeof(msg), "block %d: level %d out of range 0..20", b, (int)mesh->level[b]);
+      return set_error(errbuf, errlen, TGH_ERR_ARG, msg);
+    }
+    for (int d = 0; d < 3; ++d)
+      if (mesh->corner[3 * b + d] % mesh->N) {
+        std::snprintf(msg, sizeof(msg), "block %d: a corner is not a multiple of N", b);
+        return set_error(errbuf, errlen, TGH_ERR_ARG, msg);
+      }
   }
   int dev = 0;
   cudaError_t e = cudaGetDevice(&dev);
@@ -169,7 +187,7 @@ extern "C" int tgh_max_speed_noalloc(const tgh_config* cfg, const tgh_mesh* mesh
   double lam;
   std::memcpy(&lam, &h[0], sizeof(lam));
   *lambda = lam;
-  if (!(lam > 0.0 && lam < 1e300)) {
+  if (!(std::isfinite(lam) && lam > 0.0)) {
     std::snprintf(msg, sizeof(msg), "the maximum characteristic speed came out as %g", lam);
     return set_error(errbuf, errlen, TGH_ERR_SPEED, msg);
   }

@@ -106,6 +106,13 @@ struct tgh_problem {
   long last_launches = 0;  // kernels the last tgh_step_batched call (or sharded step) ran
   long launches = 0;       // kernels launched since tgh_shard_begin
   const double* gu = nullptr;
+  // the contract between prepare and rhs: rhs reads the working array as the last tgh_prepare
+  // left it. prep_gen counts the tgh_prepare calls; work_prepared says whether the working array
+  // still holds the last one's fill (every other verb that writes it clears the flag and names
+  // itself in work_writer), so that tgh_rhs refuses a stale array with TGH_ERR_STALE.
+  long prep_gen = 0;
+  bool work_prepared = false;
+  const char* work_writer = "nothing (no tgh_prepare yet)";
 };
 
 #define CK(call)                                                         \
@@ -120,6 +127,12 @@ struct tgh_problem {
 static int fail(tgh_problem* p, int code, const std::string& msg) {
   p->err = msg;
   return code;
+}
+
+// a verb other than tgh_prepare wrote the working array: the next tgh_rhs needs a new prepare
+static void work_overwritten(tgh_problem* p, const char* who) {
+  p->work_prepared = false;
+  p->work_writer = who;
 }
 
 // ---- the forest: owners, positions ----
@@ -820,14 +833,37 @@ int tgh_copy_work(tgh_problem* p, double* dst) {
   return TGH_OK;
 }
 
-int tgh_prepare(tgh_problem* p, const double* u, double t) { return launch_fill(p, u, false, p->work, t); }
+// the fill of u into the working array, shared by tgh_prepare and the verbs that prepare for
+// their own use (which then mark the array overwritten)
+static int prepare_impl(tgh_problem* p, const double* u, double t, const char* who) {
+  const int s = launch_fill(p, u, false, p->work, t);
+  if (who) work_overwritten(p, who);
+  return s;
+}
+
+int tgh_prepare(tgh_problem* p, const double* u, double t) {
+  const int s = prepare_impl(p, u, t, nullptr);
+  if (s) {
+    work_overwritten(p, "a tgh_prepare that failed");
+    return s;
+  }
+  ++p->prep_gen;
+  p->work_prepared = true;
+  return TGH_OK;
+}
+
+int tgh_prepare_generation(const tgh_problem* p, long* generation, int* current) {
+  *generation = p->prep_gen;
+  *current = p->work_prepared ? 1 : 0;
+  return TGH_OK;
+}
 
 // ---- the constraint monitors (src/constraints.jl:535-609) ----
 static int monitor_prepare(tgh_problem* p, const double* u, double t, int mask, MonArgs& a) {
   if (p->nranks > 1) return fail(p, TGH_ERR_ARG, "the constraint monitors run on a problem of one rank");
   if (mask != TGH_MASK_INTERIOR && mask != TGH_MASK_ALL)
     return fail(p, TGH_ERR_ARG, "mask must be TGH_MASK_INTERIOR or TGH_MASK_ALL");
-  int s = tgh_prepare(p, u, t);
+  int s = prepare_impl(p, u, t, "a constraint monitor or the refinement indicator");
   if (s) return s;
   std::memset(&a, 0, sizeof(a));
   a.work = p->work;
@@ -958,7 +994,7 @@ int tgh_transfer(tgh_problem* dst, tgh_problem* src, const double* u_src, double
   for (int d = 0; d < 3; ++d)
     same = same && dst->lo[d] == src->lo[d] && dst->cells0[d] == src->cells0[d] && dst->periodic[d] == src->periodic[d];
   if (!same) return fail(dst, TGH_ERR_ARG, "the two problems differ in order, block size or root grid");
-  int s = tgh_prepare(src, u_src, t);
+  int s = prepare_impl(src, u_src, t, "tgh_transfer (as its source)");
   if (s) return s;
   const int G = src->G, Wd = src->Wd, P = src->q + 2;
   std::vector<CopyPt> cp;
@@ -1042,6 +1078,9 @@ int tgh_copy_diag(tgh_problem* p, double* out) {
 }
 
 int tgh_rhs(tgh_problem* p, double* du, double t, const double* matter) {
+  if (!p->work_prepared)
+    return fail(p, TGH_ERR_STALE, std::string("the working array no longer holds the last tgh_prepare's fill: ") +
+                                      p->work_writer + " wrote it since; call tgh_prepare again");
   RhsArgs a = base_args(p, p->work, t);
   a.du = du;
   a.matter = matter;
@@ -1131,7 +1170,7 @@ int tgh_max_speed(tgh_problem* p, const double* u, double t, double* lambda) {
 }
 
 int tgh_error_norm(tgh_problem* p, const double* u, double t, double* l2, double* linf) {
-  int s = tgh_prepare(p, u, t);
+  int s = prepare_impl(p, u, t, "tgh_error_norm");
   if (s) return s;
   error_kernel<<<p->npart, 128, 0, p->stream>>>(p->work, p->blk, p->primary, p->geo, p->npts, p->cs, t, p->part);
   CK(cudaGetLastError());
@@ -1172,6 +1211,7 @@ int tgh_rk4_step(tgh_problem* p, double* u, double t, double dt) {
   if ((s = tgh_gh_rhs(p, p->k, p->y, te, nullptr))) return s;
   stage_update_kernel<<<g, 256, 0, p->stream>>>(2, (long)L, p->k, nullptr, p->acc, nullptr, u, 0.0, b16);
   CK(cudaGetLastError());
+  work_overwritten(p, "tgh_rk4_step (its last stage's fill)");
   return stage_limit_impl(p, u, te);
 }
 
@@ -1249,6 +1289,7 @@ int tgh_step_batched(tgh_problem* p, double* u, double t, double dt, int nsteps)
   int s = batched_buffers(p);
   if (s) return s;
   // the state into W0's owned points (and ghosts), outside the graph
+  work_overwritten(p, "tgh_step_batched");
   if ((s = launch_fill(p, u, false, p->work, t))) return s;
   // a stationary hook into the two stage buffers once, also outside the graph; the graph's
   // stage fills of those buffers then skip it
@@ -1402,6 +1443,7 @@ int tgh_shard_begin(tgh_problem* p, const double* u) {
   if (p->has_bounds) return fail(p, TGH_ERR_ARG, "the batched form has no range projection; use tgh_rk4_step");
   int s = batched_buffers(p);
   if (s) return s;
+  work_overwritten(p, "the sharded step");
   scatter_owned_kernel<<<grid_for(p->npts, 256), 256, 0, p->stream>>>(u, p->work, p->geo, p->npts);
   CK(cudaGetLastError());
   p->launches = 1;
@@ -1478,7 +1520,7 @@ int tgh_time_rhs(tgh_problem* p, const double* u, double t, int mode, int nlaunc
   }
   // a rank of a sharded problem cannot fill from u alone: it is timed on its working array as
   // its last step left it (filled)
-  int s = p->nranks > 1 ? TGH_OK : tgh_prepare(p, u, t);
+  int s = p->nranks > 1 ? TGH_OK : prepare_impl(p, u, t, "tgh_time_rhs");
   if (s) return s;
   RhsArgs a = base_args(p, p->work, t);
   a.du = p->k;
@@ -1578,7 +1620,7 @@ static int launch_fill_tangent(tgh_problem* p, const double* ut) {
 int tgh_tangent_rhs(tgh_problem* p, double* du, double* dut, const double* u, const double* ut, double t, int dir) {
   int s = tangent_check(p, dir);
   if (s) return s;
-  if ((s = launch_fill(p, u, false, p->work, t))) return s;
+  if ((s = prepare_impl(p, u, t, "the tangent-linear form"))) return s;
   if ((s = launch_fill_tangent(p, ut))) return s;
   RhsArgs a = base_args(p, p->work, t);
   a.du = du;
@@ -1615,7 +1657,7 @@ int tgh_tangent_rk4_step(tgh_problem* p, double* u, double* ut, double t, double
 int tgh_tangent_error_norm(tgh_problem* p, const double* u, const double* ut, double t, double* l2, double* dl2) {
   int s = tangent_check(p, TAN_STATE);
   if (s) return s;
-  if ((s = launch_fill(p, u, false, p->work, t))) return s;
+  if ((s = prepare_impl(p, u, t, "the tangent-linear form"))) return s;
   if ((s = launch_fill_tangent(p, ut))) return s;
   error_tangent_kernel<<<p->npart, 128, 0, p->stream>>>(p->work, p->twork, p->blk, p->primary, p->geo, p->npts, p->cs,
                                                          t, p->part);

@@ -76,8 +76,15 @@ class GHProblem:
         return self
 
     def rhs(self, du, t, matter=None):
-        """rhs!(du, p, t; matter): the right-hand side of the state prepare left."""
+        """rhs!(du, p, t; matter): the right-hand side of the state prepare left. Raises
+        TGHError(TGH_ERR_STALE) when another verb has written the working array since."""
         self._check(self.lib.tgh_rhs(self._h, _ptr(du), float(t), _ptr(matter)))
+
+    def prepare_generation(self):
+        """(number of prepare calls, whether the working array still holds the last one)."""
+        g, c = ctypes.c_long(), ctypes.c_int()
+        self._check(self.lib.tgh_prepare_generation(self._h, ctypes.byref(g), ctypes.byref(c)))
+        return g.value, bool(c.value)
 
     def gh_rhs(self, du, u, t, matter=None):
         """gh_rhs!(du, u, p, t; matter) = prepare! then rhs!."""

@@ -166,27 +166,38 @@ class ShardedGHProblem:
         self._check(self.lib.tgh_shard_end(self._h, _ptr(u)))
 
     def exchange(self, phase):
-        """The phase's all-to-all over the process group (NCCL between GPUs): peer-major
-        buffers of 20 doubles per point, counts from the plan."""
+        """The phase's all-to-all over the process group: peer-major buffers of 20 doubles per
+        point, counts from the plan. NCCL moves device buffers between GPUs; a gloo group (ranks
+        that share a GPU, or tests) moves host copies of them, the waits all on the host."""
         import torch.distributed as dist
         if self.nranks == 1:
             return
-        dist.all_to_all_single(self.recv_buf[phase][:int(self.recv_count[phase].sum()) * NV],
-                               self.send_buf[phase][:int(self.send_count[phase].sum()) * NV],
-                               output_split_sizes=[int(c) * NV for c in self.recv_count[phase]],
-                               input_split_sizes=[int(c) * NV for c in self.send_count[phase]], group=self.group)
+        ns, nr = int(self.send_count[phase].sum()) * NV, int(self.recv_count[phase].sum()) * NV
+        send, recv = self.send_buf[phase][:ns], self.recv_buf[phase][:nr]
+        osz = [int(c) * NV for c in self.recv_count[phase]]
+        isz = [int(c) * NV for c in self.send_count[phase]]
+        if dist.get_backend(self.group) == "gloo":
+            hs = send.cpu()  # ordered after pack on the current (the problem's) stream
+            hr = torch.empty(nr, dtype=torch.float64)
+            dist.all_to_all_single(hr, hs, output_split_sizes=osz, input_split_sizes=isz, group=self.group)
+            recv.copy_(hr)
+        else:
+            dist.all_to_all_single(recv, send, output_split_sizes=osz, input_split_sizes=isz, group=self.group)
 
     def step(self, u, t, dt, nsteps=1):
         """nsteps RK4 steps of the batched form on this rank's leaves, exchanging with the other
-        ranks before every fill phase; u holds this rank's leaves and is updated in place."""
-        self.begin(u)
-        for n in range(int(nsteps)):
-            tn = float(t) + n * float(dt)
-            for st in range(4):
-                for ph in range(self.phases):
-                    self.pack(st, ph)
-                    self.exchange(ph)
-                    self.unpack(st, ph)
-                    self.fill(st, ph, tn, dt)
-                self.rhs(st, tn, dt)
-        self.end(u)
+        ranks before every fill phase; u holds this rank's leaves and is updated in place. The
+        exchange is ordered on the problem's stream (the current stream while the step runs),
+        whatever stream the caller has current."""
+        with torch.cuda.stream(self.stream):
+            self.begin(u)
+            for n in range(int(nsteps)):
+                tn = float(t) + n * float(dt)
+                for st in range(4):
+                    for ph in range(self.phases):
+                        self.pack(st, ph)
+                        self.exchange(ph)
+                        self.unpack(st, ph)
+                        self.fill(st, ph, tn, dt)
+                    self.rhs(st, tn, dt)
+            self.end(u)
