@@ -5,7 +5,7 @@ One "step" is one classical RK4 step (four right-hand sides with Kreiss-Oliger d
 the ghost fill before each, the stage arithmetic) over the whole mesh of the workload. A
 point is an owned point counted N^3 per block, as the reference counts it.
 
-    python bench.py [--gpus N] [--steps K] [--warmup W] [--workload kerr_schild_static|fourier|hierarchy]
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--workload hierarchy|kerr_schild_static|fourier]
     python bench.py --impl reference ...   # the CPU restatement of the reference's path
 
 One GPU: the batched form (the whole K-step run one CUDA graph). N GPUs (torchrun, one rank
@@ -14,15 +14,16 @@ all-to-all of halo points before each fill phase; the mesh is the same for every
 scaling). --shard runs that sharded path on one GPU.
 
 Workloads (seeded synthetic inputs, fully specified by their parameters):
+  hierarchy           (the default) the hole of kerr_schild_static boosted to v = 0.1 along x,
+                      on [-40,40]^3 refined around its path in 5 levels to 2472 blocks of 32^3
+                      (finest h = 5/256), algebraic Kerr-Schild gauge source, moving :damped
+                      core; ~117 GB on the device in the batched form. The plain forms are
+                      timed after the batched problem is released, on a problem of their own
   kerr_schild_static  static Kerr-Schild hole M=1, a=7/10 on [-8,8]^3, 64 blocks of 32^3
                       (h = 1/8), Dirichlet faces, :damped interior r_0=0.8 r_1=1.3 rho_max=4/M,
                       sampled gauge source, Gaussian damping, eps_KO = 1/2, q = 4, dt = h/(4 lambda)
   fourier             Minkowski + 8 Fourier modes (amplitude 1e-4) per component on the periodic
                       [-1,1]^3, 8 blocks of 32^3, q = 4, eps_KO = 1/2, gamma0 = 1, dt = h/4
-  hierarchy           the hole of kerr_schild_static boosted to v = 0.1 along x, on [-40,40]^3
-                      refined around its path in 5 levels to 2472 blocks of 32^3 (finest h =
-                      5/256), algebraic Kerr-Schild gauge source, moving :damped core; ~117 GB
-                      on the device, so the plain-form and host-buffer legs are left out
   hierarchy_small     the same hole on [-6,6]^3 refined in 2 levels (radii 3.0, 1.6) to 120
                       blocks of 32^3: one coarse-fine interface, a few GB, for ncu captures
 """
@@ -358,19 +359,20 @@ def time_monitors(P, u, stream, gauge, n1pts, peak, reps=5):
     return out
 
 
-def end_to_end(P, u0, dt, K, world, pts, stream, dist):
+def end_to_end(P, uh, dt, K, world, pts, stream, dist, NB=3):
     """The metric through the public API with host buffers: per step the state is copied in
-    from pinned host memory, stepped, and copied back, all inside the timed region. The steps
-    are independent requests, pipelined over three device buffers: step n+1's upload (one copy
-    stream) and step n-1's download (another) run while step n computes, and no upload waits
-    for the download of the buffer it refills (that one was step n-2's, long finished)."""
+    from pinned host memory (uh), stepped, and copied back, all inside the timed region. The
+    steps are independent requests, pipelined over NB device buffers: step n+1's upload (one
+    copy stream) and step n-1's download (another) run while step n computes; with NB = 3 no
+    upload waits for the download of the buffer it refills (step n-2's, long finished), with
+    NB = 2 (the hierarchy, whose state is 14 GB) the upload of step n+1 waits for step n-1's
+    download."""
     import torch
-    NB = 3
-    uh = u0.cpu().pin_memory()
-    res_h = [torch.empty_like(uh).pin_memory() for _ in range(NB)]
-    P.step_batched(u0.clone(), 0.0, dt, 1)  # graph for one step
+    res_h = [torch.empty(uh.numel(), dtype=uh.dtype, pin_memory=True) for _ in range(NB)]
+    ud = [torch.empty(uh.numel(), dtype=uh.dtype, device="cuda") for _ in range(NB)]
+    ud[0].copy_(uh)
+    P.step_batched(ud[0], 0.0, dt, 1)  # graph for one step
     torch.cuda.synchronize()
-    ud = [torch.empty_like(u0) for _ in range(NB)]
     s_in, s_out = torch.cuda.Stream(), torch.cuda.Stream()
     ev_in = [torch.cuda.Event() for _ in range(NB)]
     ev_done = [torch.cuda.Event() for _ in range(NB)]
@@ -404,9 +406,38 @@ def end_to_end(P, u0, dt, K, world, pts, stream, dist):
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         e2e_ms = float(t.item())
     nbytes = uh.numel() * 8
-    return {"value": world * pts * K / (e2e_ms * 1e-3), "unit": "point-updates/s",
-            "h2d_bytes_per_step": nbytes, "d2h_bytes_per_step": nbytes,
-            "pipelining": "step n+1's upload and step n-1's download overlap step n (three buffers, two copy streams)"}
+    ok = all(bool(torch.isfinite(r).all()) for r in res_h[:min(NB, K)])
+    return {"value": world * pts * K / (e2e_ms * 1e-3), "unit": "point-updates/s", "ms_per_step": e2e_ms / K,
+            "h2d_bytes_per_step": nbytes, "d2h_bytes_per_step": nbytes, "results_finite": ok,
+            "pipelining": f"step n+1's upload and step n-1's download overlap step n ({NB} device buffers, "
+                          "two copy streams, one cudaMemcpyAsync each way per step)"}
+
+
+def plain_forms(P, u0, dt, K, pts, stream):
+    """The plain per-stage form (per stage: fill of u, RHS into du over all blocks, stage update;
+    host-issued) and the plain per-block form (the same, with one RHS launch and one stage update
+    per block), each timed with CUDA events over a few steps from the workload's state."""
+    import torch
+    out = {}
+    for name, fn, steps in (("per_stage", P.rk4_step, max(3, K // 3)), ("per_block", P.rk4_step_blocks, 3)):
+        up = u0.clone()
+        fn(up, 0.0, dt)
+        torch.cuda.synchronize()
+        e4, e5 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e4.record(stream)
+        for n in range(steps):
+            fn(up, n * dt, dt)
+        e5.record(stream)
+        torch.cuda.synchronize()
+        ms = e4.elapsed_time(e5) / steps
+        out[name] = {"value": pts / (ms * 1e-3), "unit": "point-updates/s", "ms_per_step": ms, "steps": steps}
+        if name == "per_block":
+            out[name]["gpu_launches_per_step"] = P.last_launch_count()
+        del up
+    out["per_stage"]["form"] = "per stage: fill of u, one RHS launch pair over all blocks into du, stage update"
+    out["per_block"]["form"] = ("per stage: fill of u, then per block one RHS launch pair and one stage update "
+                                "(the reference's block map), host-issued")
+    return out
 
 
 def main():
@@ -415,8 +446,8 @@ def main():
     ap.add_argument("--steps", type=int, default=30)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="kerr_schild_static", choices=["kerr_schild_static", "fourier", "hierarchy",
-                                                                                "hierarchy_small"])
+    ap.add_argument("--workload", default="hierarchy", choices=["hierarchy", "kerr_schild_static", "fourier",
+                                                                       "hierarchy_small"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"],
                     help="mixed: FP32 stencil sums and algebra on the FP64 state (one GPU)")
@@ -500,29 +531,6 @@ def main():
     pts = forest.points()
     value = world * pts * K / (ms * 1e-3)
 
-    # the plain per-stage form on the same workload (fill of u, RHS into du, stage update; each
-    # launch issued from the host), for the batched form's speed-up
-    plain = {"skipped": "its three state-sized buffers do not fit beside the batched form's"}
-    if not big:
-        up = u0.clone()
-        P.rk4_step(up, 0.0, dt)
-        torch.cuda.synchronize()
-        Kp = max(3, K // 3)
-        e4, e5 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        e4.record(stream)
-        for n in range(Kp):
-            P.rk4_step(up, n * dt, dt)
-        e5.record(stream)
-        torch.cuda.synchronize()
-        plain_ms = e4.elapsed_time(e5) / Kp
-        if world > 1:
-            t = torch.tensor([plain_ms], device="cuda")
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            plain_ms = float(t.item())
-        del up
-        plain = {"value": world * pts / (plain_ms * 1e-3), "unit": "point-updates/s", "ms_per_step": plain_ms,
-                 "steps": Kp, "form": "per stage: fill of u, RHS into du, stage update (host-issued launches)"}
-
     # the dominant kernel alone: the right-hand side with the fused RK4 epilogue
     rhs_ms = P.time_rhs(u0, 0.0, mode=1, nlaunch=max(4, K))
     n1pts = (forest.N + 1) ** 3 * forest.nblocks
@@ -542,10 +550,21 @@ def main():
 
     # end to end through the public API with host buffers: per step the state is copied in
     # from pinned host memory and the result copied back
+    uh = torch.empty(u0.numel(), dtype=u0.dtype, pin_memory=True)
+    uh.copy_(u0)
+    del u
     if big:
-        e2e = {"skipped": "two pinned host copies of the 14 GB state", "unit": "point-updates/s"}
-    else:
-        e2e = end_to_end(P, u0, dt, K, world, pts, stream, dist)
+        del u0  # the hierarchy's state is 14 GB: two device buffers beside the batched problem's
+        torch.cuda.empty_cache()
+    e2e = end_to_end(P, uh, dt, K, world, pts, stream, dist, NB=2 if big else 3)
+    if big:
+        # the plain forms' own buffers (k, acc, y) do not fit beside the batched form's: a problem
+        # of their own once the batched one is released
+        P.close()
+        torch.cuda.empty_cache()
+        P = tgh.GHProblem(case, forest, 4, margin_check=False, precision=args.precision)
+        u0 = uh.cuda()
+    plain = plain_forms(P, u0, dt, K, pts, stream)
 
     out = {"metric": "RK4 point-updates/s", "value": value, "unit": "point-updates/s", "n_gpus": world,
            "steps": K, "warmup": W, "ms_per_step": ms / K, "higher_is_better": True, "scaling": "weak",
@@ -562,7 +581,10 @@ def main():
                         "ms_per_launch": rhs_ms,
                         "peak_source": "measured FP64 FMA probe on this GPU (MEASURED_PEAKS.json has no FP64)"},
            "e2e": e2e,
-           "plain_form": plain,
+           "plain_form": plain["per_stage"],
+           "plain_per_block": plain["per_block"],
+           "speedup_vs_plain_per_block": plain["per_block"]["ms_per_step"] / (ms / K),
+           "speedup_vs_plain_per_stage": plain["per_stage"]["ms_per_step"] / (ms / K),
            "monitors": monitors,
            "gpu_launches": launches, "clocks": ck}
     if rank == 0 and world == 1 and not args.no_cpu_baseline:

@@ -148,6 +148,9 @@ size_t tgh_state_length(const tgh_problem* p);
 size_t tgh_work_length(const tgh_problem* p);
 /* copy the working array (device to device) for inspection */
 int tgh_copy_work(tgh_problem* p, double* dst);
+/* the same for the blocks b0 .. b0 + nblocks - 1 of the working array (each (N+2G+1)^3 * 20
+ * doubles, blocks in forest order on a problem of one rank) */
+int tgh_copy_work_blocks(tgh_problem* p, int b0, int nblocks, double* dst);
 
 /* --- the verbs (src/evolution.jl:1327-1390, src/stepping.jl:91-125) --- */
 int tgh_prepare(tgh_problem* p, const double* u, double t);
@@ -169,11 +172,35 @@ int tgh_initial_state(tgh_problem* p, double* u, double t);
 /* --- one classical RK4 step (IMEXRungeKutta RK4 via gh_integrator, src/stepping.jl:208-225) ---
  * plain form: per stage one ghost fill, one right-hand-side launch, one stage update */
 int tgh_rk4_step(tgh_problem* p, double* u, double t, double dt);
+/* plain per-block form: the same step with the reference's block-wise map (map_blocks!,
+ * src/evolution.jl:1387): per stage one fill, then one right-hand-side launch and one stage
+ * update per block, issued from the host. Bit for bit tgh_rk4_step's result. */
+int tgh_rk4_step_blocks(tgh_problem* p, double* u, double t, double dt);
 /* batched form: the state stays ghosted on the device; each stage is one fill launch and
  * one right-hand-side launch with the RK4 epilogue fused in; nsteps steps are captured
  * once as a CUDA graph and replayed. u is read before the first step and written after
  * the last. */
 int tgh_step_batched(tgh_problem* p, double* u, double t, double dt, int nsteps);
+
+/* --- the right-hand side's kernel variants (no counterpart in the reference, whose kernels
+ * are compiled per problem by KernelAbstractions) ---
+ * tgh_set_variant picks the kernels the right-hand side launches; the autotuner (autotune.py)
+ * times them on the problem's own mesh and records the fastest per configuration:
+ *   pi_variant  TGH_PI_L1:  the Pi half as one point per thread, its stencils read through L1;
+ *               TGH_PI_TMA: two points per thread from tiles of the working array staged into
+ *               shared memory by the Tensor Memory Accelerator (q = 4, N = 32, FP64 only);
+ *   threads     CTA size of the head and one-point Pi kernels, 64 or 128;
+ *   pi_mb       the one-point Pi kernel's resident CTAs per SM (its launch bound), 3, 4 or 5.
+ * All variants give the same bits. A change drops the batched form's captured graph.
+ * tgh_set_wait_limit bounds the polls of every device-side wait (the TMA kernel's waits for its
+ * copies); a wait that runs out records TGH_ERR_TIMEOUT and its CTA writes nothing. A negative
+ * limit gives up at once (for tests). tgh_device_status synchronizes the problem's stream and
+ * returns (and clears) TGH_ERR_TIMEOUT if a wait gave up since the last call. */
+enum { TGH_PI_L1 = 0, TGH_PI_TMA = 1 };
+int tgh_set_variant(tgh_problem* p, int pi_variant, int threads, int pi_mb);
+int tgh_get_variant(const tgh_problem* p, int* pi_variant, int* threads, int* pi_mb);
+int tgh_set_wait_limit(tgh_problem* p, long long polls);
+int tgh_device_status(tgh_problem* p);
 
 /* --- analysis (src/constraints.jl:311-396, 716-792) ---
  * masked, volume-weighted L2 and max of |u - u_exact| over the evolved primaries */

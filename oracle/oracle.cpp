@@ -1009,6 +1009,13 @@ int orc_copy_work(void* p, double* dst) {
   std::memcpy(dst, P->work.data(), P->work.size() * sizeof(double));
   return TGH_OK;
 }
+// the working array set from outside (a filled array of the product's layout): the right-hand
+// side of blocks cut out of a larger mesh, whose ghosts another fill has already written
+int orc_set_work(void* p, const double* src) {
+  Problem* P = (Problem*)p;
+  P->work.assign(src, src + P->npt_work() * NV * P->nb);
+  return TGH_OK;
+}
 int orc_copy_hsrc(void* p, double* dst) {
   Problem* P = (Problem*)p;
   std::memcpy(dst, P->Hsrc.data(), P->Hsrc.size() * sizeof(double));

@@ -36,3 +36,12 @@ def tgh():
 def oracle():
     import oracle_binding
     return oracle_binding.Oracle.load()
+
+
+@pytest.fixture(scope="session")
+def bench_module():
+    """bench.py as a module: the workloads' definitions (cases, forests) the tests share."""
+    spec = importlib.util.spec_from_file_location("bench_workloads", ROOT / "bench.py")
+    mod = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mod)
+    return mod

@@ -40,6 +40,7 @@ class Oracle:
             "orc_gh_rhs": (ctypes.c_int, [_VP, _DP, _DP, _D, _DP]),
             "orc_copy_work": (ctypes.c_int, [_VP, _DP]),
             "orc_copy_hsrc": (ctypes.c_int, [_VP, _DP]),
+            "orc_set_work": (ctypes.c_int, [_VP, _DP]),
             "orc_initial_state": (ctypes.c_int, [_VP, _DP, _D]),
             "orc_stage_limit": (ctypes.c_int, [_VP, _DP, _D]),
             "orc_max_speed": (ctypes.c_int, [_VP, _DP, _D, _DP]),
@@ -227,6 +228,11 @@ class OracleProblem:
         w = np.zeros(self.LW)
         self.lib.orc_copy_work(self.h, _dp(w))
         return w
+
+    def set_work(self, w):
+        w = np.ascontiguousarray(w, dtype=float)
+        assert w.size == self.LW
+        self.lib.orc_set_work(self.h, _dp(w))
 
     def hsrc(self):
         w = np.zeros(self.L)

@@ -51,5 +51,6 @@ def test_rhs_refuses_a_working_array_another_verb_wrote(tgh):
     P.gh_constraint(u, 0.0)
     P.gh_rhs(du, u, 0.0)
     assert torch.equal(du, ref)
-    assert P.prepare_generation() == (6, True)
+    # six fills by tgh_prepare and settle and gh_rhs, four more by the RK4 step's stages
+    assert P.prepare_generation() == (10, True)
     P.close()

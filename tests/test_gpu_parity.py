@@ -1,9 +1,10 @@
 """The CUDA path against the CPU oracle on identical inputs (the parity gate).
 
 Tolerances (the reference's own, test/evolution_tests.jl:141-179): the right-hand side
-within 1e-12 of rhs_scale per point; copies of the ghost fill bit for bit, prolongation
-bit for bit, Dirichlet ghosts within 1e-13 relative (two evaluations of the analytic
-metric); one RK4 step within 1e-12 absolute on states of order one.
+within 1e-12 of rhs_scale per point, on every row, the moving hole's included; the ghost
+fill bit for bit: copies, prolongation and the Dirichlet ghosts (the analytic state is
+evaluated on the device in the oracle's order with every operation rounded on its own); one
+RK4 step within 1e-12 absolute on states of order one.
 """
 import math
 
@@ -16,7 +17,6 @@ from helpers import N_ROWS, cases, rhs_error, rhs_scale, two_level_forest
 pytestmark = pytest.mark.gpu
 
 RHS_TOL = 1e-12
-MOVING = ("kerr_schild_moving", "kerr_schild_hierarchy_moving")
 
 
 def _to_gpu(a):
@@ -51,11 +51,11 @@ def test_rhs_matches_oracle(tgh, oracle, row):
     assert np.all(np.isfinite(du))
     err = rhs_error(du, du_ref, rhs_scale(O.work(), forest, q), forest)
     # A moving hole's layer and core read the target's rate as the centered difference
-    # (Pi(t + d) - Pi(t - d)) / 2d with d = eps^(1/3) r_0 (src/initialdata.jl:1721-1729): two
-    # evaluations of the analytic Pi that agree to an ulp differ by ~eps |Pi| / d ~ 1e-11 |Pi|
-    # there, the reference's own roundoff estimate for that rate. Elsewhere the bound is 1e-12.
-    tol = 1e-9 if name in MOVING else RHS_TOL
-    assert err < tol, f"{name}: {err}"
+    # (Pi(t + d) - Pi(t - d)) / 2d with d = eps^(1/3) r_0 (src/initialdata.jl:1721-1729): an ulp
+    # of difference between two evaluations of the analytic Pi would move it by ~1e-11 |Pi|.
+    # The device evaluates that state bit for bit as the oracle does, so the bound holds there
+    # as everywhere else.
+    assert err < RHS_TOL, f"{name}: {err}"
 
 
 def test_matter_source_matches_oracle(tgh, oracle):
@@ -95,10 +95,7 @@ def test_fill_matches_oracle(tgh, oracle, which):
     P.prepare(_to_gpu(u), 0.2)
     wg = P.copy_work().cpu().numpy()
     wo = O.work()
-    if which == "dirichlet":
-        assert np.max(np.abs(wg - wo) / np.maximum(1.0, np.abs(wo))) < 1e-13
-    else:
-        assert np.array_equal(wg, wo)
+    assert np.array_equal(wg, wo)
 
 
 @pytest.mark.parametrize("row", [0, 2, 6, 7, 9, 11, 14, 17, 18, 19])
@@ -112,10 +109,7 @@ def test_rk4_step_matches_oracle(tgh, oracle, row):
     P.rk4_step(ug, t, dt)
     uo = u.copy()
     O.rk4_step(uo, t, dt)
-    # the moving core's target lies on the sphere r_0 = 0.8 just outside the a = 0.7 ring
-    # singularity, where the analytic state's roundoff (two correct evaluations differ by
-    # ~1e-13 relative) is amplified 1e5-fold by the target rate's centered time difference
-    tol = 1e-7 if name in MOVING else 1e-12
+    tol = 1e-12
     assert np.max(np.abs(ug.cpu().numpy() - uo)) < tol
     if not name.endswith("pasted"):
         ub = _to_gpu(u)
@@ -185,3 +179,53 @@ def test_hole_interior_is_masked_for_speed(tgh):
     # block 0 is [-2,0]^3; its corner point (N, N, N) is the origin
     u[0 * 20 * N1 ** 3 + f.N + N1 * (f.N + N1 * f.N)] = float("nan")
     assert math.isfinite(P.max_speed(u, 0.0))
+
+
+def test_analytic_state_is_the_oracles_bit_for_bit(tgh, oracle):
+    """The device's analytic state (Dirichlet ghosts, layer and core targets) at points around a
+    resting and a moving (boosted) spinning hole and near its ring singularity: every h, Pi bit
+    for bit the oracle's. The moving hole's target rates are centred differences of this state
+    over 1.2e-5 r_0 in t, which would turn one ulp into ~1e-11. Kerr-Schild takes only
+    +, -, *, / and square roots, correctly rounded on both sides; shifted Minkowski's tanh (and
+    the gauge wave's sin) come from CUDA's and the C library's own functions, which may differ
+    in the last bit, and psi = A (1 - tanh^2) carries that on: there, within 1e-15 of max(1, |u|)."""
+    rng = np.random.default_rng(7)
+    for case in (tgh.kerr_schild_case(M=1.0, a=0.7, halfwidth=2.0, r0=0.8, r1=1.3, gauge="algebraic"),
+                 tgh.kerr_schild_case(M=1.0, a=0.7, v=0.1, halfwidth=2.0, r0=0.8, r1=1.3, gauge="algebraic"),
+                 tgh.shifted_minkowski_case(eps_ko=0.5, gamma0=1.0, gamma2=-0.5)):
+        f = tgh.gh_forest(case, 8, 2)
+        P = tgh.GHProblem(case, f, 4, margin_check=False)
+        bg = oracle.background(case)
+        pts = np.concatenate([rng.uniform(-2.0, 2.0, (40, 3)), rng.uniform(-0.9, 0.9, (20, 3))])
+        for k, x in enumerate(pts):
+            t = 0.3 + 1e-5 * k
+            got = np.array(P.point_physics(t, x)[:20])
+            it = case.interior
+            if it and np.linalg.norm(x - (np.array(it["c0"]) + t * np.array(it["v"]))) < it["r0"]:
+                continue  # the core rule moves the point; the background is compared off the core
+            h, Pi, _, _ = oracle.background_state(bg, t, x)
+            ref = np.concatenate([h, Pi])
+            if case.background["kind"] == "kerr_schild":
+                assert np.array_equal(got, ref), (k, x, got - ref)
+            else:
+                assert np.all(np.abs(got - ref) <= 1e-15 * np.maximum(np.abs(ref), 1.0)), (k, x, got - ref)
+        P.close()
+
+
+@pytest.mark.parametrize("row", [7, 19])
+def test_per_block_form_is_the_plain_form(tgh, oracle, row):
+    """The plain per-block form (one right-hand-side launch and one stage update per block, the
+    reference's block map) is the plain per-stage form's step bit for bit."""
+    name, case, forest, q, t = cases(tgh)[row]
+    P = tgh.GHProblem(case, forest, q, margin_check=False)
+    O = oracle.problem(case, forest, q)
+    u = _to_gpu(_initial(tgh, P, O, case, forest, name, t))
+    dt = 0.25 * (forest.h0 / 2 ** int(forest.level.max())) / 2.0
+    a, b = u.clone(), u.clone()
+    for n in range(2):
+        P.rk4_step(a, t + n * dt, dt)
+        P.rk4_step_blocks(b, t + n * dt, dt)
+    torch.cuda.synchronize()
+    assert torch.equal(a, b)
+    assert P.last_launch_count() >= 4 * 3 * forest.nblocks
+    P.close()

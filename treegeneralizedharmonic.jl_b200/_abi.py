@@ -19,6 +19,7 @@ DISS_CONSTANT, DISS_HORIZON = range(2)
 INT_NONE, INT_DAMPED, INT_FROZEN, INT_PASTED = range(4)
 PREC_FP64, PREC_MIXED = range(2)
 MASK_INTERIOR, MASK_ALL = range(2)
+TGH_PI_L1, TGH_PI_TMA = range(2)
 NDIAG = 10  # diag slots per block: C_a (0..3), H (4), M_i (5..7), mask (8), tau (9)
 
 D3 = ctypes.c_double * 3
@@ -68,6 +69,7 @@ SIGNATURES = {
     "tgh_state_length": (ctypes.c_size_t, [_VP]),
     "tgh_work_length": (ctypes.c_size_t, [_VP]),
     "tgh_copy_work": (ctypes.c_int, [_VP, _VP]),
+    "tgh_copy_work_blocks": (ctypes.c_int, [_VP, ctypes.c_int, ctypes.c_int, _VP]),
     "tgh_prepare": (ctypes.c_int, [_VP, _VP, _D]),
     "tgh_prepare_generation": (ctypes.c_int, [_VP, ctypes.POINTER(ctypes.c_long), ctypes.POINTER(ctypes.c_int)]),
     "tgh_rhs": (ctypes.c_int, [_VP, _VP, _D, _VP]),
@@ -78,6 +80,12 @@ SIGNATURES = {
     "tgh_max_speed": (ctypes.c_int, [_VP, _VP, _D, ctypes.POINTER(_D)]),
     "tgh_initial_state": (ctypes.c_int, [_VP, _VP, _D]),
     "tgh_rk4_step": (ctypes.c_int, [_VP, _VP, _D, _D]),
+    "tgh_rk4_step_blocks": (ctypes.c_int, [_VP, _VP, _D, _D]),
+    "tgh_set_variant": (ctypes.c_int, [_VP, ctypes.c_int, ctypes.c_int, ctypes.c_int]),
+    "tgh_get_variant": (ctypes.c_int, [_VP, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int),
+                                       ctypes.POINTER(ctypes.c_int)]),
+    "tgh_set_wait_limit": (ctypes.c_int, [_VP, ctypes.c_longlong]),
+    "tgh_device_status": (ctypes.c_int, [_VP]),
     "tgh_step_batched": (ctypes.c_int, [_VP, _VP, _D, _D, ctypes.c_int]),
     "tgh_error_norm": (ctypes.c_int, [_VP, _VP, _D, ctypes.POINTER(_D), ctypes.POINTER(_D)]),
     "tgh_gh_constraint": (ctypes.c_int, [_VP, _VP, _D, ctypes.c_int]),

@@ -7,7 +7,7 @@
 // their grouping follow the reference's lean spelling; the summation order inside a
 // contraction is the compiler's (fused multiply-adds), which moves results by roundoff.
 #pragma once
-#include "physics.cuh"
+#include "analytic.cuh"
 
 namespace tgh {
 

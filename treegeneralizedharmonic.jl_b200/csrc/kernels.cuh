@@ -5,7 +5,7 @@
 #pragma once
 #include <cstdint>
 
-#include "physics.cuh"
+#include "analytic.cuh"
 
 namespace tgh {
 
@@ -34,10 +34,16 @@ struct HookPt {
   int b, w;
 };
 
+// A block's working array per variable is Wd^3 points (the reference's ghosted cube) stored
+// with rows of Wx >= Wd doubles (Wx even: every row starts on a 16-byte boundary, as the tensor
+// copies into shared memory require); point (x, y, z) of the cube sits at x + Wx (y + Wd z).
 struct Geo {
-  int N1, Wd, G;
-  long S, Wv;  // points per block in state / work layout
+  int N1, Wd, G, Wx;
+  long S, Wv;  // points per block in state layout; doubles per block and variable in work layout
 };
+__host__ __device__ __forceinline__ long work_index(const Geo& g, int x, int y, int z) {
+  return x + (long)g.Wx * (y + (long)g.Wd * z);
+}
 
 // The position of point (i, j, k) of block b (i may lie in the ghost zone): blk holds per
 // block the domain's low corner, the spacing and the integer corner, 8 doubles; the point
@@ -89,7 +95,7 @@ __global__ void fill_hook_kernel(const HookPt* __restrict__ pts, int n, const do
   const int id = blockIdx.x * blockDim.x + threadIdx.x;
   if (id >= n) return;
   const HookPt p = pts[id];
-  const int i = p.w % g.Wd, j = (p.w / g.Wd) % g.Wd, k = p.w / (g.Wd * g.Wd);
+  const int i = p.w % g.Wx, j = (p.w / g.Wx) % g.Wd, k = p.w / (g.Wx * g.Wd);
   double x[3];
   point_pos(blk, p.b, i - g.G, j - g.G, k - g.G, x);
   double v20[NV];
@@ -145,7 +151,7 @@ template <int P> __host__ __device__ constexpr ProlongWeights<P> prolong_weights
 template <int P, int ODD> __device__ __forceinline__ double prolong_odd(const double* src, Geo g) {
   constexpr int cx = (ODD & 1) ? P : 1, cy = (ODD & 2) ? P : 1, cz = (ODD & 4) ? P : 1;
   constexpr ProlongWeights<P> W = prolong_weights<P>();
-  const long sy = g.Wd, sz = (long)g.Wd * g.Wd;
+  const long sy = g.Wx, sz = (long)g.Wx * g.Wd;
   double szv = 0.0;
 #pragma unroll
   for (int kz = 0; kz < cz; ++kz) {
@@ -299,7 +305,7 @@ __global__ void error_kernel(const double* __restrict__ work, const double* __re
     if (evolved(cs, t, x)) {
       double ex[NV];
       exact_state(cs, t, x, ex);
-      const double* q = work + (long)b * NV * g.Wv + (i + g.G) + (long)g.Wd * ((j + g.G) + (long)g.Wd * (k + g.G));
+      const double* q = work + (long)b * NV * g.Wv + work_index(g, i + g.G, j + g.G, k + g.G);
       double e2 = 0.0;
       for (int v = 0; v < NV; ++v) {
         const double d = q[v * g.Wv] - ex[v];
@@ -385,7 +391,7 @@ __global__ void gather_kernel(const double* __restrict__ work, double* __restric
   const int b = (int)(p / g.S);
   const long ip = p - (long)b * g.S;
   const int k = (int)(ip / ((long)g.N1 * g.N1)), j = (int)((ip / g.N1) % g.N1), i = (int)(ip % g.N1);
-  const double* q = work + (long)b * NV * g.Wv + (i + g.G) + (long)g.Wd * ((j + g.G) + (long)g.Wd * (k + g.G));
+  const double* q = work + (long)b * NV * g.Wv + work_index(g, i + g.G, j + g.G, k + g.G);
   double* o = u + (long)b * NV * g.S + ip;
 #pragma unroll
   for (int v = 0; v < NV; ++v) o[v * g.S] = q[v * g.Wv];
@@ -398,7 +404,7 @@ __global__ void scatter_owned_kernel(const double* __restrict__ u, double* __res
   const int b = (int)(p / g.S);
   const long ip = p - (long)b * g.S;
   const int k = (int)(ip / ((long)g.N1 * g.N1)), j = (int)((ip / g.N1) % g.N1), i = (int)(ip % g.N1);
-  double* q = work + (long)b * NV * g.Wv + (i + g.G) + (long)g.Wd * ((j + g.G) + (long)g.Wd * (k + g.G));
+  double* q = work + (long)b * NV * g.Wv + work_index(g, i + g.G, j + g.G, k + g.G);
   const double* s = u + (long)b * NV * g.S + ip;
 #pragma unroll
   for (int v = 0; v < NV; ++v) q[v * g.Wv] = s[v * g.S];
@@ -440,7 +446,7 @@ __global__ void error_tangent_kernel(const double* __restrict__ work, const doub
     if (cs.interior == TGH_INT_NONE || interior_radius(cs, t, x) >= cs.r1) {
       double ex[NV];
       exact_state(cs, t, x, ex);
-      const long o = (long)bk * NV * g.Wv + (i + g.G) + (long)g.Wd * ((j + g.G) + (long)g.Wd * (k + g.G));
+      const long o = (long)bk * NV * g.Wv + work_index(g, i + g.G, j + g.G, k + g.G);
       double e2 = 0.0, ed = 0.0;
       for (int v = 0; v < NV; ++v) {
         const double d = work[o + v * g.Wv] - ex[v];

@@ -21,6 +21,7 @@ struct MonArgs {
   const double* blk;
   double* diag;          // NDIAG x N1^3 per block
   int N1, Wd, G, all;    // all: every point is evolved (the trivial mask)
+  int Wx;                // the working array's row pitch (kernels.cuh Geo)
   long S, Wv, npts;
   double t;
 };
@@ -42,7 +43,7 @@ __device__ __forceinline__ MonPoint mon_point(const MonArgs& A, long p) {
   m.x[0] = __dadd_rn(bl[0], __dmul_rn(bl[4] + (double)i, m.h));
   m.x[1] = __dadd_rn(bl[1], __dmul_rn(bl[5] + (double)j, m.h));
   m.x[2] = __dadd_rn(bl[2], __dmul_rn(bl[6] + (double)k, m.h));
-  m.wk = A.work + (long)m.b * NV * A.Wv + (i + A.G) + (long)A.Wd * ((j + A.G) + (long)A.Wd * (k + A.G));
+  m.wk = A.work + (long)m.b * NV * A.Wv + (i + A.G) + (long)A.Wx * ((j + A.G) + (long)A.Wd * (k + A.G));
   return m;
 }
 
@@ -87,7 +88,7 @@ __global__ void __launch_bounds__(128) gauge_constraint_kernel(const Case cs, co
     dg[DG_MASK * A.S] = 0.0;
     return;
   }
-  const long s[3] = {1, A.Wd, (long)A.Wd * A.Wd};
+  const long s[3] = {1, A.Wx, (long)A.Wx * A.Wd};
   const double ih = 1.0 / m.h;
   double hv[NC], dth[NC], dh[3][NC];
 #pragma unroll
@@ -322,8 +323,8 @@ __global__ void __launch_bounds__(128) adm_constraint_kernel(const Case cs, cons
   P.wk = m.wk;
   P.Wv = A.Wv;
   P.s[0] = 1;
-  P.s[1] = A.Wd;
-  P.s[2] = (long)A.Wd * A.Wd;
+  P.s[1] = A.Wx;
+  P.s[2] = (long)A.Wx * A.Wd;
   P.ih = 1.0 / m.h;
   P.ih2 = P.ih * P.ih;
   double hv[NC], dh[3][NC];
@@ -530,7 +531,7 @@ static __global__ void __launch_bounds__(128) tau_kernel(const MonArgs A, const 
     const MonPoint m = mon_point(A, p);
     double tau = 0.0;
     if (A.all || evolved(cs, A.t, m.x)) {
-      const long s[3] = {1, A.Wd, (long)A.Wd * A.Wd};
+      const long s[3] = {1, A.Wx, (long)A.Wx * A.Wd};
 #pragma unroll
       for (int v = 0; v < NC; ++v) {
         const double* q = m.wk + v * A.Wv;

@@ -3,10 +3,8 @@
 // profiles and the sphere interior. Everything here is evaluated per point inside the
 // kernels (Dirichlet ghosts, the layer target, the sampled gauge source at set-up).
 //
-// Reference behaviour followed:
-//   background_state            src/initialdata.jl:1674-1694
-//   background_state_rate       src/initialdata.jl:1721-1729
-//   core_target_rate            src/initialdata.jl:1784-1796
+// Reference behaviour followed (the analytic state itself, background_state, which the
+// centred-difference rates of src/initialdata.jl:1721-1796 are built on, is in analytic.cuh):
 //   KerrSchildSource            src/gauge.jl:257-336
 //   gauge_tuple / gauge_at      src/gauge.jl:156-212  (H_b, then d_a H_b column-major)
 //   Constant/GaussianDamping    src/gauge.jl:1094-1147
@@ -22,6 +20,23 @@
 #include "../../include/tgh.h"
 
 #define TGH_HD __host__ __device__ __forceinline__
+
+// one rounded operation each, never contracted into a fused multiply-add (the interior's
+// placement and profiles and the analytic state are evaluated this way, in the reference's
+// order, so that they agree with a CPU evaluation bit for bit)
+#ifdef __CUDA_ARCH__
+#define TGH_RADD(a, b) __dadd_rn(a, b)
+#define TGH_RSUB(a, b) __dsub_rn(a, b)
+#define TGH_RMUL(a, b) __dmul_rn(a, b)
+#define TGH_RDIV(a, b) __ddiv_rn(a, b)
+#define TGH_RSQRT(a) __dsqrt_rn(a)
+#else
+#define TGH_RADD(a, b) ((a) + (b))
+#define TGH_RSUB(a, b) ((a) - (b))
+#define TGH_RMUL(a, b) ((a) * (b))
+#define TGH_RDIV(a, b) ((a) / (b))
+#define TGH_RSQRT(a) std::sqrt(a)
+#endif
 
 namespace tgh {
 
@@ -310,38 +325,6 @@ template <class T> TGH_HD void metric_quantities(const T* h, Coef<T>& C) {
   C.sqrtg = dsqrt(T(1.0) + detgm1);
 }
 
-// the analytic state (h, Pi) at (t, x) from one dual pass (background_state)
-TGH_HD void background_state(const Case& c, double t, const double* x, double* h, double* Pi,
-                             double* dtg_out = nullptr) {
-  Dn<double> p[4];
-  const double pv[4] = {t, x[0], x[1], x[2]};
-#pragma unroll
-  for (int i = 0; i < 4; ++i) {
-    p[i] = dconst(pv[i]);
-    p[i].d[i] = 1.0;
-  }
-  Dn<double> g[4][4];
-  metric(c, p, g);
-  double dtg[NC], dh[3][NC];
-#pragma unroll
-  for (int n = 0; n < NC; ++n) {
-    const Dn<double>& e = g[prow(n)][pcol(n)];
-    h[n] = e.v - (prow(n) == pcol(n) ? etad(prow(n)) : 0.0);
-    dtg[n] = e.d[0];
-    dh[0][n] = e.d[1];
-    dh[1][n] = e.d[2];
-    dh[2][n] = e.d[3];
-  }
-  Coef<double> C;
-  metric_quantities(h, C);
-  double f = C.sqrtg / C.alpha;
-#pragma unroll
-  for (int n = 0; n < NC; ++n) {
-    Pi[n] = f * (dtg[n] - C.beta[0] * dh[0][n] - C.beta[1] * dh[1][n] - C.beta[2] * dh[2][n]);
-    if (dtg_out) dtg_out[n] = dtg[n];
-  }
-}
-
 // H_b = -g^{cd} Gamma_{b,cd} of the background and d_a H_b, by nested forward-mode numbers;
 // out[0..3] = H_b, out[4 + a + 4 b] = d_a H_b (the sampled field's 20 values)
 TGH_HD void gauge_tuple(const Case& c, double t, const double* x, double* out) {
@@ -420,32 +403,41 @@ TGH_HD void ks_gauge_source(const Case& c, const T* h, const T* const D[4], T Hl
   }
 }
 
-// ---- profiles ----
+// ---- profiles (each operation rounded on its own, in the reference's order) ----
+// src/interior.jl:117-120
 TGH_HD double smoothstep(double s) {
-  double u = s < 0.0 ? 0.0 : (s > 1.0 ? 1.0 : s);
-  double p = u * u * u * (10.0 + u * (6.0 * u - 15.0));
+  const double u = s < 0.0 ? 0.0 : (s > 1.0 ? 1.0 : s);
+  const double uuu = TGH_RMUL(TGH_RMUL(u, u), u);
+  const double p = TGH_RMUL(uuu, TGH_RADD(10.0, TGH_RMUL(u, TGH_RSUB(TGH_RMUL(6.0, u), 15.0))));
   return p < 0.0 ? 0.0 : (p > 1.0 ? 1.0 : p);
+}
+// |x - (c0 + t v)|
+TGH_HD double moving_distance(const double c0[3], const double v[3], double t, const double* x) {
+  double d[3];
+#pragma unroll
+  for (int i = 0; i < 3; ++i) d[i] = TGH_RSUB(x[i], TGH_RADD(c0[i], TGH_RMUL(t, v[i])));
+  return TGH_RSQRT(TGH_RADD(TGH_RADD(TGH_RMUL(d[0], d[0]), TGH_RMUL(d[1], d[1])), TGH_RMUL(d[2], d[2])));
 }
 TGH_HD double damping_rate(const Case& c, double t, const double* x) {
   if (c.damping == TGH_DAMP_CONSTANT) return c.g0;
-  double d1 = x[0] - (c.dc0[0] + t * c.dv[0]), d2 = x[1] - (c.dc0[1] + t * c.dv[1]),
-         d3 = x[2] - (c.dc0[2] + t * c.dv[2]);
-  double r2 = d1 * d1 + d2 * d2 + d3 * d3;
-  return c.dfar + (c.dnear - c.dfar) * exp(-r2 / (2.0 * c.dwidth * c.dwidth));
+  double d[3];
+#pragma unroll
+  for (int i = 0; i < 3; ++i) d[i] = TGH_RSUB(x[i], TGH_RADD(c.dc0[i], TGH_RMUL(t, c.dv[i])));
+  const double r2 = TGH_RADD(TGH_RADD(TGH_RMUL(d[0], d[0]), TGH_RMUL(d[1], d[1])), TGH_RMUL(d[2], d[2]));
+  const double e = exp(TGH_RDIV(-r2, TGH_RMUL(TGH_RMUL(2.0, c.dwidth), c.dwidth)));
+  return TGH_RADD(c.dfar, TGH_RMUL(TGH_RSUB(c.dnear, c.dfar), e));
 }
 TGH_HD double dissipation_rate(const Case& c, double t, const double* x) {
   if (c.dissipation == TGH_DISS_CONSTANT) return c.eps;
-  double d1 = x[0] - (c.ec0[0] + t * c.ev[0]), d2 = x[1] - (c.ec0[1] + t * c.ev[1]),
-         d3 = x[2] - (c.ec0[2] + t * c.ev[2]);
-  double r = sqrt(d1 * d1 + d2 * d2 + d3 * d3);
+  const double r = moving_distance(c.ec0, c.ev, t, x);
   if (r >= c.erh) return c.eout;
   if (r <= c.er1) return c.ein;
-  return c.eout + (c.ein - c.eout) * smoothstep((c.erh - r) / (c.erh - c.er1));
+  const double s = TGH_RDIV(TGH_RSUB(c.erh, r), TGH_RSUB(c.erh, c.er1));
+  return TGH_RADD(c.eout, TGH_RMUL(TGH_RSUB(c.ein, c.eout), smoothstep(s)));
 }
+// the distance from the interior's centre c0 + t v (HoleCenter, src/interior.jl:75-93)
 TGH_HD double interior_radius(const Case& c, double t, const double* x) {
-  double d1 = x[0] - (c.ic0[0] + t * c.iv[0]), d2 = x[1] - (c.ic0[1] + t * c.iv[1]),
-         d3 = x[2] - (c.ic0[2] + t * c.iv[2]);
-  return sqrt(d1 * d1 + d2 * d2 + d3 * d3);
+  return moving_distance(c.ic0, c.iv, t, x);
 }
 // is_evolved(mask, x) of the interior's mask: r >= r_1 (src/constraints.jl:74-75)
 TGH_HD bool evolved(const Case& cs, double t, const double* x) {
@@ -454,41 +446,50 @@ TGH_HD bool evolved(const Case& cs, double t, const double* x) {
 TGH_HD bool core_follows(const Case& c) {
   return c.interior == TGH_INT_DAMPED && !(c.iv[0] == 0.0 && c.iv[1] == 0.0 && c.iv[2] == 0.0);
 }
+// core_position (src/interior.jl:615-625): a point of the core is placed on the sphere r_0
+// along its direction from the centre (straight up at the centre itself)
 TGH_HD void core_position(const Case& c, double t, const double* x, double* out) {
   if (c.interior == TGH_INT_NONE) {
     out[0] = x[0]; out[1] = x[1]; out[2] = x[2];
     return;
   }
-  double cc[3] = {c.ic0[0] + t * c.iv[0], c.ic0[1] + t * c.iv[1], c.ic0[2] + t * c.iv[2]};
-  double d[3] = {x[0] - cc[0], x[1] - cc[1], x[2] - cc[2]};
-  double r = sqrt(d[0] * d[0] + d[1] * d[1] + d[2] * d[2]);
+  double cc[3], d[3];
+#pragma unroll
+  for (int i = 0; i < 3; ++i) {
+    cc[i] = TGH_RADD(c.ic0[i], TGH_RMUL(t, c.iv[i]));
+    d[i] = TGH_RSUB(x[i], cc[i]);
+  }
+  const double r = TGH_RSQRT(TGH_RADD(TGH_RADD(TGH_RMUL(d[0], d[0]), TGH_RMUL(d[1], d[1])), TGH_RMUL(d[2], d[2])));
   if (r >= c.r0) {
     out[0] = x[0]; out[1] = x[1]; out[2] = x[2];
     return;
   }
   double n[3] = {0.0, 0.0, 1.0};
-  if (r != 0.0) { n[0] = d[0] / r; n[1] = d[1] / r; n[2] = d[2] / r; }
-  for (int i = 0; i < 3; ++i) out[i] = cc[i] + c.r0 * n[i];
+  if (r != 0.0) {
+#pragma unroll
+    for (int i = 0; i < 3; ++i) n[i] = TGH_RDIV(d[i], r);
+  }
+#pragma unroll
+  for (int i = 0; i < 3; ++i) out[i] = TGH_RADD(cc[i], TGH_RMUL(c.r0, n[i]));
 }
+// _layer_profiles (src/interior.jl:567-590): the switch-on w and the relaxation rate rho
 TGH_HD void layer_profiles(const Case& c, double r, double& w, double& rho) {
-  double s = (r - c.r0) / (c.r1 - c.r0);
-  w = smoothstep(s / c.w_ramp);
-  rho = c.interior == TGH_INT_FROZEN ? 0.0 : c.rho_max * smoothstep((1.0 - s) / c.rho_ramp);
+  const double s = TGH_RDIV(TGH_RSUB(r, c.r0), TGH_RSUB(c.r1, c.r0));
+  w = smoothstep(TGH_RDIV(s, c.w_ramp));
+  rho = c.interior == TGH_INT_FROZEN ? 0.0 : TGH_RMUL(c.rho_max, smoothstep(TGH_RDIV(TGH_RSUB(1.0, s), c.rho_ramp)));
 }
 TGH_HD double core_rate(const Case& c) {
-  double s = sqrt(c.iv[0] * c.iv[0] + c.iv[1] * c.iv[1] + c.iv[2] * c.iv[2]);
-  double k = 12.0 * s / c.r0;
+  const double s = TGH_RSQRT(TGH_RADD(TGH_RADD(TGH_RMUL(c.iv[0], c.iv[0]), TGH_RMUL(c.iv[1], c.iv[1])),
+                                      TGH_RMUL(c.iv[2], c.iv[2])));
+  const double k = TGH_RDIV(TGH_RMUL(12.0, s), c.r0);
   return c.rho_max > k ? c.rho_max : k;
+}
+// core_rate_weight (src/interior.jl:560-565): smoothstep(4 r / r_0 - 1)
+TGH_HD double core_rate_weight(const Case& c, double r) {
+  return smoothstep(TGH_RSUB(TGH_RDIV(TGH_RMUL(4.0, r), c.r0), 1.0));
 }
 // cbrt(eps) r_0 with eps the double epsilon (src/interior.jl:545)
 TGH_HD double layer_rate_step(const Case& c) { return 6.0554544523933395e-06 * c.r0; }
-
-// the state the case puts at x (case_state_tuple): the background through the core rule
-TGH_HD void exact_state(const Case& c, double t, const double* x, double* out) {
-  double xc[3];
-  core_position(c, t, x, xc);
-  background_state(c, t, xc, out, out + NC);
-}
 
 TGH_HD void inv3sym(const double g[3][3], double o[3][3]) {
   double c00 = g[1][1] * g[2][2] - g[1][2] * g[2][1];

@@ -17,9 +17,21 @@
 #include "kernels.cuh"
 #include "monitors.cuh"
 #include "rhs_inst.cuh"
+#include "rhs_pi_tma.cuh"
 #include "tangent_rhs.cuh"
 
 using namespace tgh;
+
+namespace tgh {
+bool make_pi_tma_maps(double* work, int nwb, PiTmaMaps* out, std::string& err);
+cudaError_t launch_pi_tma(bool diss, int mode, cudaStream_t s, const Case& cs, const RhsArgs& a, const PiTmaMaps& M,
+                          PiTmaStatus st, int b0, int nb);
+}  // namespace tgh
+
+// the Pi kernel a problem launches: the one-point kernel reading through L1, or the pair kernel
+// whose stencil tiles the Tensor Memory Accelerator stages into shared memory (q = 4, N = 32,
+// FP64 only; the one-point kernel serves every other problem)
+enum { PI_L1 = TGH_PI_L1, PI_TMA = TGH_PI_TMA };
 
 struct GraphKey {
   double t, dt;
@@ -39,7 +51,7 @@ struct tgh_problem {
   tgh_config cfg;
   // nb: the blocks this rank computes (its own leaves); nwb: the working arrays' blocks, its
   // own leaves first, then the halo: other ranks' leaves its fill reads
-  int q, G, N, N1, Wd, nb, nwb, maxlevel = 0;
+  int q, G, N, N1, Wd, Wx, nb, nwb, maxlevel = 0;  // Wx: the working array's row pitch
   double lo[3], h0;
   int cells0[3], periodic[3];
   std::vector<int> level, corner;  // of every leaf of the forest (global numbering)
@@ -113,6 +125,22 @@ struct tgh_problem {
   long prep_gen = 0;
   bool work_prepared = false;
   const char* work_writer = "nothing (no tgh_prepare yet)";
+  // the right-hand side's kernel variants (tgh_set_variant) and the TMA kernel's tensor maps,
+  // one pair per working array it has read
+  int pi_variant = PI_L1;
+  int threads = 128;  // CTA size of the head and one-point Pi kernels
+  int pi_mb = 4;      // the one-point Pi kernel's resident CTAs per SM (its launch bound)
+  std::vector<std::pair<const double*, PiTmaMaps>> tma_maps;
+  int* dev_err = nullptr;                 // a bounded device wait that gave up records it here
+  // the blocks interior_kernel visits: those that can hold a point with r < r_1 at some time of
+  // [lo, hi]; one list for direct launches, one for the captured graph (built before capture)
+  struct BlockList {
+    int* dev = nullptr;
+    int n = -1;
+    double lo = 0, hi = -1;
+  } ilist, ilist_graph;
+  const BlockList* ilist_use = nullptr;
+  long long wait_limit = 1ll << 26;       // polls a device wait may make
 };
 
 #define CK(call)                                                         \
@@ -128,6 +156,11 @@ static int fail(tgh_problem* p, int code, const std::string& msg) {
   p->err = msg;
   return code;
 }
+
+// doubles in one of the problem's working arrays (rows padded to the pitch Wx)
+static size_t work_doubles(const tgh_problem* p) { return (size_t)p->Wv * NV * p->nwb; }
+// a padded work index as the index of the same point in the reference's dense cube
+static int dense_index(const tgh_problem* p, int w) { return (w % p->Wx) + p->Wd * (w / p->Wx); }
 
 // a verb other than tgh_prepare wrote the working array: the next tgh_rhs needs a new prepare
 static void work_overwritten(tgh_problem* p, const char* who) {
@@ -294,7 +327,7 @@ static bool plan_rank(const tgh_problem* p, int r, bool entries, HostPlan& hp, s
   prol.assign(p->maxlevel + 1, {});
   if (entries) prim.assign((size_t)hp.nloc * p->S, 0);
   const bool one = p->nranks == 1;
-  const int Wd = p->Wd, G = p->G, P = p->q + 2;
+  const int Wd = p->Wd, Wx = p->Wx, G = p->G, P = p->q + 2;
   for (int b = 0; b < hp.nloc; ++b) {
     const int gb = hp.i2g[b];
     const int l = p->level[gb];
@@ -315,12 +348,12 @@ static bool plan_rank(const tgh_problem* p, int r, bool entries, HostPlan& hp, s
               outside = true;
             }
           }
-          const int w = i + Wd * (j + Wd * k);
+          const int w = i + Wx * (j + Wd * k);
           int leaf = -1, loc[3], lev = -1;
           if (!outside && find_owner(p, l, n, leaf, loc, lev)) {
             const int step = 1 << (lev - l);
             const bool own = i >= G && i <= G + p->N && j >= G && j <= G + p->N && k >= G && k <= G + p->N;
-            const int sw = (loc[0] + G) + Wd * ((loc[1] + G) + Wd * (loc[2] + G));
+            const int sw = (loc[0] + G) + Wx * ((loc[1] + G) + Wd * (loc[2] + G));
             if (own && leaf == gb) {
               if (entries) prim[(size_t)b * p->S + (i - G) + (size_t)p->N1 * ((j - G) + (size_t)p->N1 * (k - G))] = 1;
             } else {
@@ -373,12 +406,12 @@ static bool plan_rank(const tgh_problem* p, int r, bool entries, HostPlan& hp, s
             }
           }
           const int sw = (int)((base[0] - p->corner[3 * c] + G) +
-                               Wd * ((base[1] - p->corner[3 * c + 1] + G) + (int64_t)Wd * (base[2] - p->corner[3 * c + 2] + G)));
+                               Wx * ((base[1] - p->corner[3 * c + 1] + G) + (int64_t)Wd * (base[2] - p->corner[3 * c + 2] + G)));
           if (p->owner[c] != r) {
             auto& v = hp.req[{p->owner[c], l}];
             for (int64_t kz = 0; kz < ext[2]; ++kz)
               for (int64_t ky = 0; ky < ext[1]; ++ky)
-                for (int64_t kx = 0; kx < ext[0]; ++kx) v.push_back({c, (int)(sw + kx + Wd * (ky + Wd * kz))});
+                for (int64_t kx = 0; kx < ext[0]; ++kx) v.push_back({c, (int)(sw + kx + Wx * (ky + Wd * kz))});
           }
           if (entries) prol[l].push_back(ProlongPt{b, w, intern(c), sw, odd});
         }
@@ -543,10 +576,87 @@ static cudaError_t launch_part(tgh_problem* p, int part, int mode, cudaStream_t 
   }
 }
 
-// One right-hand side: the head kernel, then the Pi kernel, over all blocks on the problem's
-// stream.
+// whether a launch may take the TMA Pi kernel: the variant chosen, its configuration, whole blocks
+static bool pi_tma_applies(const tgh_problem* p, const RhsArgs& a) {
+  return p->pi_variant == PI_TMA && p->q == 4 && p->N == 32 && !p->mixed && a.p0 % p->S == 0 && a.p1 % p->S == 0;
+}
+
+// the tensor maps of one of the problem's working arrays (made once per array)
+static const PiTmaMaps* pi_tma_maps(tgh_problem* p, const double* work) {
+  for (auto& e : p->tma_maps)
+    if (e.first == work) return &e.second;
+  PiTmaMaps m;
+  std::string err;
+  if (!make_pi_tma_maps(const_cast<double*>(work), p->nwb, &m, err)) {
+    p->err = err;
+    return nullptr;
+  }
+  p->tma_maps.push_back({work, m});
+  return &p->tma_maps.back().second;
+}
+
+// The blocks of this rank that can hold a point with r < r_1 while t runs over [tlo, thi]: their
+// boxes lie within r_1 of the axis-aligned box around the centre's path c0 + t v (a superset; the
+// kernel decides point by point). Built on the host, copied to the list's device buffer.
+static int interior_blocks(tgh_problem* p, tgh_problem::BlockList& L, double tlo, double thi) {
+  if (!p->intr) return TGH_OK;
+  if (L.n >= 0 && L.lo == tlo && L.hi == thi) return TGH_OK;
+  if (!L.dev) CK(cudaMalloc(&L.dev, (size_t)p->nb * sizeof(int)));
+  double clo[3], chi[3];
+  for (int d = 0; d < 3; ++d) {
+    const double a = p->cfg.int_c0[d] + tlo * p->cfg.int_v[d], b = p->cfg.int_c0[d] + thi * p->cfg.int_v[d];
+    clo[d] = std::min(a, b);
+    chi[d] = std::max(a, b);
+  }
+  std::vector<int> v;
+  for (int b = 0; b < p->nb; ++b) {
+    const int g = p->i2g[b];
+    const double h = std::ldexp(p->h0, -p->level[g]);
+    double d2 = 0.0;
+    for (int d = 0; d < 3; ++d) {
+      const double lo = p->lo[d] + p->corner[3 * g + d] * h, hi = lo + p->N * h;
+      const double gap = std::max(0.0, std::max(lo - chi[d], clo[d] - hi));
+      d2 += gap * gap;
+    }
+    if (std::sqrt(d2) <= p->cfg.r1 * (1.0 + 1e-12) + 1e-12) v.push_back(b);
+  }
+  if (!v.empty())
+    CK(cudaMemcpyAsync(L.dev, v.data(), v.size() * sizeof(int), cudaMemcpyHostToDevice, p->stream));
+  CK(cudaStreamSynchronize(p->stream));  // the host vector goes out of scope
+  L.n = (int)v.size();
+  L.lo = tlo;
+  L.hi = thi;
+  return TGH_OK;
+}
+
+// One right-hand side over all blocks on the problem's stream: the interior's points (a problem
+// with an interior, over the blocks of the list in use), the head kernel, then the Pi kernel.
 static int launch_rhs(tgh_problem* p, const RhsArgs& a, int mode) {
+  if (p->intr) {
+    const tgh_problem::BlockList* L = p->ilist_use;
+    if (!L) {
+      // a direct launch: the list for this t
+      int s = interior_blocks(p, p->ilist, a.t, a.t);
+      if (s) return s;
+      L = &p->ilist;
+    }
+    if (L->n > 0) {
+      const long per = (p->S + 127) / 128;
+      if (mode == MODE_DU)
+        interior_kernel<MODE_DU><<<(unsigned)(L->n * per), 128, 0, p->stream>>>(p->cs, a, L->dev);
+      else
+        interior_kernel<MODE_STAGE><<<(unsigned)(L->n * per), 128, 0, p->stream>>>(p->cs, a, L->dev);
+      CK(cudaGetLastError());
+    }
+  }
   CK(launch_part(p, 0, mode, p->stream, a));
+  if (pi_tma_applies(p, a)) {
+    const PiTmaMaps* M = pi_tma_maps(p, a.work);
+    if (!M) return TGH_ERR_CUDA;
+    CK(launch_pi_tma(p->diss, mode, p->stream, p->cs, a, *M, PiTmaStatus{p->dev_err, p->wait_limit},
+                     (int)(a.p0 / p->S), (int)((a.p1 - a.p0) / p->S)));
+    return TGH_OK;
+  }
   CK(launch_part(p, 1, mode, p->stream, a));
   return TGH_OK;
 }
@@ -560,11 +670,14 @@ static RhsArgs base_args(tgh_problem* p, const double* work, double t) {
   a.blk = p->blk;
   a.N1 = p->N1;
   a.Wd = p->Wd;
+  a.Wx = p->Wx;
   a.G = p->G;
   a.npts = p->npts;
   a.p0 = 0;
   a.p1 = p->npts;
   a.t = t;
+  a.threads = p->threads;
+  a.pi_mb = p->pi_mb;
   return a;
 }
 
@@ -697,6 +810,7 @@ static int setup_host(tgh_problem* p, const tgh_config* cfg, const tgh_mesh* m, 
   p->N = m->N;
   p->N1 = m->N + 1;
   p->Wd = m->N + 2 * p->G + 1;
+  p->Wx = p->Wd + (p->Wd & 1);
   p->h0 = m->h0;
   for (int d = 0; d < 3; ++d) {
     p->lo[d] = m->lo[d];
@@ -718,9 +832,9 @@ static int setup_host(tgh_problem* p, const tgh_config* cfg, const tgh_mesh* m, 
     if (!p->lut[p->level[b]].emplace(key, b).second) return fail(p, TGH_ERR_ARG, "two leaves share a corner and level");
   }
   p->S = (long)p->N1 * p->N1 * p->N1;
-  p->Wv = (long)p->Wd * p->Wd * p->Wd;
+  p->Wv = (long)p->Wx * p->Wd * p->Wd;
   p->npts = p->S * p->nb;
-  p->geo = Geo{p->N1, p->Wd, p->G, p->S, p->Wv};
+  p->geo = Geo{p->N1, p->Wd, p->G, p->Wx, p->S, p->Wv};
   p->cs = make_case(*cfg);
   p->diss = cfg->dissipation == TGH_DISS_CONSTANT ? cfg->eps_ko != 0.0 : !(cfg->eps_out == 0.0 && cfg->eps_in == 0.0);
   p->intr = cfg->interior != TGH_INT_NONE;
@@ -775,6 +889,8 @@ static int setup_device(tgh_problem* p) {
   CK(cudaMemsetAsync(p->work, 0, (size_t)p->Wv * NV * p->nwb * sizeof(double), p->stream));
   CK(cudaMalloc(&p->scratch, 2 * sizeof(unsigned long long)));
   CK(cudaMalloc(&p->bcounts, 3 * sizeof(unsigned long long)));
+  CK(cudaMalloc(&p->dev_err, sizeof(int)));
+  CK(cudaMemsetAsync(p->dev_err, 0, sizeof(int), p->stream));
   CK(cudaMalloc(&p->coef, (size_t)NCOEF * p->npts * sizeof(double)));
   p->npart = (int)grid_for(p->npts, 128);
   CK(cudaMalloc(&p->part, (3 * (size_t)p->npart + 2) * sizeof(double)));
@@ -813,7 +929,7 @@ void tgh_problem_destroy(tgh_problem* p) {
     if (x.recv) cudaFree(x.recv);
   }
   void* bufs[] = {p->work, p->Hsrc, p->blk, p->primary, p->runs, p->gpts, p->hooks, p->hook_cache, p->scratch,
-                  p->bcounts,
+                  p->bcounts, p->dev_err, p->ilist.dev, p->ilist_graph.dev,
                   p->part, p->coef, p->diag, p->dpart, p->ind, p->ind_tol, p->ind_counts, p->ind_boxes,
                   p->k, p->acc, p->y, p->u0, p->W1, p->W2, p->bacc, p->twork, p->kt, p->acct, p->yt};
   for (void* b : bufs)
@@ -825,10 +941,20 @@ void tgh_problem_destroy(tgh_problem* p) {
 
 const char* tgh_last_error(const tgh_problem* p) { return p ? p->err.c_str() : "no problem"; }
 size_t tgh_state_length(const tgh_problem* p) { return (size_t)p->S * NV * p->nb; }
-size_t tgh_work_length(const tgh_problem* p) { return (size_t)p->Wv * NV * p->nwb; }
+// The ABI's view of the working array is the reference's layout, (N+2G+1)^3 points per block
+// and variable; the problem stores rows padded to the even pitch Wx.
+size_t tgh_work_length(const tgh_problem* p) { return (size_t)p->Wd * p->Wd * p->Wd * NV * p->nwb; }
 
-int tgh_copy_work(tgh_problem* p, double* dst) {
-  CK(cudaMemcpyAsync(dst, p->work, tgh_work_length(p) * sizeof(double), cudaMemcpyDeviceToDevice, p->stream));
+int tgh_copy_work(tgh_problem* p, double* dst) { return tgh_copy_work_blocks(p, 0, p->nwb, dst); }
+
+int tgh_copy_work_blocks(tgh_problem* p, int b0, int nblocks, double* dst) {
+  if (b0 < 0 || nblocks < 0 || b0 + nblocks > p->nwb) return fail(p, TGH_ERR_ARG, "block range out of bounds");
+  if (nblocks == 0) return TGH_OK;
+  // one row of Wd doubles per copy: rows of the padded array are Wx apart, of the dense one Wd
+  const size_t rows = (size_t)p->Wd * p->Wd * NV * nblocks;
+  CK(cudaMemcpy2DAsync(dst, (size_t)p->Wd * sizeof(double), p->work + (size_t)p->Wv * NV * b0,
+                       (size_t)p->Wx * sizeof(double), (size_t)p->Wd * sizeof(double), rows, cudaMemcpyDeviceToDevice,
+                       p->stream));
   CK(cudaStreamSynchronize(p->stream));
   return TGH_OK;
 }
@@ -872,6 +998,7 @@ static int monitor_prepare(tgh_problem* p, const double* u, double t, int mask, 
   a.diag = p->diag;
   a.N1 = p->N1;
   a.Wd = p->Wd;
+  a.Wx = p->Wx;
   a.G = p->G;
   a.all = mask == TGH_MASK_ALL;
   a.S = p->S;
@@ -996,7 +1123,7 @@ int tgh_transfer(tgh_problem* dst, tgh_problem* src, const double* u_src, double
   if (!same) return fail(dst, TGH_ERR_ARG, "the two problems differ in order, block size or root grid");
   int s = prepare_impl(src, u_src, t, "tgh_transfer (as its source)");
   if (s) return s;
-  const int G = src->G, Wd = src->Wd, P = src->q + 2;
+  const int G = src->G, Wd = src->Wd, Wx = src->Wx, P = src->q + 2;
   std::vector<CopyPt> cp;
   std::vector<ProlongPt> pp;
   for (int b = 0; b < dst->nb; ++b) {
@@ -1015,7 +1142,7 @@ int tgh_transfer(tgh_problem* dst, tgh_problem* src, const double* u_src, double
             }
           int leaf, loc[3], lev;
           if (find_owner(src, l, n, leaf, loc, lev)) {
-            const int sw = (loc[0] + G) + Wd * ((loc[1] + G) + Wd * (loc[2] + G));
+            const int sw = (loc[0] + G) + Wx * ((loc[1] + G) + Wd * (loc[2] + G));
             cp.push_back(CopyPt{b, ip, src->g2i[leaf], sw});
             continue;
           }
@@ -1032,7 +1159,7 @@ int tgh_transfer(tgh_problem* dst, tgh_problem* src, const double* u_src, double
               return fail(dst, TGH_ERR_ARG, "a prolongation stencil of the transfer leaves the old block's ghost zone");
           }
           const int sw = (int)((base[0] - src->corner[3 * c] + G) +
-                               Wd * ((base[1] - src->corner[3 * c + 1] + G) + (int64_t)Wd * (base[2] - src->corner[3 * c + 2] + G)));
+                               Wx * ((base[1] - src->corner[3 * c + 1] + G) + (int64_t)Wd * (base[2] - src->corner[3 * c + 2] + G)));
           pp.push_back(ProlongPt{b, ip, src->g2i[c], sw, odd});
         }
   }
@@ -1075,6 +1202,53 @@ int tgh_transfer(tgh_problem* dst, tgh_problem* src, const double* u_src, double
 int tgh_copy_diag(tgh_problem* p, double* out) {
   CK(cudaMemcpyAsync(out, p->diag, (size_t)NDIAG * p->npts * sizeof(double), cudaMemcpyDeviceToDevice, p->stream));
   return TGH_OK;
+}
+
+// ---- the right-hand side's kernel variants (the autotuner's choices) and device waits ----
+int tgh_set_variant(tgh_problem* p, int pi_variant, int threads, int pi_mb) {
+  if (pi_variant != TGH_PI_L1 && pi_variant != TGH_PI_TMA) return fail(p, TGH_ERR_ARG, "unknown Pi kernel variant");
+  if (pi_variant == TGH_PI_TMA && !(p->q == 4 && p->N == 32 && !p->mixed))
+    return fail(p, TGH_ERR_ARG, "the TMA Pi kernel serves q = 4, N = 32, FP64 problems only");
+  if (threads != 64 && threads != 128) return fail(p, TGH_ERR_ARG, "the CTA size must be 64 or 128");
+  if (pi_mb < 3 || pi_mb > 5) return fail(p, TGH_ERR_ARG, "the one-point Pi kernel's CTAs per SM must be 3, 4 or 5");
+  if (pi_variant == TGH_PI_TMA) {
+    // check now that the driver can describe the working array to the copy engine
+    if (!pi_tma_maps(p, p->work)) return TGH_ERR_CUDA;
+  }
+  p->pi_variant = pi_variant;
+  p->threads = threads;
+  p->pi_mb = pi_mb;
+  if (p->gexec) {  // a captured step holds the old kernels
+    cudaGraphExecDestroy(p->gexec);
+    p->gexec = nullptr;
+  }
+  return TGH_OK;
+}
+
+int tgh_get_variant(const tgh_problem* p, int* pi_variant, int* threads, int* pi_mb) {
+  *pi_variant = p->pi_variant;
+  *threads = p->threads;
+  *pi_mb = p->pi_mb;
+  return TGH_OK;
+}
+
+int tgh_set_wait_limit(tgh_problem* p, long long polls) {
+  p->wait_limit = polls;
+  if (p->gexec) {
+    cudaGraphExecDestroy(p->gexec);
+    p->gexec = nullptr;
+  }
+  return TGH_OK;
+}
+
+int tgh_device_status(tgh_problem* p) {
+  int h = 0;
+  CK(cudaMemcpyAsync(&h, p->dev_err, sizeof(int), cudaMemcpyDeviceToHost, p->stream));
+  CK(cudaStreamSynchronize(p->stream));
+  if (h == 0) return TGH_OK;
+  CK(cudaMemsetAsync(p->dev_err, 0, sizeof(int), p->stream));
+  CK(cudaStreamSynchronize(p->stream));
+  return fail(p, h, "a bounded wait inside a kernel gave up (its results were not written)");
 }
 
 int tgh_rhs(tgh_problem* p, double* du, double t, const double* matter) {
@@ -1215,6 +1389,62 @@ int tgh_rk4_step(tgh_problem* p, double* u, double t, double dt) {
   return stage_limit_impl(p, u, te);
 }
 
+// The plain per-block form: the reference's block-wise map (map_blocks!, src/evolution.jl:1387)
+// as host-issued launches, one right-hand side (head and Pi kernel) and one stage update per
+// block and stage, after the same fill as the plain form. The baseline the batched form's
+// fusion and graph are measured against; its arithmetic is the plain form's.
+static int gh_rhs_blocks(tgh_problem* p, double* du, const double* u, double t) {
+  int s = prepare_impl(p, u, t, "tgh_rk4_step_blocks");
+  if (s) return s;
+  for (int b = 0; b < p->nb; ++b) {
+    RhsArgs a = base_args(p, p->work, t);
+    a.du = du;
+    a.p0 = (long)b * p->S;
+    a.p1 = (long)(b + 1) * p->S;
+    if ((s = launch_rhs(p, a, MODE_DU))) return s;
+  }
+  return TGH_OK;
+}
+
+static int stage_update_blocks(tgh_problem* p, int kind, const double* k, const double* u0, double* acc, double* y,
+                               double* uout, double ca, double cb) {
+  const long per = (long)NV * p->S;
+  const unsigned g = (unsigned)grid_for(per, 256);
+  for (int b = 0; b < p->nb; ++b) {
+    const long o = per * b;
+    stage_update_kernel<<<g, 256, 0, p->stream>>>(kind, per, k + o, u0 ? u0 + o : nullptr, acc + o,
+                                                  y ? y + o : nullptr, uout ? uout + o : nullptr, ca, cb);
+    CK(cudaGetLastError());
+  }
+  return TGH_OK;
+}
+
+int tgh_rk4_step_blocks(tgh_problem* p, double* u, double t, double dt) {
+  if (p->nranks > 1) return fail(p, TGH_ERR_ARG, "the per-block form runs on a problem of one rank");
+  const size_t L = tgh_state_length(p);
+  if (!p->k) CK(cudaMalloc(&p->k, L * sizeof(double)));
+  if (!p->acc) {
+    CK(cudaMalloc(&p->acc, L * sizeof(double)));
+    CK(cudaMalloc(&p->y, L * sizeof(double)));
+  }
+  const double b16 = dt / 6.0, b13 = dt / 3.0, a12 = 0.5 * dt;
+  const double tm = t + 0.5 * dt, te = t + dt;
+  int s;
+  if ((s = gh_rhs_blocks(p, p->k, u, t))) return s;
+  if ((s = stage_update_blocks(p, 0, p->k, u, p->acc, p->y, nullptr, a12, b16))) return s;
+  if ((s = stage_limit_impl(p, p->y, tm))) return s;
+  if ((s = gh_rhs_blocks(p, p->k, p->y, tm))) return s;
+  if ((s = stage_update_blocks(p, 1, p->k, u, p->acc, p->y, nullptr, a12, b13))) return s;
+  if ((s = stage_limit_impl(p, p->y, tm))) return s;
+  if ((s = gh_rhs_blocks(p, p->k, p->y, tm))) return s;
+  if ((s = stage_update_blocks(p, 1, p->k, u, p->acc, p->y, nullptr, dt, b13))) return s;
+  if ((s = stage_limit_impl(p, p->y, te))) return s;
+  if ((s = gh_rhs_blocks(p, p->k, p->y, te))) return s;
+  if ((s = stage_update_blocks(p, 2, p->k, nullptr, p->acc, nullptr, u, 0.0, b16))) return s;
+  p->last_launches = 4 * (fill_launches(p, false) + 3L * p->nb);
+  return stage_limit_impl(p, u, te);
+}
+
 // batched form, one step's launches on the stream (captured into a graph by the caller)
 // Stage st (0..3) of the batched form's RK4 step from t: the time it evaluates at, the working
 // array it reads (filled first) and the one it writes, and its update coefficients.
@@ -1272,7 +1502,7 @@ static int launch_fill_phase(tgh_problem* p, double* work, int phase, double t) 
 
 static int batched_buffers(tgh_problem* p) {
   if (p->W1) return TGH_OK;
-  const size_t Lw = tgh_work_length(p), L = tgh_state_length(p);
+  const size_t Lw = work_doubles(p), L = tgh_state_length(p);
   CK(cudaMalloc(&p->W1, Lw * sizeof(double)));
   CK(cudaMalloc(&p->W2, Lw * sizeof(double)));
   CK(cudaMalloc(&p->bacc, L * sizeof(double)));
@@ -1307,15 +1537,19 @@ int tgh_step_batched(tgh_problem* p, double* u, double t, double dt, int nsteps)
     // capture on the problem's own stream (the caller's may be the legacy default stream,
     // which cannot be captured); the graph is then launched on the caller's stream
     if (!p->cap) CK(cudaStreamCreateWithFlags(&p->cap, cudaStreamNonBlocking));
+    // the interior's block list for the whole span the graph steps over, built before capture
+    if ((s = interior_blocks(p, p->ilist_graph, t, t + nsteps * dt))) return s;
     cudaGraph_t graph;
     cudaStream_t user = p->stream;
     p->stream = p->cap;
+    p->ilist_use = &p->ilist_graph;
     cudaError_t eb = cudaStreamBeginCapture(p->cap, cudaStreamCaptureModeThreadLocal);
     int st = TGH_OK;
     p->capturing = true;
     if (eb == cudaSuccess)
       for (int n = 0; n < nsteps && st == TGH_OK; ++n) st = batched_step(p, t + n * dt, dt);
     p->capturing = false;
+    p->ilist_use = nullptr;
     cudaError_t ee = eb == cudaSuccess ? cudaStreamEndCapture(p->cap, &graph) : eb;
     p->stream = user;
     if (st) return st;
@@ -1406,7 +1640,7 @@ int tgh_shard_plan(const tgh_config* cfg, const tgh_mesh* m, const int* owner, i
       for (const auto& e : a->second)
         if (send_pts) {
           send_pts[2 * ns] = e.first;
-          send_pts[2 * ns++ + 1] = e.second;
+          send_pts[2 * ns++ + 1] = dense_index(&p, e.second);
         }
     }
     auto b = mine.req.find({o, phase});
@@ -1415,7 +1649,7 @@ int tgh_shard_plan(const tgh_config* cfg, const tgh_mesh* m, const int* owner, i
       for (const auto& e : b->second)
         if (recv_pts) {
           recv_pts[2 * nr] = e.first;
-          recv_pts[2 * nr++ + 1] = e.second;
+          recv_pts[2 * nr++ + 1] = dense_index(&p, e.second);
         }
     }
   }
@@ -1510,7 +1744,7 @@ int tgh_shard_end(tgh_problem* p, double* u) {
 // events on the problem's stream over nlaunch launches. mode 0: the plain form's kernel
 // (du); mode 1: the batched form's kernel with the stage-2 epilogue. u is filled first.
 int tgh_time_rhs(tgh_problem* p, const double* u, double t, int mode, int nlaunch, double* ms_per_launch) {
-  const size_t L = tgh_state_length(p), Lw = tgh_work_length(p);
+  const size_t L = tgh_state_length(p), Lw = work_doubles(p);
   if (mode == 0 && !p->k) CK(cudaMalloc(&p->k, L * sizeof(double)));
   if (mode == 1 && !p->W1) {
     CK(cudaMalloc(&p->W1, Lw * sizeof(double)));
@@ -1585,7 +1819,7 @@ static int tangent_check(tgh_problem* p, int dir) {
   if (p->mixed) return fail(p, TGH_ERR_ARG, "the tangent-linear form is FP64");
   if (p->intr && (core_follows(p->cs) || p->cfg.interior == TGH_INT_PASTED))
     return fail(p, TGH_ERR_ARG, "the tangent-linear form takes a static :damped or :frozen interior");
-  const size_t L = tgh_state_length(p), Lw = tgh_work_length(p);
+  const size_t L = tgh_state_length(p), Lw = work_doubles(p);
   if (!p->twork) {
     CK(cudaMalloc(&p->twork, Lw * sizeof(double)));
     CK(cudaMemsetAsync(p->twork, 0, Lw * sizeof(double), p->stream));

@@ -163,10 +163,12 @@ struct RhsArgs {
   double* next;           // the next stage's ghosted working array (owned points written)
   double ca, cb;          // next = u0 + ca k ; acc = (stage 1 ? u0 : acc) + cb k ; final: next = acc + cb k
   int stage;              // 1..4
-  int N1, Wd, G;
+  int N1, Wd, G, Wx;      // block edge + 1, ghosted cube edge, ghost width, row pitch
   long npts;              // N1^3 * nblocks
   long p0, p1;            // the points [p0, p1) this launch covers (whole blocks)
   double t;
+  int threads;            // CTA size of the launch (64 or 128)
+  int pi_mb;              // the one-point Pi kernel's resident CTAs per SM (3, 4 or 5)
 };
 
 // Where a finished component goes: straight to du (plain form) or into the RK4 stage
@@ -225,8 +227,8 @@ __device__ __forceinline__ PointIdx point_index(const RhsArgs& A, long p) {
   q.x[0] = __dadd_rn(bl[0], __dmul_rn(bl[4] + (double)q.i, q.h));
   q.x[1] = __dadd_rn(bl[1], __dmul_rn(bl[5] + (double)q.j, q.h));
   q.x[2] = __dadd_rn(bl[2], __dmul_rn(bl[6] + (double)q.k, q.h));
-  const long sv = (long)A.Wd * A.Wd * A.Wd;
-  q.wo = (long)q.b * NV * sv + (q.i + A.G) + (long)A.Wd * ((q.j + A.G) + (long)A.Wd * (q.k + A.G));
+  const long sv = (long)A.Wx * A.Wd * A.Wd;
+  q.wo = (long)q.b * NV * sv + (q.i + A.G) + (long)A.Wx * ((q.j + A.G) + (long)A.Wd * (q.k + A.G));
   return q;
 }
 
@@ -238,6 +240,7 @@ template <int Q, int N1S> __device__ __forceinline__ RhsArgs fixed_geometry(cons
     B.N1 = N1S;
     B.G = Q / 2 + 1;
     B.Wd = N1S + 2 * (Q / 2 + 1);
+    B.Wx = B.Wd + (B.Wd & 1);
   }
   return B;
 }
@@ -260,7 +263,7 @@ __device__ __forceinline__ void rhs_dt(const Case& cs, const RhsArgs& A, const d
                                        const double* x, double inv_h, typename StateT<T>::type hv[NC], T dh0[NC],
                                        T dh1[NC], T dh2[NC], Coef<typename StateT<T>::type>& C, T dth[NC], T& eh) {
   using H = typename StateT<T>::type;
-  const long s1 = 1, s2 = A.Wd, s3 = (long)A.Wd * A.Wd;
+  const long s1 = 1, s2 = A.Wx, s3 = (long)A.Wx * A.Wd;
   const T ih = T(inv_h);
   eh = T(DISS ? dissipation_rate(cs, A.t, x) * inv_h : 0.0);
 #pragma unroll
@@ -373,22 +376,59 @@ __device__ __forceinline__ void rhs_source(const Case& cs, const RhsArgs& A, int
   gh_source<T, true>(C, D, Hl, dHs, g0, T(cs.g2), msrc);
 }
 
-// The head kernel: d_t h at every owned point (emitted in the plain form; in the batched
-// form left in the coefficients for the Pi kernel's stage update), the coefficients and
-// additive source of the Pi components (stored for the Pi kernel), and - with an interior - the
-// branches of gh_rhs_point! (src/evolution.jl:489-695): a frozen core is finished here and
-// never reaches a stencil; a layer point combines w F - rho (u - u_exact) (+ the moving
-// target's rate), the Pi half as w * (stencil part) + coef[CF_M0 + v].
-template <int Q, bool DISS, int MODE, bool INT, int N1S, class T>
-__global__ void __launch_bounds__(128, is_fp32<T>() ? 3 : 1) rhs_head_kernel(const Case cs, const RhsArgs A0) {
-  const RhsArgs A = fixed_geometry<Q, N1S>(A0);
-  const long p = A.p0 + (long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (p >= A.p1) return;
-  const PointIdx q = point_index(A, p);
+// The interior layer's parts that do not depend on the stencils (src/evolution.jl:600-695): for
+// the d_t h half D_v = (1 - w) d_t h_target - rho (h - h_target), for the Pi half
+// T_v = (1 - w) d_t Pi_target - rho (Pi - Pi_target); the point's right-hand side is then
+// w F + D (resp. w F_Pi + T). A resting interior's target is the analytic state at the point;
+// a moving core's (core_follows) adds its rate: d_t g from the dual pass and d_t Pi as the
+// centred difference over t +- cbrt(eps) r_0 (src/initialdata.jl:1721-1729). Evaluated by
+// interior_kernel ahead of the head kernel and parked in the point's own output slots until the
+// stencil part is known.
+static __device__ __noinline__ void layer_targets(const Case& cs, double t, const double* x, const double* wk, long sv,
+                                           double w, double rho, double* dD, long sD, double* dT, long sT) {
+  const double om = 1.0 - w;
+  double he[NC], Pe[NC];
+  if (core_follows(cs)) {
+    double dthe[NC], hx[NC], Pp[NC], Pq[NC];
+    rn_background_state(cs, t, x, he, Pe, dthe);
+    const double dl = layer_rate_step(cs), tp = t + dl, tm = t - dl;
+    rn_background_state(cs, tp, x, hx, Pp);
+    rn_background_state(cs, tm, x, hx, Pq);
+    for (int v = 0; v < NC; ++v) {
+      dD[v * sD] = om * dthe[v] - rho * (wk[v * sv] - he[v]);
+      const double dtP = (Pp[v] - Pq[v]) / (tp - tm);
+      dT[v * sT] = om * dtP - rho * (wk[(NC + v) * sv] - Pe[v]);
+    }
+  } else {
+    rn_background_state(cs, t, x, he, Pe);
+    for (int v = 0; v < NC; ++v) {
+      dD[v * sD] = -(rho * (wk[v * sv] - he[v]));
+      dT[v * sT] = -(rho * (wk[(NC + v) * sv] - Pe[v]));
+    }
+  }
+}
+
+// The interior's points, ahead of the head kernel (gh_rhs_point!'s branches,
+// src/evolution.jl:489-695), over the blocks that can hold a point with r < r_1: a frozen core
+// point's whole right-hand side - zero, or with a moving :damped core (core_follows) the
+// relaxation of the ADM variables towards the core target and its rate (src/interior.jl:420-459,
+// src/initialdata.jl:1784-1796) - and a layer point's target parts D, T (layer_targets), parked
+// where the head and Pi kernels will add the stencil part. Kept out of the head kernel so that
+// its registers serve the main path alone.
+template <int MODE>
+__global__ void __launch_bounds__(128) interior_kernel(const Case cs, const RhsArgs A, const int* __restrict__ blocks) {
   const long S = (long)A.N1 * A.N1 * A.N1;
-  const long sv = (long)A.Wd * A.Wd * A.Wd;
+  const long per = (S + blockDim.x - 1) / blockDim.x;
+  const int b = blocks[blockIdx.x / per];
+  const long ip = (blockIdx.x % per) * blockDim.x + threadIdx.x;
+  if (ip >= S) return;
+  const long p = (long)b * S + ip;
+  if (p < A.p0 || p >= A.p1) return;
+  const PointIdx q = point_index(A, p);
+  const double r = interior_radius(cs, A.t, q.x);
+  if (r >= cs.r1) return;
+  const long sv = (long)A.Wx * A.Wd * A.Wd;
   const double* wk = A.work + q.wo;
-  const double inv_h = 1.0 / q.h;
   double* cfo = A.coef + p;
   EmitDu ed{A.du + (long)q.b * NV * S + q.ip, S};
   EmitStage es{A.acc + (long)q.b * NV * S + q.ip, A.next + q.wo, A.u0 + q.wo, S, sv, A.ca, A.cb, A.stage};
@@ -396,6 +436,73 @@ __global__ void __launch_bounds__(128, is_fp32<T>() ? 3 : 1) rhs_head_kernel(con
     if (MODE == MODE_DU) ed.put(v, val);
     else es.put(v, val);
   };
+  const bool frozen = cs.interior == TGH_INT_PASTED ? r < cs.r1 : r < cs.r0;
+  if (!frozen) {
+    double w, rho;
+    layer_profiles(cs, r, w, rho);
+    if (MODE == MODE_DU)
+      layer_targets(cs, A.t, q.x, wk, sv, w, rho, ed.d, S, ed.d + NC * S, S);
+    else
+      layer_targets(cs, A.t, q.x, wk, sv, w, rho, cfo + CF_DTH0 * A.npts, A.npts, es.nx + NC * sv, sv);
+    return;
+  }
+  if (!core_follows(cs)) {
+    for (int v = 0; v < NV; ++v) put(v, 0.0);
+    return;
+  }
+  const double rc = core_rate(cs), dl = layer_rate_step(cs);
+  double xc[3], hd[NC], Pd[NC];
+  core_position(cs, A.t, q.x, xc);
+  rn_background_state(cs, A.t, xc, hd, Pd);
+  double dthd[NC], dtPd[NC];
+  const double sw = core_rate_weight(cs, r);
+  if (sw == 0.0) {
+    for (int n = 0; n < NC; ++n) dthd[n] = dtPd[n] = 0.0;
+  } else {
+    const double tp = A.t + dl, tm = A.t - dl;
+    double xp[3], xm[3], hp[NC], Pp[NC], hm[NC], Pm[NC];
+    core_position(cs, tp, q.x, xp);
+    core_position(cs, tm, q.x, xm);
+    rn_background_state(cs, tp, xp, hp, Pp);
+    rn_background_state(cs, tm, xm, hm, Pm);
+    const double f = sw / (tp - tm);
+    for (int n = 0; n < NC; ++n) {
+      dthd[n] = f * (hp[n] - hm[n]);
+      dtPd[n] = f * (Pp[n] - Pm[n]);
+    }
+  }
+  double hu[NC], rr[NC];
+  for (int v = 0; v < NC; ++v) hu[v] = wk[v * sv];
+  core_relaxation_rate(hu, hd, rc, dthd, rr);
+  for (int v = 0; v < NC; ++v) {
+    put(v, rr[v]);
+    put(NC + v, dtPd[v] - rc * (wk[(NC + v) * sv] - Pd[v]));
+  }
+}
+
+// The head kernel: d_t h at every owned point (emitted in the plain form; in the batched
+// form left in the coefficients for the Pi kernel's stage update), the coefficients and
+// additive source of the Pi components (stored for the Pi kernel), and - with an interior - the
+// branches of gh_rhs_point! (src/evolution.jl:489-695): a frozen core is finished here and
+// never reaches a stencil (interior_kernel has written its right-hand side); a layer point
+// combines w F - rho (u - u_exact) (+ the moving target's rate), the Pi half as
+// w * (stencil part) + coef[CF_M0 + v]. The layer's target parts are parked by interior_kernel,
+// until they are added, where the point's own results go later: D in du (plain form) or the
+// d_t h coefficient slots (batched form), T in du's Pi half or the next stage's Pi values at the
+// point, both written only by the Pi kernel afterwards.
+template <int Q, bool DISS, int MODE, bool INT, int N1S, class T>
+__global__ void __launch_bounds__(128, is_fp32<T>() ? 3 : 1) rhs_head_kernel(const Case cs, const RhsArgs A0) {
+  const RhsArgs A = fixed_geometry<Q, N1S>(A0);
+  const long p = A.p0 + (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= A.p1) return;
+  const PointIdx q = point_index(A, p);
+  const long S = (long)A.N1 * A.N1 * A.N1;
+  const long sv = (long)A.Wx * A.Wd * A.Wd;
+  const double* wk = A.work + q.wo;
+  const double inv_h = 1.0 / q.h;
+  double* cfo = A.coef + p;
+  EmitDu ed{A.du + (long)q.b * NV * S + q.ip, S};
+  EmitStage es{A.acc + (long)q.b * NV * S + q.ip, A.next + q.wo, A.u0 + q.wo, S, sv, A.ca, A.cb, A.stage};
   // d_t h of an evolved point: stored at once in the plain form; in the batched form parked in
   // the coefficients, and the Pi kernel (more warps to cover the loads) does its stage update
   auto put_dth = [&](int v, double val) {
@@ -404,41 +511,11 @@ __global__ void __launch_bounds__(128, is_fp32<T>() ? 3 : 1) rhs_head_kernel(con
   };
   double w = 1.0, rho = 0.0, r = 0.0;
   if (INT) {
+    // the interior's points were visited first by interior_kernel: a frozen point is finished,
+    // a layer point has its target parts parked
     r = interior_radius(cs, A.t, q.x);
     const bool frozen = cs.interior == TGH_INT_PASTED ? r < cs.r1 : r < cs.r0;
     if (frozen) {
-      if (core_follows(cs)) {
-        const double rc = core_rate(cs), dl = layer_rate_step(cs);
-        double xc[3], hd[NC], Pd[NC];
-        core_position(cs, A.t, q.x, xc);
-        background_state(cs, A.t, xc, hd, Pd);
-        double dthd[NC], dtPd[NC];
-        const double sw = smoothstep(4.0 * r / cs.r0 - 1.0);
-        if (sw == 0.0) {
-          for (int n = 0; n < NC; ++n) dthd[n] = dtPd[n] = 0.0;
-        } else {
-          const double tp = A.t + dl, tm = A.t - dl;
-          double xp[3], xm[3], hp[NC], Pp[NC], hm[NC], Pm[NC];
-          core_position(cs, tp, q.x, xp);
-          core_position(cs, tm, q.x, xm);
-          background_state(cs, tp, xp, hp, Pp);
-          background_state(cs, tm, xm, hm, Pm);
-          const double f = sw / (tp - tm);
-          for (int n = 0; n < NC; ++n) {
-            dthd[n] = f * (hp[n] - hm[n]);
-            dtPd[n] = f * (Pp[n] - Pm[n]);
-          }
-        }
-        double hu[NC], rr[NC];
-        for (int v = 0; v < NC; ++v) hu[v] = wk[v * sv];
-        core_relaxation_rate(hu, hd, rc, dthd, rr);
-        for (int v = 0; v < NC; ++v) {
-          put(v, rr[v]);
-          put(NC + v, dtPd[v] - rc * (wk[(NC + v) * sv] - Pd[v]));
-        }
-      } else {
-        for (int v = 0; v < NV; ++v) put(v, 0.0);
-      }
       cfo[CF_W * A.npts] = -1.0;
       return;
     }
@@ -451,19 +528,15 @@ __global__ void __launch_bounds__(128, is_fp32<T>() ? 3 : 1) rhs_head_kernel(con
   static_assert(sizeof(typename StateT<T>::type) == sizeof(double), "the head kernel's state is FP64");
   rhs_dt<Q, DISS, T>(cs, A, wk, sv, q.x, inv_h, hv, dh0, dh1, dh2, C, dth, eh);
   const bool layer = INT && r < cs.r1;
-  const bool follows = INT && core_follows(cs);
   if (!layer) {
 #pragma unroll
     for (int v = 0; v < NC; ++v) put_dth(v, (double)dth[v]);
-  } else if (follows) {
-    double hm[NC], Pm[NC], dthm[NC];
-    background_state(cs, A.t, q.x, hm, Pm, dthm);
-    const double om = 1.0 - w;
-    for (int v = 0; v < NC; ++v) put_dth(v, w * (double)dth[v] + om * dthm[v] - rho * (wk[v * sv] - hm[v]));
   } else {
-    double he[NC], Pe[NC];
-    background_state(cs, A.t, q.x, he, Pe);
-    for (int v = 0; v < NC; ++v) put_dth(v, w * (double)dth[v] - rho * (wk[v * sv] - he[v]));
+    // w d_t h + D, D parked at the layer's entry in the slot this value replaces
+    const double* dD = MODE == MODE_DU ? ed.d : cfo + CF_DTH0 * A.npts;
+    const long sD = MODE == MODE_DU ? S : A.npts;
+#pragma unroll
+    for (int v = 0; v < NC; ++v) put_dth(v, fma(w, (double)dth[v], dD[v * sD]));
   }
   // the Pi coefficients (and the matter term), then the source, in the form's arithmetic
   const T* dh[3] = {dh0, dh1, dh2};
@@ -485,23 +558,13 @@ __global__ void __launch_bounds__(128, is_fp32<T>() ? 3 : 1) rhs_head_kernel(con
     cfo[CF_W * A.npts] = 1.0;
     return;
   }
-  // the layer's Pi half: w msrc - rho (Pi - Pi_target) (+ (1 - w) d_t Pi_target, moving core)
-  if (follows) {
-    const double dl = layer_rate_step(cs);
-    double hx[NC], Pm[NC], Pp[NC], Pq[NC];
-    background_state(cs, A.t, q.x, hx, Pm);
-    const double tp = A.t + dl, tm = A.t - dl;
-    background_state(cs, tp, q.x, hx, Pp);
-    background_state(cs, tm, q.x, hx, Pq);
-    const double om = 1.0 - w;
-    for (int v = 0; v < NC; ++v) {
-      const double dtP = (Pp[v] - Pq[v]) / (tp - tm);
-      cfo[(CF_M0 + v) * A.npts] = w * msrc[v] + om * dtP - rho * (wk[(NC + v) * sv] - Pm[v]);
-    }
-  } else {
-    double he[NC], Pe[NC];
-    background_state(cs, A.t, q.x, he, Pe);
-    for (int v = 0; v < NC; ++v) cfo[(CF_M0 + v) * A.npts] = w * msrc[v] - rho * (wk[(NC + v) * sv] - Pe[v]);
+  // the layer's Pi half: w msrc + T, T = (1 - w) d_t Pi_target - rho (Pi - Pi_target) parked at
+  // the layer's entry
+  {
+    const double* dT = MODE == MODE_DU ? ed.d + NC * S : es.nx + NC * sv;
+    const long sT = MODE == MODE_DU ? S : sv;
+#pragma unroll
+    for (int v = 0; v < NC; ++v) cfo[(CF_M0 + v) * A.npts] = fma(w, (double)msrc[v], dT[v * sT]);
   }
   cfo[CF_W * A.npts] = w;
 }
@@ -510,8 +573,8 @@ __global__ void __launch_bounds__(128, is_fp32<T>() ? 3 : 1) rhs_head_kernel(con
 // contracted with the head's coefficients, formed, consumed and dropped:
 //   beta^i d_i Pi + (d_i beta^i) Pi + d_i A^{ij} d_j h + A^{ij} d_i d_j h + (eps/h) KO(Pi)
 // then w * that + coef[CF_M0 + v]. Few registers, so many warps hide the load latency.
-template <int Q, bool DISS, int MODE, class T, int N1S>
-__global__ void __launch_bounds__(128, 4) rhs_pi_kernel(const Case cs, const RhsArgs A0) {
+template <int Q, bool DISS, int MODE, class T, int N1S, int MB = 4>
+__global__ void __launch_bounds__(128, MB) rhs_pi_kernel(const Case cs, const RhsArgs A0) {
   const RhsArgs A = fixed_geometry<Q, N1S>(A0);
   const long p = A.p0 + (long)blockIdx.x * blockDim.x + threadIdx.x;
   if (p >= A.p1) return;
@@ -520,8 +583,8 @@ __global__ void __launch_bounds__(128, 4) rhs_pi_kernel(const Case cs, const Rhs
   if (w < 0.0) return;
   const PointIdx q = point_index(A, p);
   const long S = (long)A.N1 * A.N1 * A.N1;
-  const long sv = (long)A.Wd * A.Wd * A.Wd;
-  const long s1 = 1, s2 = A.Wd, s3 = (long)A.Wd * A.Wd;
+  const long sv = (long)A.Wx * A.Wd * A.Wd;
+  const long s1 = 1, s2 = A.Wx, s3 = (long)A.Wx * A.Wd;
   const double* wk = A.work + q.wo;
   const double inv_h = 1.0 / q.h;
   const T ih = T(inv_h), ih2 = T(inv_h * inv_h);

@@ -22,13 +22,20 @@ TGH_DECLARE_RHS_LAUNCH(8, f32)
 
 template <int Q, bool DISS, int MODE, int N1S, class T>
 cudaError_t launch_rhs_n(int part, bool intr, cudaStream_t s, const Case& cs, const RhsArgs& a) {
-  const int TH = 128;
+  const int TH = a.threads == 64 ? 64 : 128;
   const unsigned nb = (unsigned)((a.p1 - a.p0 + TH - 1) / TH);
   if (part == 0) {
     if (intr) rhs_head_kernel<Q, DISS, MODE, true, N1S, T><<<nb, TH, 0, s>>>(cs, a);
     else rhs_head_kernel<Q, DISS, MODE, false, N1S, T><<<nb, TH, 0, s>>>(cs, a);
   } else {
-    rhs_pi_kernel<Q, DISS, MODE, T, N1S><<<nb, TH, 0, s>>>(cs, a);
+    // the FP64 kernels for N = 32 come with three launch bounds (3, 4, 5 resident CTAs per SM)
+    if constexpr (N1S == 33 && !is_fp32<T>()) {
+      if (a.pi_mb == 3) rhs_pi_kernel<Q, DISS, MODE, T, N1S, 3><<<nb, TH, 0, s>>>(cs, a);
+      else if (a.pi_mb == 5) rhs_pi_kernel<Q, DISS, MODE, T, N1S, 5><<<nb, TH, 0, s>>>(cs, a);
+      else rhs_pi_kernel<Q, DISS, MODE, T, N1S><<<nb, TH, 0, s>>>(cs, a);
+    } else {
+      rhs_pi_kernel<Q, DISS, MODE, T, N1S><<<nb, TH, 0, s>>>(cs, a);
+    }
   }
   return cudaGetLastError();
 }

@@ -55,8 +55,8 @@ __global__ void __launch_bounds__(128) rhs_tangent_kernel(const Case cs, const R
   if (p >= A.p1) return;
   const PointIdx q = point_index(A, p);
   const long S = (long)A.N1 * A.N1 * A.N1;
-  const long sv = (long)A.Wd * A.Wd * A.Wd;
-  const long s1 = 1, s2 = A.Wd, s3 = (long)A.Wd * A.Wd;
+  const long sv = (long)A.Wx * A.Wd * A.Wd;
+  const long s1 = 1, s2 = A.Wx, s3 = (long)A.Wx * A.Wd;
   const double* wk = A.work + q.wo;
   const double inv_h = 1.0 / q.h;
   double* du = A.du + (long)q.b * NV * S + q.ip;
@@ -81,7 +81,7 @@ __global__ void __launch_bounds__(128) rhs_tangent_kernel(const Case cs, const R
   Coef<Tan> C;
   rhs_dt<Q, DISS, Tan>(cs, A, wk, sv, q.x, inv_h, hv, dh0, dh1, dh2, C, dth, eh);
   double he[NC], Pe[NC];
-  if (layer) background_state(cs, A.t, q.x, he, Pe);
+  if (layer) rn_background_state(cs, A.t, q.x, he, Pe);
 #pragma unroll 1
   for (int v = 0; v < NC; ++v) put(v, layer ? w * dth[v] - rho * (ld<Tan>(wk + v * sv) - Tan(he[v])) : dth[v]);
   // the Pi coefficients, kept in registers

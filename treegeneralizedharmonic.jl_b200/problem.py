@@ -24,7 +24,7 @@ class GHProblem:
     the forest's fill plan, the ghosted working array, the sampled gauge source and the case's
     constants, on the current CUDA device and stream."""
 
-    def __init__(self, case, forest, q, margin_check=True, precision="fp64", stream=None):
+    def __init__(self, case, forest, q, margin_check=True, precision="fp64", stream=None, tuned=True):
         if not torch.cuda.is_available():
             raise RuntimeError("GHProblem runs on a CUDA device; none is available")
         self.lib = _abi.load_library()
@@ -44,6 +44,12 @@ class GHProblem:
             raise _abi.TGHError(st, msg)
         self.state_length = int(self.lib.tgh_state_length(h))
         self.work_length = int(self.lib.tgh_work_length(h))
+        if tuned:
+            # the kernel variant the autotuner recorded as fastest for this configuration
+            from .autotune import recorded_choice
+            choice = recorded_choice(self)
+            if choice is not None:
+                self.set_variant(**choice)
 
     # ---- lifetime ----
     def close(self):
@@ -79,6 +85,30 @@ class GHProblem:
         """rhs!(du, p, t; matter): the right-hand side of the state prepare left. Raises
         TGHError(TGH_ERR_STALE) when another verb has written the working array since."""
         self._check(self.lib.tgh_rhs(self._h, _ptr(du), float(t), _ptr(matter)))
+
+    # ---- the right-hand side's kernel variants (tgh_set_variant) ----
+    PI_VARIANTS = {"l1": _abi.TGH_PI_L1, "tma": _abi.TGH_PI_TMA}
+
+    def set_variant(self, pi="l1", threads=128, pi_mb=4):
+        """The kernels the right-hand side launches: the Pi half through L1 ("l1") or from tiles
+        staged by the Tensor Memory Accelerator ("tma", q = 4 and N = 32 only), the CTA size of
+        the head and one-point Pi kernels, the one-point Pi kernel's resident CTAs per SM."""
+        self._check(self.lib.tgh_set_variant(self._h, self.PI_VARIANTS[pi], int(threads), int(pi_mb)))
+
+    def variant(self):
+        v, t, m = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+        self._check(self.lib.tgh_get_variant(self._h, ctypes.byref(v), ctypes.byref(t), ctypes.byref(m)))
+        name = {k: n for n, k in self.PI_VARIANTS.items()}[v.value]
+        return {"pi": name, "threads": t.value, "pi_mb": m.value}
+
+    def set_wait_limit(self, polls):
+        """Polls a device-side wait may make before it gives up (negative: at once)."""
+        self._check(self.lib.tgh_set_wait_limit(self._h, int(polls)))
+
+    def device_status(self):
+        """Synchronize and raise TGHError(TGH_ERR_TIMEOUT) if a device wait gave up since the
+        last call."""
+        self._check(self.lib.tgh_device_status(self._h))
 
     def prepare_generation(self):
         """(number of prepare calls, whether the working array still holds the last one)."""
@@ -225,6 +255,21 @@ class GHProblem:
                                                     ctypes.byref(dl2)))
         return l2.value, dl2.value
 
+    def point_physics(self, t, x):
+        """Diagnostics: the case's analytic state (h, Pi: the Dirichlet data through the core rule)
+        and sampled gauge tuple (H_b, d_a H_b) at one point x, evaluated on the device: 40 values."""
+        xs = (ctypes.c_double * 3)(*[float(v) for v in x])
+        out = (ctypes.c_double * 40)()
+        self._check(self.lib.tgh_point_physics(self._h, float(t), xs, out))
+        return list(out)
+
+    def copy_work_blocks(self, b0, nblocks):
+        """Blocks b0 .. b0 + nblocks - 1 of the working array, (N+2G+1)^3 x 20 doubles each."""
+        W = self.forest.N + 2 * (self.q // 2 + 1) + 1
+        w = torch.empty(nblocks * 20 * W ** 3, dtype=torch.float64, device="cuda")
+        self._check(self.lib.tgh_copy_work_blocks(self._h, int(b0), int(nblocks), _ptr(w)))
+        return w
+
     def copy_work(self):
         w = torch.empty(self.work_length, dtype=torch.float64, device="cuda")
         self._check(self.lib.tgh_copy_work(self._h, _ptr(w)))
@@ -234,6 +279,11 @@ class GHProblem:
     def rk4_step(self, u, t, dt):
         """One classical RK4 step, plain form (per stage: fill, RHS, stage update)."""
         self._check(self.lib.tgh_rk4_step(self._h, _ptr(u), float(t), float(dt)))
+
+    def rk4_step_blocks(self, u, t, dt):
+        """The same RK4 step in the plain per-block form: per stage one fill, then one
+        right-hand-side launch and one stage update per block (the reference's block map)."""
+        self._check(self.lib.tgh_rk4_step_blocks(self._h, _ptr(u), float(t), float(dt)))
 
     def step_batched(self, u, t, dt, nsteps):
         """nsteps RK4 steps, batched form: fused stage epilogue, one CUDA graph."""
