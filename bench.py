@@ -456,6 +456,9 @@ def main():
     ap.add_argument("--monitors-only", action="store_true",
                     help="time only the constraint monitors (each with its prepare) on the workload's state: "
                          "the command the monitor profiles are taken with")
+    ap.add_argument("--pi", default="auto", choices=["auto", "l1", "tma"],
+                    help="the Pi kernel: the autotuner's recorded choice (auto), the L1 one-point kernel, or "
+                         "the TMA-staged pair kernel")
     ap.add_argument("--rhs-only", action="store_true",
                     help="time only the right-hand side (head + Pi kernels, stage epilogue) on the workload: "
                          "the command the kernel profiles are taken with")
@@ -481,10 +484,12 @@ def main():
         return run_sharded(args, tgh, world, rank, local, case, forest, cfg, gauge, perturbed)
     stream = torch.cuda.current_stream()
     P = tgh.GHProblem(case, forest, 4, margin_check=False, precision=args.precision)
+    if args.pi != "auto":
+        P.set_variant(pi=args.pi)
     u0 = initial(tgh, P, forest, perturbed)
     if args.rhs_only:
         ms = P.time_rhs(u0, 0.0, mode=1, nlaunch=2)
-        print(json.dumps({"workload": cfg["workload"], "rhs_ms_per_launch": ms,
+        print(json.dumps({"workload": cfg["workload"], "rhs_ms_per_launch": ms, "variant": P.variant(),
                           "points_per_launch": (forest.N + 1) ** 3 * forest.nblocks}))
         P.close()
         return 0
@@ -563,6 +568,8 @@ def main():
         P.close()
         torch.cuda.empty_cache()
         P = tgh.GHProblem(case, forest, 4, margin_check=False, precision=args.precision)
+        if args.pi != "auto":
+            P.set_variant(pi=args.pi)
         u0 = uh.cuda()
     plain = plain_forms(P, u0, dt, K, pts, stream)
 
@@ -571,6 +578,7 @@ def main():
            "vs_baseline": None, "dtype": "f64" if args.precision == "fp64" else "f32 arithmetic, f64 state",
            "data": "synthetic",
            "config": {**cfg, "form": "batched (fused RK4 epilogue, CUDA graph)", "points": pts,
+                      "kernel_variant": P.variant(),
                       "precision": args.precision,
                       "l2_flush": "inputs larger than L2 (working arrays %.0f MB)" % (P.work_length * 8 / 1e6),
                       "parallelism": f"replicas x{world}" if world > 1 else "single GPU"},

@@ -324,6 +324,27 @@ int tgh_tangent_rhs(tgh_problem* p, double* du, double* dut, const double* u, co
 int tgh_tangent_rk4_step(tgh_problem* p, double* u, double* ut, double t, double dt, int direction);
 int tgh_tangent_error_norm(tgh_problem* p, const double* u, const double* ut, double t, double* l2, double* dl2);
 
+/* --- derivatives in reverse mode (the adjoint of the plain form; no counterpart in the reference,
+ * which differentiates nothing) ---
+ * The masked error's gradient with respect to the whole initial state in one backward sweep,
+ * and with respect to the interior layer's rho_max and ramp width and the damping strength
+ * (the directions of the tangent-linear form above):
+ *   tgh_adjoint_error_norm  the masked volume-weighted L2 error of u at t (src/constraints.jl:
+ *                           311-396) and lam = its gradient (device, state layout; zero away from
+ *                           the evolved primary entries)
+ *   tgh_adjoint_rhs         lam_u = (d du / d u)^T lam_du for du = gh_rhs!(u, t); th3 (host,
+ *                           nullable) = lam_du . d du / d(rho_max, ramp, damping strength)
+ *   tgh_adjoint_rk4_step    lam: in, the cotangent of the state after one plain RK4 step of dt
+ *                           from u at t; out, the cotangent of u. The step's stage values are
+ *                           recomputed from u; th3 (host, nullable) is accumulated
+ * A caller checkpoints the states of the forward run and sweeps back (adjoint.py). FP64, one
+ * rank, no matter term, an interior that does not move and is not :pasted, no range projection.
+ * The first adjoint call allocates the adjoint's buffers (20 x 8 doubles of feature cotangents
+ * per working-array point, and six state vectors). */
+int tgh_adjoint_error_norm(tgh_problem* p, const double* u, double t, double* l2, double* lam);
+int tgh_adjoint_rhs(tgh_problem* p, const double* u, double t, const double* lam_du, double* lam_u, double* th3);
+int tgh_adjoint_rk4_step(tgh_problem* p, const double* u, double t, double dt, double* lam, double* th3);
+
 /* --- one rank per GPU (TreeAMR's distribution of a forest's blocks over the ranks of a
  * communicator, src/distributed.jl:1-22; the forest itself is on every rank) ---
  * tgh_partition: the owner rank of every leaf: per refinement level, the level's leaves in

@@ -16,6 +16,9 @@ Public surface, named after the reference's:
   refinement Refinement, level_bounds, refine_flags, indicator_flags: the masked Loehner verdict
   shard      partition, exchange_plan, ShardedGHProblem (one rank per GPU)
   gradient   MaskedErrorStudy, MaskedError: the masked error's gradient by forward-mode tangents
+             or by the reverse sweep
+  adjoint    masked_error_adjoint, MaskedErrorOfState: the reverse sweep with checkpoints
+  autotune   tune, recorded_choice: the right-hand side's kernel variants, timed and recorded
 """
 from . import _abi
 from . import bounds, checkpoint, refinement
@@ -29,12 +32,14 @@ from .initialdata import fourier_modes, perturbation
 from .problem import GHProblem, fp64_peak_tflops
 from .shard import ShardedGHProblem, exchange_plan, partition
 from .gradient import MaskedError, MaskedErrorStudy
+from .adjoint import MaskedErrorOfState, masked_error_adjoint
+from . import autotune
 
 __all__ = ["StateBounds", "check_bounds_gate", "default_bounds", "default_gate", "layer_spacing", "Case", "Forest", "GHProblem", "gauge_wave_case", "gh_forest", "hole_forest", "kerr_schild_case",
            "minkowski_case", "perturbed_minkowski_case", "shifted_minkowski_case", "horizon_min_radius",
            "fourier_modes", "perturbation", "fp64_peak_tflops", "load_library", "ShardedGHProblem",
            "exchange_plan", "partition", "MaskedError", "MaskedErrorStudy", "Refinement", "indicator_flags",
            "level_bounds", "refine_flags", "refinement", "checkpoint", "latest_checkpoint", "load_checkpoint",
-           "save_checkpoint"]
+           "save_checkpoint", "MaskedErrorOfState", "masked_error_adjoint", "autotune"]
 
 load_library = _abi.load_library

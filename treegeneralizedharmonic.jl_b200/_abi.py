@@ -82,6 +82,9 @@ SIGNATURES = {
     "tgh_rk4_step": (ctypes.c_int, [_VP, _VP, _D, _D]),
     "tgh_rk4_step_blocks": (ctypes.c_int, [_VP, _VP, _D, _D]),
     "tgh_set_variant": (ctypes.c_int, [_VP, ctypes.c_int, ctypes.c_int, ctypes.c_int]),
+    "tgh_adjoint_error_norm": (ctypes.c_int, [_VP, _VP, _D, ctypes.POINTER(_D), _VP]),
+    "tgh_adjoint_rhs": (ctypes.c_int, [_VP, _VP, _D, _VP, _VP, ctypes.POINTER(_D)]),
+    "tgh_adjoint_rk4_step": (ctypes.c_int, [_VP, _VP, _D, _D, _VP, ctypes.POINTER(_D)]),
     "tgh_get_variant": (ctypes.c_int, [_VP, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int),
                                        ctypes.POINTER(ctypes.c_int)]),
     "tgh_set_wait_limit": (ctypes.c_int, [_VP, ctypes.c_longlong]),

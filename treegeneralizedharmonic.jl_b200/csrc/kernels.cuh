@@ -57,7 +57,7 @@ __device__ __forceinline__ void point_pos(const double* blk, int b, int i, int j
 
 // stage 0 of the plain form's fill: the scatter of the state vector u into the working
 // array and the copies into ghost points, one warp per run of points along x
-__global__ void fill_copy_kernel(const CopyRun* __restrict__ runs, int nruns, const double* __restrict__ u,
+static __global__ void fill_copy_kernel(const CopyRun* __restrict__ runs, int nruns, const double* __restrict__ u,
                                  double* __restrict__ work, Geo g) {
   const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int lane = threadIdx.x & 31;
@@ -75,7 +75,7 @@ __global__ void fill_copy_kernel(const CopyRun* __restrict__ runs, int nruns, co
 // primary owner, and every owned point held by a block that is not its primary, from the
 // primary's working array (whose owned points the stage update has just written). A
 // primary's own points are not listed: they already hold their value.
-__global__ void fill_points_kernel(const CopyPt* __restrict__ pts, long n, double* __restrict__ work, Geo g) {
+static __global__ void fill_points_kernel(const CopyPt* __restrict__ pts, long n, double* __restrict__ work, Geo g) {
   const long id = (long)blockIdx.x * blockDim.x + threadIdx.x;
   if (id >= n) return;
   const CopyPt c = pts[id];
@@ -90,7 +90,7 @@ __global__ void fill_points_kernel(const CopyPt* __restrict__ pts, long n, doubl
 
 // the Dirichlet hook: the analytic state (through the core rule) at each outer ghost point;
 // with `cache` (stationary cases) the values are also kept, 20 per point
-__global__ void fill_hook_kernel(const HookPt* __restrict__ pts, int n, const double* __restrict__ blk,
+static __global__ void fill_hook_kernel(const HookPt* __restrict__ pts, int n, const double* __restrict__ blk,
                                  double* __restrict__ work, Geo g, const Case cs, double t, double* cache) {
   const int id = blockIdx.x * blockDim.x + threadIdx.x;
   if (id >= n) return;
@@ -111,7 +111,7 @@ __global__ void fill_hook_kernel(const HookPt* __restrict__ pts, int n, const do
 
 // the Dirichlet hook of a stationary case from the values kept by fill_hook_kernel (variable
 // after variable, so that consecutive points read and write consecutive doubles)
-__global__ void hook_copy_kernel(const HookPt* __restrict__ pts, int n, const double* __restrict__ cache,
+static __global__ void hook_copy_kernel(const HookPt* __restrict__ pts, int n, const double* __restrict__ cache,
                                  double* __restrict__ work, Geo g) {
   const int id = blockIdx.x * blockDim.x + threadIdx.x;
   if (id >= n) return;
@@ -191,7 +191,7 @@ template <int P> __device__ __forceinline__ double prolong_value(const double* s
 // The regrid's transfer (the fill's operators between two forests): the value of every owned
 // point of the new forest, copied from the old filled working array or prolonged from it,
 // into a state vector (S points per block and variable)
-__global__ void transfer_copy_kernel(const CopyPt* __restrict__ pts, long n, const double* __restrict__ work,
+static __global__ void transfer_copy_kernel(const CopyPt* __restrict__ pts, long n, const double* __restrict__ work,
                                      Geo g, double* __restrict__ u, long S) {
   const long id = (long)blockIdx.x * blockDim.x + threadIdx.x;
   if (id >= n) return;
@@ -205,7 +205,7 @@ __global__ void transfer_copy_kernel(const CopyPt* __restrict__ pts, long n, con
 // their coarse stencils are neighbours in memory (the lists are grouped by odd-axis mask, so a
 // warp's points do the same amount of work)
 template <int P>
-__global__ void transfer_prolong_kernel(const ProlongPt* __restrict__ pts, int n, const double* __restrict__ work,
+static __global__ void transfer_prolong_kernel(const ProlongPt* __restrict__ pts, int n, const double* __restrict__ work,
                                         Geo g, double* __restrict__ u, long S) {
   const int id = blockIdx.x * blockDim.x + threadIdx.x;
   if (id >= n * NV) return;
@@ -216,7 +216,7 @@ __global__ void transfer_prolong_kernel(const ProlongPt* __restrict__ pts, int n
 }
 
 template <int P>
-__global__ void fill_prolong_kernel(const ProlongPt* __restrict__ pts, int n, double* __restrict__ work, Geo g) {
+static __global__ void fill_prolong_kernel(const ProlongPt* __restrict__ pts, int n, double* __restrict__ work, Geo g) {
   const int id = blockIdx.x * blockDim.x + threadIdx.x;
   if (id >= n * NV) return;
   const int pi = id % n, v = id / n;
@@ -228,7 +228,7 @@ __global__ void fill_prolong_kernel(const ProlongPt* __restrict__ pts, int n, do
 // plain-form RK4 stage updates over the whole state vector (each one fused multiply-add):
 //  kind 0: acc = u + cb k, y = u + ca k   kind 1: acc = acc + cb k, y = u + ca k
 //  kind 2: u = acc + cb k
-__global__ void stage_update_kernel(int kind, long n, const double* __restrict__ k, const double* __restrict__ u0,
+static __global__ void stage_update_kernel(int kind, long n, const double* __restrict__ k, const double* __restrict__ u0,
                                     double* __restrict__ acc, double* __restrict__ y, double* __restrict__ uout,
                                     double ca, double cb) {
   for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) {
@@ -249,7 +249,7 @@ __global__ void stage_update_kernel(int kind, long n, const double* __restrict__
 // The speed lambda = alpha sqrt(tr gamma^{ij}) + |beta| at every evolved owned point and the
 // count of non-finite evolved values; reduced per CTA into scratch[0] (max, as the ordered
 // bits of a non-negative double or a NaN) and scratch[1] (count).
-__global__ void speed_kernel(const double* __restrict__ u, const double* __restrict__ blk, Geo g, long npts,
+static __global__ void speed_kernel(const double* __restrict__ u, const double* __restrict__ blk, Geo g, long npts,
                              const Case cs, double t, unsigned long long* scratch) {
   const long p = (long)blockIdx.x * blockDim.x + threadIdx.x;
   double lam = 0.0;
@@ -290,7 +290,7 @@ __global__ void speed_kernel(const double* __restrict__ u, const double* __restr
 // |u - u_exact| over the evolved primaries of the settled working array: per point the
 // squared magnitude weighted by h^3, the weight and the magnitude; per CTA partial sums in
 // a fixed order into part[3 * blockIdx.x + {0,1,2}] (sum e^2 h^3, sum h^3, max e)
-__global__ void error_kernel(const double* __restrict__ work, const double* __restrict__ blk,
+static __global__ void error_kernel(const double* __restrict__ work, const double* __restrict__ blk,
                              const uint8_t* __restrict__ primary, Geo g, long npts, const Case cs, double t,
                              double* part) {
   __shared__ double sh[3][128];
@@ -337,7 +337,7 @@ __global__ void error_kernel(const double* __restrict__ work, const double* __re
     part[3 * blockIdx.x + 2] = sh[2][0];
   }
 }
-__global__ void error_final_kernel(const double* part, int n, double* out) {
+static __global__ void error_final_kernel(const double* part, int n, double* out) {
   if (threadIdx.x != 0 || blockIdx.x != 0) return;
   double s2 = 0.0, vol = 0.0, mx = 0.0;
   for (int i = 0; i < n; ++i) {
@@ -351,7 +351,7 @@ __global__ void error_final_kernel(const double* part, int n, double* out) {
 
 // the case's state at every owned point (initial_state!); paste_only: only inside r_1 (the
 // :pasted limiter, gh_paste_kernel!)
-__global__ void exact_state_kernel(double* __restrict__ u, const double* __restrict__ blk, Geo g, long npts,
+static __global__ void exact_state_kernel(double* __restrict__ u, const double* __restrict__ blk, Geo g, long npts,
                                    const Case cs, double t, int paste_only) {
   const long p = (long)blockIdx.x * blockDim.x + threadIdx.x;
   if (p >= npts) return;
@@ -369,7 +369,7 @@ __global__ void exact_state_kernel(double* __restrict__ u, const double* __restr
 }
 
 // the sampled gauge source at every owned point, through the core rule (src/gauge.jl:156-170)
-__global__ void sample_gauge_kernel(double* __restrict__ H, const double* __restrict__ blk, Geo g, long npts,
+static __global__ void sample_gauge_kernel(double* __restrict__ H, const double* __restrict__ blk, Geo g, long npts,
                                     const Case cs, double t) {
   const long p = (long)blockIdx.x * blockDim.x + threadIdx.x;
   if (p >= npts) return;
@@ -385,7 +385,7 @@ __global__ void sample_gauge_kernel(double* __restrict__ H, const double* __rest
 }
 
 // owned values of the working array back to the state vector (the batched form's output)
-__global__ void gather_kernel(const double* __restrict__ work, double* __restrict__ u, Geo g, long npts) {
+static __global__ void gather_kernel(const double* __restrict__ work, double* __restrict__ u, Geo g, long npts) {
   const long p = (long)blockIdx.x * blockDim.x + threadIdx.x;
   if (p >= npts) return;
   const int b = (int)(p / g.S);
@@ -398,7 +398,7 @@ __global__ void gather_kernel(const double* __restrict__ work, double* __restric
 }
 
 // the owned points of the first npts / S blocks of a working array from the state vector u
-__global__ void scatter_owned_kernel(const double* __restrict__ u, double* __restrict__ work, Geo g, long npts) {
+static __global__ void scatter_owned_kernel(const double* __restrict__ u, double* __restrict__ work, Geo g, long npts) {
   const long p = (long)blockIdx.x * blockDim.x + threadIdx.x;
   if (p >= npts) return;
   const int b = (int)(p / g.S);
@@ -413,14 +413,14 @@ __global__ void scatter_owned_kernel(const double* __restrict__ u, double* __res
 // The exchange of a sharded fill: the listed (block, work index) points of a working array
 // packed into, or unpacked from, a buffer of 20 values per point (point-major), one thread per
 // value.
-__global__ void pack_kernel(const HookPt* __restrict__ pts, long n, const double* __restrict__ work, Geo g,
+static __global__ void pack_kernel(const HookPt* __restrict__ pts, long n, const double* __restrict__ work, Geo g,
                             double* __restrict__ buf) {
   const long id = (long)blockIdx.x * blockDim.x + threadIdx.x;
   if (id >= n * NV) return;
   const HookPt pt = pts[id / NV];
   buf[id] = work[(long)pt.b * NV * g.Wv + (id % NV) * g.Wv + pt.w];
 }
-__global__ void unpack_kernel(const HookPt* __restrict__ pts, long n, const double* __restrict__ buf,
+static __global__ void unpack_kernel(const HookPt* __restrict__ pts, long n, const double* __restrict__ buf,
                               double* __restrict__ work, Geo g) {
   const long id = (long)blockIdx.x * blockDim.x + threadIdx.x;
   if (id >= n * NV) return;
@@ -431,7 +431,7 @@ __global__ void unpack_kernel(const HookPt* __restrict__ pts, long n, const doub
 // The masked error norm's sums and their tangents over the evolved primaries
 // (src/constraints.jl:311-396): per CTA sum w e^2, sum w e.de and sum w, w = h^3,
 // e = |u - u_exact| over the 20 variables.
-__global__ void error_tangent_kernel(const double* __restrict__ work, const double* __restrict__ twork,
+static __global__ void error_tangent_kernel(const double* __restrict__ work, const double* __restrict__ twork,
                                      const double* __restrict__ blk, const uint8_t* __restrict__ primary, Geo g,
                                      long npts, const Case cs, double t, double* part) {
   __shared__ double sh[3][128];
@@ -480,7 +480,7 @@ __global__ void error_tangent_kernel(const double* __restrict__ work, const doub
 
 // the tangent working array's Dirichlet ghosts: the analytic data do not depend on the
 // parameters or the initial perturbation, so their tangent is zero
-__global__ void hook_zero_kernel(const HookPt* __restrict__ pts, int n, double* __restrict__ work, Geo g) {
+static __global__ void hook_zero_kernel(const HookPt* __restrict__ pts, int n, double* __restrict__ work, Geo g) {
   const long id = (long)blockIdx.x * blockDim.x + threadIdx.x;
   if (id >= (long)n * NV) return;
   const HookPt p = pts[id / NV];
@@ -488,13 +488,13 @@ __global__ void hook_zero_kernel(const HookPt* __restrict__ pts, int n, double* 
 }
 
 // one point's analytic state (20) and gauge tuple (20), for diagnostics
-__global__ void point_physics_kernel(const Case cs, double t, const double* x, double* out) {
+static __global__ void point_physics_kernel(const Case cs, double t, const double* x, double* out) {
   exact_state(cs, t, x, out);
   gauge_tuple(cs, t, x, out + NV);
 }
 
 // sustained FP64 fused multiply-add throughput probe: 8 independent chains per thread
-__global__ void fp64_probe_kernel(double* out, int iters, double a, double b) {
+static __global__ void fp64_probe_kernel(double* out, int iters, double a, double b) {
   double x0 = threadIdx.x * 1e-9, x1 = x0 + 1e-9, x2 = x0 + 2e-9, x3 = x0 + 3e-9;
   double x4 = x0 + 4e-9, x5 = x0 + 5e-9, x6 = x0 + 6e-9, x7 = x0 + 7e-9;
   for (int i = 0; i < iters; ++i) {

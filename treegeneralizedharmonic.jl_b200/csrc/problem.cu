@@ -18,6 +18,7 @@
 #include "monitors.cuh"
 #include "rhs_inst.cuh"
 #include "rhs_pi_tma.cuh"
+#include "adjoint.cuh"
 #include "tangent_rhs.cuh"
 
 using namespace tgh;
@@ -112,6 +113,10 @@ struct tgh_problem {
   double *W1 = nullptr, *W2 = nullptr, *bacc = nullptr;
   // tangent-linear buffers: the tangent working array, and the plain form's k, acc, y tangents
   double *twork = nullptr, *kt = nullptr, *acct = nullptr, *yt = nullptr;
+  // adjoint buffers: the feature cotangents, mu on the working array, the parameters' partials,
+  // the recomputed stage states and two state-sized accumulators
+  double *adj_cot = nullptr, *adj_mu = nullptr, *adj_part = nullptr;
+  double *adj_y[3] = {nullptr, nullptr, nullptr}, *adj_a = nullptr, *adj_acc = nullptr, *adj_m = nullptr;
   cudaGraphExec_t gexec = nullptr;
   GraphKey gkey{0, 0, 0};
   long graph_kernels = 0;  // kernel nodes of the captured graph
@@ -931,7 +936,9 @@ void tgh_problem_destroy(tgh_problem* p) {
   void* bufs[] = {p->work, p->Hsrc, p->blk, p->primary, p->runs, p->gpts, p->hooks, p->hook_cache, p->scratch,
                   p->bcounts, p->dev_err, p->ilist.dev, p->ilist_graph.dev,
                   p->part, p->coef, p->diag, p->dpart, p->ind, p->ind_tol, p->ind_counts, p->ind_boxes,
-                  p->k, p->acc, p->y, p->u0, p->W1, p->W2, p->bacc, p->twork, p->kt, p->acct, p->yt};
+                  p->k, p->acc, p->y, p->u0, p->W1, p->W2, p->bacc, p->twork, p->kt, p->acct, p->yt,
+                  p->adj_cot, p->adj_mu, p->adj_part, p->adj_y[0], p->adj_y[1], p->adj_y[2], p->adj_a,
+                  p->adj_acc, p->adj_m};
   for (void* b : bufs)
     if (b) cudaFree(b);
   for (auto* pp : p->prol)
@@ -1908,6 +1915,133 @@ int tgh_tangent_error_norm(tgh_problem* p, const double* u, const double* ut, do
   if (!(w > 0.0)) return fail(p, TGH_ERR_ARG, "no evolved point to measure the error on");
   *l2 = std::sqrt(a / w);
   *dl2 = *l2 > 0.0 ? (b / w) / *l2 : 0.0;
+  return TGH_OK;
+}
+
+// ---- the adjoint (reverse mode) of the plain form: the right-hand side, one RK4 step and the
+// masked error, for gradients with respect to the whole initial state in one reverse sweep ----
+
+static int adjoint_check(tgh_problem* p) {
+  if (p->nranks > 1) return fail(p, TGH_ERR_ARG, "the adjoint form runs on one rank");
+  if (p->mixed) return fail(p, TGH_ERR_ARG, "the adjoint form is FP64");
+  if (p->intr && (core_follows(p->cs) || p->cfg.interior == TGH_INT_PASTED))
+    return fail(p, TGH_ERR_ARG, "the adjoint form takes a static :damped or :frozen interior");
+  if (p->has_bounds) return fail(p, TGH_ERR_ARG, "the adjoint form does not differentiate the range projection");
+  const size_t L = tgh_state_length(p);
+  if (!p->adj_cot) {
+    const size_t cs = (size_t)p->Wv * p->nb;
+    CK(cudaMalloc(&p->adj_cot, (size_t)NC * ADJ_NF * cs * sizeof(double)));
+    CK(cudaMemsetAsync(p->adj_cot, 0, (size_t)NC * ADJ_NF * cs * sizeof(double), p->stream));
+    CK(cudaMalloc(&p->adj_mu, work_doubles(p) * sizeof(double)));
+    CK(cudaMalloc(&p->adj_part, 3 * (size_t)p->npart * sizeof(double)));
+    for (int i = 0; i < 3; ++i) CK(cudaMalloc(&p->adj_y[i], L * sizeof(double)));
+    CK(cudaMalloc(&p->adj_a, L * sizeof(double)));
+    CK(cudaMalloc(&p->adj_acc, L * sizeof(double)));
+    CK(cudaMalloc(&p->adj_m, L * sizeof(double)));
+  }
+  if (!p->k) CK(cudaMalloc(&p->k, L * sizeof(double)));
+  return TGH_OK;
+}
+
+// mu_u = (d gh_rhs!(y, t) / d y)^T a; th3 (host, nullable) += a . d gh_rhs! / d(rho_max, ramp, damping)
+static int vjp_rhs(tgh_problem* p, const double* y, double t, const double* a, double* mu_u, double* th3) {
+  int s = prepare_impl(p, y, t, "the adjoint form");
+  if (s) return s;
+  RhsArgs ra = base_args(p, p->work, t);
+  const long cstride = (long)p->Wv * p->nb;
+  AdjArgs J{a, p->adj_cot, cstride, p->adj_part};
+  CK(launch_adjoint_point(p->q, p->diss, p->intr, p->stream, p->cs, ra, J));
+  CK(launch_adjoint_gather(p->q, p->diss, p->stream, p->adj_cot, cstride, p->geo, p->nb, p->adj_mu));
+  for (int l = p->maxlevel; l >= 1; --l) {
+    if (!p->nprol[l]) continue;
+    const unsigned g = grid_for((long)p->nprol[l] * NV, 256);
+    switch (p->q + 2) {
+      case 4: prolong_adjoint_kernel<4><<<g, 256, 0, p->stream>>>(p->prol[l], p->nprol[l], p->adj_mu, p->geo); break;
+      case 6: prolong_adjoint_kernel<6><<<g, 256, 0, p->stream>>>(p->prol[l], p->nprol[l], p->adj_mu, p->geo); break;
+      case 8: prolong_adjoint_kernel<8><<<g, 256, 0, p->stream>>>(p->prol[l], p->nprol[l], p->adj_mu, p->geo); break;
+      default: prolong_adjoint_kernel<10><<<g, 256, 0, p->stream>>>(p->prol[l], p->nprol[l], p->adj_mu, p->geo); break;
+    }
+    CK(cudaGetLastError());
+  }
+  CK(cudaMemsetAsync(mu_u, 0, tgh_state_length(p) * sizeof(double), p->stream));
+  if (p->nruns) {
+    copy_adjoint_kernel<<<grid_for((long)p->nruns * 32, 256), 256, 0, p->stream>>>(p->runs, p->nruns, p->adj_mu, mu_u,
+                                                                                    p->geo);
+    CK(cudaGetLastError());
+  }
+  if (th3) {
+    std::vector<double> h(3 * (size_t)p->npart);
+    CK(cudaMemcpyAsync(h.data(), p->adj_part, h.size() * sizeof(double), cudaMemcpyDeviceToHost, p->stream));
+    CK(cudaStreamSynchronize(p->stream));
+    for (int i = 0; i < p->npart; ++i)  // in block order, on the host
+      for (int k = 0; k < 3; ++k) th3[k] += h[3 * i + k];
+  }
+  return TGH_OK;
+}
+
+int tgh_adjoint_rhs(tgh_problem* p, const double* u, double t, const double* lam_du, double* lam_u, double* th3) {
+  int s = adjoint_check(p);
+  if (s) return s;
+  if (th3) th3[0] = th3[1] = th3[2] = 0.0;
+  return vjp_rhs(p, u, t, lam_du, lam_u, th3);
+}
+
+int tgh_adjoint_rk4_step(tgh_problem* p, const double* u, double t, double dt, double* lam, double* th3) {
+  int s = adjoint_check(p);
+  if (s) return s;
+  const long L = (long)tgh_state_length(p);
+  const unsigned g = 148 * 8;
+  const double a12 = 0.5 * dt, b16 = dt / 6.0, b13 = dt / 3.0;
+  const double tm = t + 0.5 * dt, te = t + dt;
+  double **y = p->adj_y, *a = p->adj_a, *acc = p->adj_acc, *m = p->adj_m;
+  // the step's stage values, recomputed (the plain form's: y1 = u + dt/2 k1, y2 = u + dt/2 k2,
+  // y3 = u + dt k3; the limiters do nothing on the problems the adjoint accepts)
+  if ((s = tgh_gh_rhs(p, p->k, u, t, nullptr))) return s;
+  axpby_kernel<<<g, 256, 0, p->stream>>>(L, 1.0, u, a12, p->k, y[0]);
+  if ((s = tgh_gh_rhs(p, p->k, y[0], tm, nullptr))) return s;
+  axpby_kernel<<<g, 256, 0, p->stream>>>(L, 1.0, u, a12, p->k, y[1]);
+  if ((s = tgh_gh_rhs(p, p->k, y[1], tm, nullptr))) return s;
+  axpby_kernel<<<g, 256, 0, p->stream>>>(L, 1.0, u, dt, p->k, y[2]);
+  CK(cudaGetLastError());
+  // backwards: u_{n+1} = u + dt/6 k1 + dt/3 k2 + dt/3 k3 + dt/6 k4, k_s = F(y_{s-1})
+  CK(cudaMemcpyAsync(acc, lam, L * sizeof(double), cudaMemcpyDeviceToDevice, p->stream));
+  axpby_kernel<<<g, 256, 0, p->stream>>>(L, b16, lam, 0.0, lam, a);
+  if ((s = vjp_rhs(p, y[2], te, a, m, th3))) return s;  // k4
+  axpy_kernel<<<g, 256, 0, p->stream>>>(L, 1.0, m, acc);
+  axpby_kernel<<<g, 256, 0, p->stream>>>(L, b13, lam, dt, m, a);
+  if ((s = vjp_rhs(p, y[1], tm, a, m, th3))) return s;  // k3
+  axpy_kernel<<<g, 256, 0, p->stream>>>(L, 1.0, m, acc);
+  axpby_kernel<<<g, 256, 0, p->stream>>>(L, b13, lam, a12, m, a);
+  if ((s = vjp_rhs(p, y[0], tm, a, m, th3))) return s;  // k2
+  axpy_kernel<<<g, 256, 0, p->stream>>>(L, 1.0, m, acc);
+  axpby_kernel<<<g, 256, 0, p->stream>>>(L, b16, lam, a12, m, a);
+  if ((s = vjp_rhs(p, u, t, a, m, th3))) return s;  // k1
+  axpy_kernel<<<g, 256, 0, p->stream>>>(L, 1.0, m, acc);
+  CK(cudaGetLastError());
+  CK(cudaMemcpyAsync(lam, acc, L * sizeof(double), cudaMemcpyDeviceToDevice, p->stream));
+  return TGH_OK;
+}
+
+int tgh_adjoint_error_norm(tgh_problem* p, const double* u, double t, double* l2, double* lam) {
+  int s = adjoint_check(p);
+  if (s) return s;
+  if ((s = prepare_impl(p, u, t, "the adjoint form"))) return s;
+  error_kernel<<<p->npart, 128, 0, p->stream>>>(p->work, p->blk, p->primary, p->geo, p->npts, p->cs, t, p->part);
+  CK(cudaGetLastError());
+  std::vector<double> h(3 * (size_t)p->npart);
+  CK(cudaMemcpyAsync(h.data(), p->part, h.size() * sizeof(double), cudaMemcpyDeviceToHost, p->stream));
+  CK(cudaStreamSynchronize(p->stream));
+  double a = 0.0, w = 0.0;
+  for (int i = 0; i < p->npart; ++i) {
+    a += h[3 * i];
+    w += h[3 * i + 1];
+  }
+  if (!(w > 0.0)) return fail(p, TGH_ERR_ARG, "no evolved point to measure the error on");
+  *l2 = std::sqrt(a / w);
+  const double scale = *l2 > 0.0 ? 1.0 / (*l2 * w) : 0.0;
+  error_adjoint_kernel<<<grid_for(p->npts, 128), 128, 0, p->stream>>>(u, p->blk, p->primary, p->geo, p->npts, p->cs,
+                                                                       t, scale, lam);
+  CK(cudaGetLastError());
   return TGH_OK;
 }
 

@@ -7,10 +7,13 @@
 // computed and dropped). 12 warps per CTA: 3 per SM sub-partition leave 168 registers a thread,
 // enough for two points' coefficients without spilling. For each component v in turn, one thread
 // issues two tiled tensor copies of the block's working array into shared memory:
-//   h_v   x -2..41, the tile's rows and planes widened by SR = 2 (44 x 15 x 6 doubles)
-//   Pi_v  x -2..41, widened by KR = 3 for the dissipation      (44 x 17 x 8 doubles)
+//   h_v   x -2..47, the tile's rows and planes widened by SR = 2 (50 x 15 x 6 doubles)
+//   Pi_v  x -2..47, widened by KR = 3 for the dissipation      (50 x 17 x 8 doubles)
 // completing on an mbarrier; two such stages alternate, so that the copies of component v + 1
-// run while component v is computed. Each thread computes two neighbouring points along x,
+// run while component v is computed. The boxes are 50 doubles wide (the rows used are 44): a
+// row pitch of 25 sixteen-byte units, 1 modulo the 8 bank groups of a 128-byte shared-memory
+// wavefront, keeps the 16-byte loads of a warp whose lanes cross from one row to the next free
+// of bank conflicts. Each thread computes two neighbouring points along x,
 // (i0, i0 + 1) with i0 = -1, 1, ..., 31, from 16-byte shared-memory loads: one load serves
 // both points of every y and z tap and two x taps, so a point costs about 34 shared loads per
 // component against the 80 global loads of the one-point kernel. The point i = -1 of the first
@@ -33,7 +36,7 @@ namespace tgh {
 namespace pitma {
 constexpr int N1 = 33, G = 3, SR = 2, KR = 3;  // q = 4, N = 32
 constexpr int TY = 11, TZ = 2, NPAIR = 17;
-constexpr int XB = 44;                                   // box width: x = -2 .. 41
+constexpr int XB = 50;                                   // box width: x = -2 .. 47 (see below)
 constexpr int HY = TY + 2 * SR, HZ = TZ + 2 * SR;          // 15, 7
 constexpr int PY = TY + 2 * KR, PZ = TZ + 2 * KR;        // 17, 9
 constexpr int HN = XB * HY * HZ, PN = XB * PY * PZ;      // doubles per box
@@ -192,13 +195,16 @@ __global__ void __launch_bounds__(pitma::THREADS)
         }
       }
     }
-    // every thread waits (bounded) for the stage; the CTA goes on only if all of them saw it
+    // every thread waits (bounded) for the stage; the CTA goes on only if all of them saw it.
+    // The vote is also the barrier after component v - 1: its stage may now be refilled with
+    // component v + 1, which lands while v is computed.
     const bool got = mbar_wait(st ? bar1 : bar0, (v >> 1) & 1, stat.limit);
     if (!__syncthreads_and(got)) {
       ok = false;
       failed_at = v;
       break;
     }
+    if (tid == 0 && v >= 1 && v + 1 < NC) pitma_issue(M, base, st ? bar0 : bar1, st ^ 1, b, v + 1, y0, z0);
     const double* H = smd + (st * STAGE + HOFF) / 8;
     const double* P = smd + (st * STAGE + POFF) / 8;
     double s[2], p2[2];
@@ -367,8 +373,6 @@ __global__ void __launch_bounds__(pitma::THREADS)
         if (DISS) s[e] = fma(c[CF_EH], kox[e] + koy[e] + koz[e], s[e]);
       }
     }
-    __syncthreads();  // every thread is done with stage st: it may be refilled
-    if (tid == 0 && v + 2 < NC) pitma_issue(M, base, st ? bar1 : bar0, st, b, v + 2, y0, z0);
     if (active) {
 #pragma unroll
       for (int e = 0; e < 2; ++e) {
@@ -393,11 +397,12 @@ __global__ void __launch_bounds__(pitma::THREADS)
     }
   }
   if (!ok) {
-    // a wait gave up: record it, let the copies already issued (components failed_at and
-    // failed_at + 1) land, bounded, then leave without writing
+    // a wait gave up: record it, let the copies already issued (component failed_at, and
+    // component 1 when it was the first) land, bounded, then leave without writing
     if (tid == 0) atomicExch(stat.err, TGH_ERR_TIMEOUT);
     const long long drain = 1ll << 24;
-    for (int v = failed_at; v < failed_at + 2 && v < NC; ++v) mbar_wait(v & 1 ? bar1 : bar0, (v >> 1) & 1, drain);
+    const int last = failed_at == 0 ? 1 : failed_at;
+    for (int v = failed_at; v <= last; ++v) mbar_wait(v & 1 ? bar1 : bar0, (v >> 1) & 1, drain);
   }
 }
 

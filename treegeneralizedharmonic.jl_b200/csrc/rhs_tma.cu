@@ -9,7 +9,7 @@
 namespace tgh {
 
 // The working array of nwb blocks viewed as a 4-d tensor (x: Wx = 40 with 39 used, y: 39,
-// z: 39, block x 20 + variable), with the h box (44, 15, 6, 1) and the Pi box (44, 17, 8, 1).
+// z: 39, block x 20 + variable), with the h box (50, 15, 6, 1) and the Pi box (50, 17, 8, 1).
 // Rows are 320 bytes apart (a multiple of 16, as the copies need); a box starting at x = -2
 // reads zeros left of the array and beyond x = 39 (the pad column, also zero).
 bool make_pi_tma_maps(double* work, int nwb, PiTmaMaps* out, std::string& err) {

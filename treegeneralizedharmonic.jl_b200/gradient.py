@@ -10,10 +10,15 @@ the plain FP64 form from the analytic data plus seeded perturbation modes. Its p
                      has none, so the loss does not depend on it and its derivative is 0
     a0 .. a7         the amplitudes of the 8 seeded perturbation modes
 
-The derivatives are exact (to roundoff) forward-mode tangents: one tangent-linear run of the
-step per parameter (tgh_tangent_rk4_step), which needs no checkpoints because the tangent is
-carried along with the state. `MaskedError` wraps the loss and its gradient as a
-torch.autograd.Function.
+Two ways to the same derivatives (exact to roundoff):
+  gradient          forward-mode tangents, one tangent-linear run of the step per parameter
+                    (tgh_tangent_rk4_step); no checkpoints, the tangent travels with the state
+  gradient_adjoint  one reverse sweep of the adjoint step (tgh_adjoint_rk4_step, adjoint.py)
+                    with checkpointed recomputation: the gradient with respect to the whole
+                    initial state at once, the modes' amplitudes read off it, the layer's and
+                    damping's parameters accumulated along the sweep
+`MaskedError` wraps the loss and its gradient as a torch.autograd.Function (method "tangent" or
+"adjoint"); adjoint.MaskedErrorOfState differentiates with respect to the initial state itself.
 """
 import numpy as np
 import torch
@@ -88,6 +93,20 @@ class MaskedErrorStudy:
             grad[i] = dl2
         return loss, grad
 
+    def gradient_adjoint(self, params, every=8):
+        """(loss, d loss / d params, d loss / d u0) from one reverse sweep (adjoint.py) with a
+        checkpoint every `every` steps: the parameters' part accumulated along the sweep, the
+        amplitudes' as the state gradient against each mode."""
+        from .adjoint import masked_error_adjoint
+        P = self.problem(params)
+        u0 = self.initial(P, params)
+        loss, lam, th = masked_error_adjoint(P, u0, 0.0, self.dt, self.nsteps, every)
+        grad = np.zeros(len(NAMES))
+        grad[0:3] = th
+        for m in range(8):
+            grad[4 + m] = float(torch.dot(lam, self.modes[m]))
+        return loss, grad, lam
+
     def finite_differences(self, params, rel=1e-3, i=None):
         """Central differences of the loss, step rel * |p| (rel for a zero parameter)."""
         idx = range(len(NAMES)) if i is None else [i]
@@ -108,16 +127,19 @@ class MaskedError(torch.autograd.Function):
     parameters (NAMES order), differentiable through the forward-mode tangents."""
 
     @staticmethod
-    def forward(ctx, params, study):
+    def forward(ctx, params, study, method="tangent"):
         p = params.detach().cpu().numpy()
-        loss, grad = study.gradient(p)
+        if method == "adjoint":
+            loss, grad, _ = study.gradient_adjoint(p)
+        else:
+            loss, grad = study.gradient(p)
         ctx.save_for_backward(torch.as_tensor(grad, dtype=params.dtype, device=params.device))
         return torch.as_tensor(loss, dtype=params.dtype, device=params.device)
 
     @staticmethod
     def backward(ctx, g):
         (grad,) = ctx.saved_tensors
-        return g * grad, None
+        return g * grad, None, None
 
 
 def nominal_params(dtype=torch.float64):

@@ -255,6 +255,30 @@ class GHProblem:
                                                     ctypes.byref(dl2)))
         return l2.value, dl2.value
 
+    # ---- reverse mode (tgh_adjoint_*) ----
+    def adjoint_error_norm(self, u, t):
+        """(the masked L2 error of u at t, its gradient with respect to u as a state vector)."""
+        lam = torch.zeros_like(u)
+        l2 = ctypes.c_double()
+        self._check(self.lib.tgh_adjoint_error_norm(self._h, _ptr(u), float(t), ctypes.byref(l2), _ptr(lam)))
+        return l2.value, lam
+
+    def adjoint_rhs(self, u, t, lam_du):
+        """((d du/d u)^T lam_du, lam_du . d du/d(rho_max, ramp, damping strength)) for du = gh_rhs!(u, t)."""
+        lam_u = torch.empty_like(u)
+        th = (ctypes.c_double * 3)()
+        self._check(self.lib.tgh_adjoint_rhs(self._h, _ptr(u), float(t), _ptr(lam_du), _ptr(lam_u), th))
+        return lam_u, list(th)
+
+    def adjoint_rk4_step(self, u, t, dt, lam, th=None):
+        """lam (in place): the cotangent of the state after one plain RK4 step of dt from u at t
+        becomes the cotangent of u; th (a list of 3, accumulated) the parameters' cotangents."""
+        acc = (ctypes.c_double * 3)(*(th if th is not None else [0.0, 0.0, 0.0]))
+        self._check(self.lib.tgh_adjoint_rk4_step(self._h, _ptr(u), float(t), float(dt), _ptr(lam), acc))
+        if th is not None:
+            th[:] = list(acc)
+        return lam
+
     def point_physics(self, t, x):
         """Diagnostics: the case's analytic state (h, Pi: the Dirichlet data through the core rule)
         and sampled gauge tuple (H_b, d_a H_b) at one point x, evaluated on the device: 40 values."""
