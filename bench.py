@@ -459,6 +459,9 @@ def main():
     ap.add_argument("--pi", default="auto", choices=["auto", "l1", "tma"],
                     help="the Pi kernel: the autotuner's recorded choice (auto), the L1 one-point kernel, or "
                          "the TMA-staged pair kernel")
+    ap.add_argument("--step-only", action="store_true",
+                    help="time only the batched step (the graph of K steps) on the workload: the command the "
+                         "launch lists are taken with")
     ap.add_argument("--rhs-only", action="store_true",
                     help="time only the right-hand side (head + Pi kernels, stage epilogue) on the workload: "
                          "the command the kernel profiles are taken with")
@@ -535,6 +538,11 @@ def main():
         raise SystemExit("the evolved state is not finite")
     pts = forest.points()
     value = world * pts * K / (ms * 1e-3)
+    if args.step_only:
+        print(json.dumps({"workload": cfg["workload"], "value": value, "unit": "point-updates/s", "ms_per_step": ms / K,
+                          "steps": K, "variant": P.variant(), "gpu_launches": launches, "clocks": ck}))
+        P.close()
+        return 0
 
     # the dominant kernel alone: the right-hand side with the fused RK4 epilogue
     rhs_ms = P.time_rhs(u0, 0.0, mode=1, nlaunch=max(4, K))
