@@ -145,6 +145,11 @@ struct tgh_problem {
     double lo = 0, hi = -1;
   } ilist, ilist_graph;
   const BlockList* ilist_use = nullptr;
+  // the batched form's side branch: the interior kernel runs beside the hook and the
+  // prolongation (it reads owned points only, which those write none of)
+  cudaStream_t side = nullptr;
+  cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
+  bool interior_done = false;  // the stage's interior kernel ran on the side branch
   long long wait_limit = 1ll << 26;       // polls a device wait may make
 };
 
@@ -636,23 +641,29 @@ static int interior_blocks(tgh_problem* p, tgh_problem::BlockList& L, double tlo
 
 // One right-hand side over all blocks on the problem's stream: the interior's points (a problem
 // with an interior, over the blocks of the list in use), the head kernel, then the Pi kernel.
+static int launch_interior(tgh_problem* p, const RhsArgs& a, int mode, cudaStream_t s) {
+  const tgh_problem::BlockList* L = p->ilist_use;
+  if (!L) {
+    // a direct launch: the list for this t
+    int st = interior_blocks(p, p->ilist, a.t, a.t);
+    if (st) return st;
+    L = &p->ilist;
+  }
+  if (L->n > 0) {
+    const long per = (p->S + 127) / 128;
+    if (mode == MODE_DU)
+      interior_kernel<MODE_DU><<<(unsigned)(L->n * per), 128, 0, s>>>(p->cs, a, L->dev);
+    else
+      interior_kernel<MODE_STAGE><<<(unsigned)(L->n * per), 128, 0, s>>>(p->cs, a, L->dev);
+    CK(cudaGetLastError());
+  }
+  return TGH_OK;
+}
+
 static int launch_rhs(tgh_problem* p, const RhsArgs& a, int mode) {
-  if (p->intr) {
-    const tgh_problem::BlockList* L = p->ilist_use;
-    if (!L) {
-      // a direct launch: the list for this t
-      int s = interior_blocks(p, p->ilist, a.t, a.t);
-      if (s) return s;
-      L = &p->ilist;
-    }
-    if (L->n > 0) {
-      const long per = (p->S + 127) / 128;
-      if (mode == MODE_DU)
-        interior_kernel<MODE_DU><<<(unsigned)(L->n * per), 128, 0, p->stream>>>(p->cs, a, L->dev);
-      else
-        interior_kernel<MODE_STAGE><<<(unsigned)(L->n * per), 128, 0, p->stream>>>(p->cs, a, L->dev);
-      CK(cudaGetLastError());
-    }
+  if (p->intr && !p->interior_done) {
+    int s = launch_interior(p, a, mode, p->stream);
+    if (s) return s;
   }
   CK(launch_part(p, 0, mode, p->stream, a));
   if (pi_tma_applies(p, a)) {
@@ -929,6 +940,9 @@ void tgh_problem_destroy(tgh_problem* p) {
   if (!p) return;
   if (p->gexec) cudaGraphExecDestroy(p->gexec);
   if (p->cap) cudaStreamDestroy(p->cap);
+  if (p->side) cudaStreamDestroy(p->side);
+  if (p->ev_fork) cudaEventDestroy(p->ev_fork);
+  if (p->ev_join) cudaEventDestroy(p->ev_join);
   for (auto& x : p->xch) {
     if (x.send) cudaFree(x.send);
     if (x.recv) cudaFree(x.recv);
@@ -1468,7 +1482,7 @@ static StagePlan stage_plan(tgh_problem* p, int st, double t, double dt) {
   return StagePlan{ts[st], ca[st], cb[st], rd[st], wr[st]};
 }
 
-static int stage_rhs(tgh_problem* p, const StagePlan& sp, int st) {
+static RhsArgs stage_args(tgh_problem* p, const StagePlan& sp, int st) {
   RhsArgs a = base_args(p, sp.rd, sp.ts);
   a.u0 = p->work;
   a.acc = p->bacc;
@@ -1476,15 +1490,43 @@ static int stage_rhs(tgh_problem* p, const StagePlan& sp, int st) {
   a.ca = sp.ca;
   a.cb = sp.cb;
   a.stage = st + 1;
-  return launch_rhs(p, a, MODE_STAGE);
+  return a;
 }
 
+static int stage_rhs(tgh_problem* p, const StagePlan& sp, int st) { return launch_rhs(p, stage_args(p, sp, st), MODE_STAGE); }
+
+// One batched step: per stage the copies, then the interior kernel on a side branch beside the
+// Dirichlet hook and the prolongation (it reads owned points only, which the copies have just
+// made current and those two do not write), joined before the head and Pi kernels.
 static int batched_step(tgh_problem* p, double t, double dt) {
   int s;
+  const bool branch = p->intr && p->side;
   for (int st = 0; st < 4; ++st) {
     const StagePlan sp = stage_plan(p, st, t, dt);
-    if ((s = launch_fill(p, sp.rd, true, sp.rd, sp.ts))) return s;
-    if ((s = stage_rhs(p, sp, st))) return s;
+    if (!branch) {
+      if ((s = launch_fill(p, sp.rd, true, sp.rd, sp.ts))) return s;
+      if ((s = stage_rhs(p, sp, st))) return s;
+      continue;
+    }
+    if (p->ngpts) {
+      fill_points_kernel<<<grid_for(p->ngpts, 256), 256, 0, p->stream>>>(p->gpts, p->ngpts, sp.rd, p->geo);
+      CK(cudaGetLastError());
+    }
+    const RhsArgs a = stage_args(p, sp, st);
+    CK(cudaEventRecord(p->ev_fork, p->stream));
+    CK(cudaStreamWaitEvent(p->side, p->ev_fork, 0));
+    if ((s = launch_interior(p, a, MODE_STAGE, p->side))) return s;
+    CK(cudaEventRecord(p->ev_join, p->side));
+    if ((s = launch_hooks(p, sp.rd, sp.ts))) return s;
+    for (int l = 1; l <= p->maxlevel; ++l) {
+      if (!p->nprol[l]) continue;
+      CK(launch_prolong(p, l, sp.rd));
+    }
+    CK(cudaStreamWaitEvent(p->stream, p->ev_join, 0));
+    p->interior_done = true;
+    s = launch_rhs(p, a, MODE_STAGE);
+    p->interior_done = false;
+    if (s) return s;
   }
   return TGH_OK;
 }
@@ -1544,8 +1586,14 @@ int tgh_step_batched(tgh_problem* p, double* u, double t, double dt, int nsteps)
     // capture on the problem's own stream (the caller's may be the legacy default stream,
     // which cannot be captured); the graph is then launched on the caller's stream
     if (!p->cap) CK(cudaStreamCreateWithFlags(&p->cap, cudaStreamNonBlocking));
-    // the interior's block list for the whole span the graph steps over, built before capture
+    // the interior's block list for the whole span the graph steps over, built before capture,
+    // and the side branch its kernel runs on
     if ((s = interior_blocks(p, p->ilist_graph, t, t + nsteps * dt))) return s;
+    if (p->intr && !p->side) {
+      CK(cudaStreamCreateWithFlags(&p->side, cudaStreamNonBlocking));
+      CK(cudaEventCreateWithFlags(&p->ev_fork, cudaEventDisableTiming));
+      CK(cudaEventCreateWithFlags(&p->ev_join, cudaEventDisableTiming));
+    }
     cudaGraph_t graph;
     cudaStream_t user = p->stream;
     p->stream = p->cap;
