@@ -150,6 +150,27 @@ class Clocks:
                 "reasons": reasons, "samples": len(sm)}
 
 
+def rhs_kernels(P, cfg):
+    """The kernels one timed right-hand side launches, as the roofline's label."""
+    v = P.variant() if hasattr(P, "variant") else {"pi": "l1"}
+    pi = "rhs_pi_tma_kernel" if v.get("pi") == "tma" else "rhs_pi_kernel"
+    names = ["rhs_head_kernel", pi]
+    if "interior" in cfg and "none" not in str(cfg["interior"]):
+        names.insert(0, "interior_kernel")
+    return " + ".join(names) + " (one RHS, RK4 stage epilogue)"
+
+
+def cpu_model():
+    """The host CPU's model name (for the CPU baseline's record)."""
+    try:
+        for line in Path("/proc/cpuinfo").read_text().splitlines():
+            if line.startswith("model name"):
+                return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "unknown"
+
+
 def cpu_baseline(tgh, sample_case, sample_forest, perturbed, seconds=10.0, max_steps=40):
     """The oracle's RK4 step (the C++ restatement of the reference's CPU path) on a bounded
     sample of the workload, with every host thread: steps until about `seconds` of work."""
@@ -182,6 +203,7 @@ def cpu_baseline(tgh, sample_case, sample_forest, perturbed, seconds=10.0, max_s
     monitors = {"gh_constraint_ms": (t2 - t1) * 1e3, "adm_constraint_ms": (t3 - t2) * 1e3,
                 "points": npts, "unit": "ms per call on the sample"}
     return {"value": pts / el, "unit": "point-updates/s", "cores": int(orc.lib.orc_get_threads()), "kind": "port",
+            "cpu_model": cpu_model(),
             "sample": f"{sample_forest.nblocks} blocks of {sample_forest.N}^3 of the same configuration, "
                       f"{steps} RK4 step(s), {el:.2f} s",
             "monitors": monitors}
@@ -216,6 +238,7 @@ def run_reference(args):
            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
            "config": cfg,
            "cpu_baseline": {"value": val, "unit": "point-updates/s", "cores": cores, "kind": "port",
+                            "cpu_model": cpu_model(),
                             "sample": f"each step: one RK4 step of {sforest.nblocks} blocks of {sforest.N}^3 of the "
                                       "same configuration (the reference is Julia and cannot run here; this is "
                                       "the C++ restatement of its CPU path)"},
@@ -295,7 +318,7 @@ def run_sharded(args, tgh, world, rank, local, case, forest, cfg, gauge, perturb
                       else "per-rank working set below L2 size",
                       "parallelism": f"sharded x{world}: per-level Morton partition, NCCL all-to-all per fill phase",
                       "blocks_per_rank": int(len(S.leaves))},
-           "roofline": {"bound": "fp64", "kernel": "rhs_head_kernel + rhs_pi_kernel (one RHS, RK4 stage epilogue)",
+           "roofline": {"bound": "fp64", "kernel": rhs_kernels(S, cfg),
                         "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
                         "traffic": None, "flop_per_point": FLOP_PER_POINT_RHS[gauge], "points_per_launch": n1pts,
                         "ms_per_launch": rhs_ms,
@@ -590,7 +613,7 @@ def main():
                       "precision": args.precision,
                       "l2_flush": "inputs larger than L2 (working arrays %.0f MB)" % (P.work_length * 8 / 1e6),
                       "parallelism": f"replicas x{world}" if world > 1 else "single GPU"},
-           "roofline": {"bound": "fp64", "kernel": "rhs_head_kernel + rhs_pi_kernel (one RHS, RK4 stage epilogue)",
+           "roofline": {"bound": "fp64", "kernel": rhs_kernels(P, cfg),
                         "achieved": achieved, "peak": peak,
                         "unit": "TFLOP/s", "frac": achieved / peak, "traffic": traffic,
                         "flop_per_point": FLOP_PER_POINT_RHS[gauge], "points_per_launch": n1pts,

@@ -1,0 +1,51 @@
+"""The reference's own end-to-end record: the gauge wave's driver run of bench/stepping.jl.
+
+bench/stepping.jl:73-82, 160-181 (driver mode, BENCH_N = 16, 8^3 roots): gauge_wave_case with
+eps_KO = 1/2, gamma0 = 1, gamma2 = 0 on one periodic wavelength cubed, q = 4, evolve! to
+t_end = 3/50 in chunks of 1/50 at cfl = 1/4. Per chunk evolve! takes dt = cfl h_min / lambda
+with lambda the speed of the state at the chunk's start, rounds the number of steps up and
+spreads them evenly over the chunk (src/driver.jl:1787-1791); the row it records after each
+chunk carries err_l2, the volume-weighted L2 norm of |u - u_exact| over the evolved points
+(src/constraints.jl:311-396, 761-768). The reference printed err_l2 = 7.683712e-09 for the last
+row (CODE.md:6478-6480, kept in tests/golden/reference_pins.json). The error after 33 steps is
+the scheme's truncation error, so the seven printed digits pin the discrete scheme - the
+stencils, the dissipation, the RK4 stages and the step sequence - not its roundoff.
+"""
+import json
+import math
+from pathlib import Path
+
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+PINS = json.loads((Path(__file__).resolve().parent / "golden" / "reference_pins.json").read_text())
+
+
+def _driver(P, u, chunk, nchunks, h_min, cfl=0.25):
+    t = 0.0
+    steps_total = 0
+    for k in range(nchunks):
+        stop = (k + 1) * chunk
+        lam = P.max_speed(u, t)
+        dt = cfl * h_min / lam
+        steps = max(1, math.ceil((stop - t) / dt))
+        dt_used = (stop - t) / steps
+        for s in range(steps):
+            P.rk4_step(u, t + s * dt_used, dt_used)
+        steps_total += steps
+        t = stop
+    return t, steps_total
+
+
+def test_gauge_wave_driver_record_matches_the_reference(tgh):
+    case = tgh.gauge_wave_case(eps_ko=0.5, gamma0=1.0, gamma2=0.0)
+    forest = tgh.gh_forest(case, 16, 8)
+    P = tgh.GHProblem(case, forest, 4)
+    u = P.initial_state(P.statevector(), 0.0)
+    t, steps = _driver(P, u, 1.0 / 50.0, 3, forest.h0)
+    err_l2 = P.error_norm(u, t)[0]
+    ref = PINS["driver_records"]["gauge_wave_err_l2"]
+    # seven significant digits printed: agreement to half a unit in the last of them
+    assert abs(err_l2 - ref) <= 0.5e-6 * ref, (err_l2, ref, steps)
+    P.close()
