@@ -75,7 +75,11 @@ enum {
   TGH_BG_MINKOWSKI = 0,          /* h = 0 */
   TGH_BG_GAUGE_WAVE = 1,         /* ds^2 = -H dt^2 + H dx^2 + dy^2 + dz^2, H = 1 - A sin(2pi(x-t)/d) */
   TGH_BG_SHIFTED_MINKOWSKI = 2,  /* flat space in t^ = t + A w tanh(x/w) */
-  TGH_BG_KERR_SCHILD = 3         /* Kerr-Schild (M, a), spin about +z */
+  TGH_BG_KERR_SCHILD = 3,        /* Kerr-Schild (M, a), spin about +z */
+  TGH_BG_HARMONIC_KERR = 4       /* Kerr (M, a) in horizon-penetrating harmonic coordinates (Harmonic(M, a),
+                                    src/initialdata.jl:1300-1326): the Kerr-Schild metric pulled back along
+                                    x + i y = (r_H + i a) e^{i phi} sin(theta), z = r_H cos(theta) with
+                                    r = r_H + M and t = T_KS - 2 M ln(r - r_-); H_a = 0 exactly */
 };
 
 /* gauge source kinds: GHProblem's HASH switch (src/evolution.jl:1099) */
@@ -84,15 +88,17 @@ enum { TGH_GAUGE_NONE = 0, TGH_GAUGE_SAMPLED = 1, TGH_GAUGE_KERR_SCHILD = 2 };
 enum { TGH_DAMP_CONSTANT = 0, TGH_DAMP_GAUSSIAN = 1 };
 /* Kreiss-Oliger amplitude (src/gauge.jl:1180-1266) */
 enum { TGH_DISS_CONSTANT = 0, TGH_DISS_HORIZON = 1 };
-/* interior variant (src/interior.jl:178-238): :none, :damped, :frozen, :pasted */
-enum { TGH_INT_NONE = 0, TGH_INT_DAMPED = 1, TGH_INT_FROZEN = 2, TGH_INT_PASTED = 3 };
+/* interior variant (src/interior.jl:178-238): :none, :damped, :frozen, :pasted, and :fitted, whose
+ * layer and core relax toward a target read from the problem's target cache (src/evolution.jl:
+ * 517-548, 600-653; the cache src/fit.jl:1030-1055), here over the sphere interior */
+enum { TGH_INT_NONE = 0, TGH_INT_DAMPED = 1, TGH_INT_FROZEN = 2, TGH_INT_PASTED = 3, TGH_INT_FITTED = 4 };
 /* arithmetic of the right-hand side */
 enum { TGH_PREC_FP64 = 0, TGH_PREC_MIXED = 1 };
 
 typedef struct {
   int kind;              /* TGH_BG_* */
   double A, d;           /* gauge wave (A, wavelength d); shifted Minkowski (A, w) */
-  double M, a;           /* Kerr-Schild mass and spin parameter */
+  double M, a;           /* Kerr mass and spin parameter (Kerr-Schild and harmonic charts) */
   double boost[3];       /* boost(metric, u): evaluated at Lambda(u) x, the hole moves at -u */
   double translate[4];   /* translate(metric, (t, x, y, z)), applied after the boost */
 } tgh_background;
@@ -117,6 +123,9 @@ typedef struct {
   double int_c0[3], int_v[3];  /* HoleCenter(c0, v) */
   double r0, r1, rho_max, w_ramp, rho_ramp;
   int precision;               /* TGH_PREC_*: FP64, or FP32 offset-metric stencils + algebra */
+  int target_rate;             /* :fitted: feed the target's rate forward (GHProblem's target_rate,
+                                  src/evolution.jl:1015-1018): (1 - w) d_t u_fit in the layer, d_t u_fit
+                                  in the core */
 } tgh_config;
 
 /* A forest's leaves: closed vertex-centered blocks of N cells per edge (N+1 points).
@@ -168,6 +177,29 @@ int tgh_stage_limit(tgh_problem* p, double* u, double t);
 int tgh_step_limit(tgh_problem* p, double* u, double t);
 int tgh_max_speed(tgh_problem* p, const double* u, double t, double* lambda);
 int tgh_initial_state(tgh_problem* p, double* u, double t);
+
+/* --- the :fitted target cache (src/fit.jl:1030-1285; GHProblem's target, t_target and
+ * target_rate, src/evolution.jl:1009-1018) ---
+ * A :fitted interior's layer and core relax toward A + (t - t_f) S read at the point, where the
+ * cache holds per block 40 fields of the owned points, state layout (N+1)^3 per field: the target
+ * A (the packed h, Pi; fields 0-19) at the fill time t_f and its slope S (fields 20-39). The
+ * right-hand side and the steps refuse a :fitted problem (TGH_ERR_ARG) until one of the first
+ * three verbs has filled the cache; every one of them needs interior = TGH_INT_FITTED.
+ *   tgh_set_target            the cache from a device array of 40 (N+1)^3 nb doubles (a caller's own
+ *                             fit: fill_target! with fit_target_kernel!, src/fit.jl:1134-1156)
+ *   tgh_fill_target_snapshot  fill_snapshot! (src/fit.jl:1189-1222): A = u, S = 0 where the
+ *                             interior radius at t_f is below r_fill, zero elsewhere
+ *   tgh_fill_target_analytic  the case's analytic state at t_f (core rule included) in place of a
+ *                             fit, with S its centred difference over t_f +- dt (dt = 0: S = 0), in
+ *                             the same region
+ *   tgh_fitted_initial_state  fitted_state_kernel! (src/fit.jl:1247-1285) without the blend: the
+ *                             background's state where r >= r_1 - d_init, the cached target at t below
+ *   tgh_copy_target           the cache into a device array of the same shape */
+int tgh_set_target(tgh_problem* p, const double* tw, double t_f);
+int tgh_fill_target_snapshot(tgh_problem* p, const double* u, double t_f, double r_fill);
+int tgh_fill_target_analytic(tgh_problem* p, double t_f, double r_fill, double dt);
+int tgh_fitted_initial_state(tgh_problem* p, double* u, double t, double d_init);
+int tgh_copy_target(tgh_problem* p, double* out);
 
 /* --- one classical RK4 step (IMEXRungeKutta RK4 via gh_integrator, src/stepping.jl:208-225) ---
  * plain form: per stage one ghost fill, one right-hand-side launch, one stage update */

@@ -59,6 +59,11 @@ struct Problem {
   std::vector<double> work, Hsrc;
   std::vector<double> ustate;  // the state the last prepare scattered
   double t_prep = 0.0;
+  // the :fitted target cache (src/fit.jl:1030-1055): per block 40 fields of the owned points, the
+  // target A (h, Pi) at the fill time t_f and its slope S
+  std::vector<double> tw;
+  double t_f = 0.0;
+  bool target_set = false;
   std::string err;
 
   explicit Problem(int q_) : st(q_) {}
@@ -359,6 +364,34 @@ static void rhs_point(const Problem& P, int b, const int I[3], double t, const d
   }
   const Interior& ia = P.in;
   double r = ia.radius(t, x);
+  if (ia.variant == TGH_INT_FITTED) {
+    // the :fitted branches (src/evolution.jl:528-548, 619-653) with the cache's target
+    // A + (t - t_f) S (_cached_target, src/fit.jl:1050) and rate S (_cached_rate, :1055)
+    const size_t S = P.npt_state();
+    const double* tw = P.tw.data() + (size_t)b * 2 * NV * S + (I[0] + P.N1 * ((size_t)I[1] + (size_t)P.N1 * I[2]));
+    auto target = [&](int v) { return tw[v * S] + (t - P.t_f) * tw[(NV + v) * S]; };
+    auto rate = [&](int v) { return tw[(NV + v) * S]; };
+    const bool rt = P.cfg.target_rate != 0;
+    if (ia.is_frozen(r)) {
+      const double rc = ia.rho_max;
+      for (int v = 0; v < NV; ++v)
+        out[v] = rt ? rate(v) - rc * (c.wk[c.var + v * c.sv] - target(v)) : -rc * (c.wk[c.var + v * c.sv] - target(v));
+      return;
+    }
+    double F[NV];
+    rhs_at_point(P, c, b, I, x, t, matter, F, F + NC);
+    if (ia.is_outside(r)) {
+      for (int v = 0; v < NV; ++v) out[v] = F[v];
+      return;
+    }
+    double w, rho;
+    ia.profiles(r, w, rho);
+    const double of = 1.0 - w;
+    for (int v = 0; v < NV; ++v)
+      out[v] = rt ? w * F[v] + of * rate(v) - rho * (c.wk[c.var + v * c.sv] - target(v))
+                  : w * F[v] - rho * (c.wk[c.var + v * c.sv] - target(v));
+    return;
+  }
   if (ia.is_frozen(r)) {
     if (ia.core_follows()) {
       double rho = ia.core_rate(), dl = ia.layer_rate_step();
@@ -461,6 +494,65 @@ static void initial_state(Problem& P, double* u, double t) {
   stage_limit(P, u, t);
 }
 
+// The :fitted target cache's fills. snapshot_target_kernel! (src/fit.jl:1189-1212): the state itself
+// inside r_fill about the interior's centre at t_f, slope 0, zero elsewhere. The analytic fill is
+// fit_target_kernel! (src/fit.jl:1070-1116) with the exact solution standing in for the fit: the
+// case's state (core rule included) at t_f and, with dt > 0, its rate as the centred difference
+// (A(t_f + dt) - A(t_f - dt)) / (2 dt).
+static void fill_target(Problem& P, const double* u, double t_f, double r_fill, double dt) {
+  const size_t S = P.npt_state();
+  P.tw.assign((size_t)P.nb * 2 * NV * S, 0.0);
+#pragma omp parallel for schedule(dynamic)
+  for (int b = 0; b < P.nb; ++b)
+    for (size_t ip = 0; ip < S; ++ip) {
+      const int i = (int)(ip % P.N1), j = (int)((ip / P.N1) % P.N1), k = (int)(ip / ((size_t)P.N1 * P.N1));
+      int64_t n[3] = {(int64_t)P.corner[3 * b] + i, (int64_t)P.corner[3 * b + 1] + j, (int64_t)P.corner[3 * b + 2] + k};
+      double x[3];
+      P.position(P.level[b], n, x);
+      if (!(P.in.radius(t_f, x) < r_fill)) continue;
+      double* o = P.tw.data() + (size_t)b * 2 * NV * S + ip;
+      if (u) {
+        for (int v = 0; v < NV; ++v) o[v * S] = u[(size_t)b * NV * S + v * S + ip];
+        continue;
+      }
+      double a[NV];
+      exact_state(P, t_f, x, a);
+      for (int v = 0; v < NV; ++v) o[v * S] = a[v];
+      if (dt > 0.0) {
+        double ap[NV], am[NV];
+        exact_state(P, t_f + dt, x, ap);
+        exact_state(P, t_f - dt, x, am);
+        const double id = 1.0 / (2.0 * dt);
+        for (int v = 0; v < NV; ++v) o[(NV + v) * S] = id * (ap[v] - am[v]);
+      }
+    }
+  P.t_f = t_f;
+  P.target_set = true;
+}
+
+// fitted_state_kernel! (src/fit.jl:1247-1285) without the blend: the background's state where
+// r >= r_1 - d_init, the cached target at t below
+static void fitted_initial_state(Problem& P, double* u, double t, double d_init) {
+  const size_t S = P.npt_state();
+#pragma omp parallel for schedule(dynamic)
+  for (int b = 0; b < P.nb; ++b)
+    for (size_t ip = 0; ip < S; ++ip) {
+      const int i = (int)(ip % P.N1), j = (int)((ip / P.N1) % P.N1), k = (int)(ip / ((size_t)P.N1 * P.N1));
+      int64_t n[3] = {(int64_t)P.corner[3 * b] + i, (int64_t)P.corner[3 * b + 1] + j, (int64_t)P.corner[3 * b + 2] + k};
+      double x[3];
+      P.position(P.level[b], n, x);
+      double* o = u + (size_t)b * NV * S + ip;
+      if (P.in.radius(t, x) >= P.in.r1 - d_init) {
+        double dh[3][NC], dg[NC], vals[NV];
+        background_state(P.cfg.bg, t, x, vals, vals + NC, dh, dg);
+        for (int v = 0; v < NV; ++v) o[v * S] = vals[v];
+      } else {
+        const double* tw = P.tw.data() + (size_t)b * 2 * NV * S + ip;
+        for (int v = 0; v < NV; ++v) o[v * S] = tw[v * S] + (t - P.t_f) * tw[(NV + v) * S];
+      }
+    }
+}
+
 static bool is_evolved(const Problem& P, double t, const double x[3]) {
   return P.in.variant == TGH_INT_NONE ? true : P.in.radius(t, x) >= P.in.r1;
 }
@@ -510,6 +602,8 @@ static int max_speed(Problem& P, const double* u, double t, double* lam) {
 //   acc = acc + (dt/3) k3;  y4 = u + dt k3
 //   u_new = acc + (dt/6) k4          each update one fused multiply-add
 static void rk4_step(Problem& P, double* u, double t, double dt) {
+  if (P.in.variant == TGH_INT_FITTED && !P.target_set)
+    throw std::runtime_error("a :fitted interior relaxes toward the target cache: fill or set it first");
   const size_t L = P.npt_state() * NV * P.nb;
   std::vector<double> k(L), acc(L), y(L), u0(u, u + L);
   const double b16 = dt / 6.0, b13 = dt / 3.0, a12 = 0.5 * dt;
@@ -998,7 +1092,15 @@ int orc_prepare(void* p, const double* u, double t) {
   try { prepare(*(Problem*)p, u, t); } catch (const std::exception& e) { ((Problem*)p)->err = e.what(); return TGH_ERR_ARG; }
   return TGH_OK;
 }
-int orc_rhs(void* p, double* du, double t, const double* matter) { rhs(*(Problem*)p, du, t, matter); return TGH_OK; }
+int orc_rhs(void* p, double* du, double t, const double* matter) {
+  Problem& P = *(Problem*)p;
+  if (P.in.variant == TGH_INT_FITTED && !P.target_set) {
+    P.err = "a :fitted interior relaxes toward the target cache: fill or set it first";
+    return TGH_ERR_ARG;
+  }
+  rhs(P, du, t, matter);
+  return TGH_OK;
+}
 int orc_gh_rhs(void* p, double* du, const double* u, double t, const double* matter) {
   int s = orc_prepare(p, u, t);
   if (s) return s;
@@ -1023,6 +1125,31 @@ int orc_copy_hsrc(void* p, double* dst) {
 }
 int orc_initial_state(void* p, double* u, double t) { initial_state(*(Problem*)p, u, t); return TGH_OK; }
 int orc_stage_limit(void* p, double* u, double t) { stage_limit(*(Problem*)p, u, t); return TGH_OK; }
+int orc_set_target(void* p, const double* tw, double t_f) {
+  Problem& P = *(Problem*)p;
+  const size_t L = (size_t)P.nb * 2 * NV * P.npt_state();
+  P.tw.assign(tw, tw + L);
+  P.t_f = t_f;
+  P.target_set = true;
+  return TGH_OK;
+}
+int orc_fill_target_snapshot(void* p, const double* u, double t_f, double r_fill) {
+  fill_target(*(Problem*)p, u, t_f, r_fill, 0.0);
+  return TGH_OK;
+}
+int orc_fill_target_analytic(void* p, double t_f, double r_fill, double dt) {
+  fill_target(*(Problem*)p, nullptr, t_f, r_fill, dt);
+  return TGH_OK;
+}
+int orc_fitted_initial_state(void* p, double* u, double t, double d_init) {
+  fitted_initial_state(*(Problem*)p, u, t, d_init);
+  return TGH_OK;
+}
+int orc_copy_target(void* p, double* out) {
+  const Problem& P = *(Problem*)p;
+  std::copy(P.tw.begin(), P.tw.end(), out);
+  return TGH_OK;
+}
 int orc_max_speed(void* p, const double* u, double t, double* lam) { return max_speed(*(Problem*)p, u, t, lam); }
 int orc_rk4_step(void* p, double* u, double t, double dt) {
   try { rk4_step(*(Problem*)p, u, t, dt); } catch (const std::exception& e) { ((Problem*)p)->err = e.what(); return TGH_ERR_ARG; }

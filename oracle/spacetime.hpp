@@ -11,6 +11,16 @@
 //   ShiftedMinkowski   flat space in t^ = t + A w tanh(x/w) (src/initialdata.jl:914-947)
 //   KerrSchild(M, a)   g = eta + 2 H l l,  H = M r^3 / (r^4 + a^2 z^2),
 //                      l = (1, (r x + a y)/(r^2+a^2), (r y - a x)/(r^2+a^2), z/r)
+//   Harmonic(M, a)     Kerr in horizon-penetrating harmonic coordinates: the Kerr-Schild metric
+//                      pulled back, g = J^T g_KS J, along the map from the harmonic chart
+//                      X + i Y = w (x + i y), Z = (r / r_H) z, T = t + 2 M ln(r_H + sqrt(M^2 - a^2)),
+//                      w = (r + i a) / (r_H + i a), r = r_H + M, r_H the spheroidal radius of
+//                      (x, y, z) with parameter a (the Kerr-Schild quartic): both charts share the
+//                      Kerr-Schild angle phi, the harmonic radius is r - M, and the harmonic time
+//                      t_BL + 2 M r_+ int dr / Delta is regular on the future horizon. J is formed
+//                      in closed form from d r_H / d x^i = r_H (x_i r_H^2 + a^2 z delta_iz) /
+//                      (r_H^4 + a^2 z^2); the chart is harmonic (H_a = 0) and at a = 0 it is the
+//                      harmonic Schwarzschild metric g_tt = -(r-M)/(r+M), g_tr = 4M^2/(r+M)^2
 //   boost(m, u)        m evaluated at Lambda(u) x and pulled back, the hole moves at -u
 //                      (src/interior.jl:67-73)
 //   translate(m, D)    m evaluated at x - D
@@ -116,6 +126,59 @@ template <class S> static inline void kerr_schild(double M, double a, const S x[
     for (int j = 0; j < 4; ++j) g[i][j] = S(i == j ? eta(i) : 0.0) + S(2.0) * H * l[i] * l[j];
 }
 
+// Kerr in harmonic coordinates in its rest frame (t = x[0]; the metric does not depend on t)
+template <class S> static inline void harmonic_kerr(double M, double a, const S x[4], S g[4][4]) {
+  S X = x[1], Y = x[2], Z = x[3];
+  S rho2 = X * X + Y * Y + Z * Z;
+  S a2 = S(a * a);
+  S half = S(0.5) * (rho2 - a2);
+  S r2 = half + sqrt(half * half + a2 * Z * Z);  // r_H^2
+  S rh = sqrt(r2);
+  S q = r2 * r2 + a2 * Z * Z;
+  // d r_H / d x^i
+  S dr[3] = {rh * (X * r2) / q, rh * (Y * r2) / q, rh * (Z * r2 + a2 * Z) / q};
+  S r = rh + S(M);
+  S D = r2 + a2;
+  S wr = (r * rh + a2) / D;  // w = (r + i a) / (r_H + i a)
+  S wi = S(-a * M) / D;
+  S D2 = D * D;
+  S dwr = S(-M) * (r2 - a2) / D2;  // d w / d r_H = -M / (r_H + i a)^2
+  S dwi = S(2.0 * M * a) * rh / D2;
+  S px = X * dwr - Y * dwi;  // Re, Im of (x + i y) d w / d r_H
+  S py = X * dwi + Y * dwr;
+  S zr = r / rh;
+  S zd = S(-M) * Z / r2;
+  S tr = S(2.0 * M) / (rh + S(std::sqrt(M * M - a * a)));
+  // the Kerr-Schild point and J[A][b] = d X^A / d x^b
+  S xk[4] = {x[0], wr * X - wi * Y, wr * Y + wi * X, zr * Z};
+  S J[4][4];
+  J[0][0] = S(1.0);
+  J[1][0] = J[2][0] = J[3][0] = S(0.0);
+  for (int j = 0; j < 3; ++j) {
+    J[0][j + 1] = tr * dr[j];
+    J[1][j + 1] = px * dr[j];
+    J[2][j + 1] = py * dr[j];
+    J[3][j + 1] = zd * dr[j];
+  }
+  J[1][1] = wr + J[1][1];
+  J[1][2] = J[1][2] - wi;
+  J[2][1] = wi + J[2][1];
+  J[2][2] = wr + J[2][2];
+  J[3][3] = zr + J[3][3];
+  S gk[4][4];
+  kerr_schild(M, a, xk, gk);
+  for (int p = 0; p < 4; ++p)
+    for (int s = 0; s < 4; ++s) {
+      S acc = S(0.0);
+      for (int A = 0; A < 4; ++A) {
+        S t = J[0][s] * gk[A][0];
+        for (int B = 1; B < 4; ++B) t = t + J[B][s] * gk[A][B];
+        acc = acc + J[A][p] * t;
+      }
+      g[p][s] = acc;
+    }
+}
+
 // the boost matrix Lambda(u): x_rest = Lambda x_lab
 static inline void boost_matrix(const double u[3], double L[4][4]) {
   double u2 = u[0] * u[0] + u[1] * u[1] + u[2] * u[2];
@@ -155,10 +218,17 @@ template <class S> static inline void metric_eval(const tgh_background& bg, cons
       g[1][1] = S(1.0) - psi * psi;
       return;
     }
-    case TGH_BG_KERR_SCHILD: {
+    case TGH_BG_KERR_SCHILD:
+    case TGH_BG_HARMONIC_KERR: {
+      auto rest = [&](const S* y, S (*gy)[4]) {
+        if (bg.kind == TGH_BG_KERR_SCHILD)
+          kerr_schild(bg.M, bg.a, y, gy);
+        else
+          harmonic_kerr(bg.M, bg.a, y, gy);
+      };
       bool boosted = bg.boost[0] != 0.0 || bg.boost[1] != 0.0 || bg.boost[2] != 0.0;
       if (!boosted) {
-        kerr_schild(bg.M, bg.a, x, g);
+        rest(x, g);
         return;
       }
       double L[4][4];
@@ -170,7 +240,7 @@ template <class S> static inline void metric_eval(const tgh_background& bg, cons
         xr[i] = s;
       }
       S gr[4][4];
-      kerr_schild(bg.M, bg.a, xr, gr);
+      rest(xr, gr);
       for (int a = 0; a < 4; ++a)
         for (int b = 0; b < 4; ++b) {
           S s = S(0.0);

@@ -58,7 +58,7 @@ def rhs_error(du_gpu, du_ref, scale, forest):
     return float(np.max(np.max(np.abs(a - b), axis=1) / scale))
 
 
-N_ROWS = 20
+N_ROWS = 22
 
 
 def cases(tgh):
@@ -97,6 +97,11 @@ def cases(tgh):
     c = tgh.kerr_schild_case(M=1.0, a=0.7, v=0.1, halfwidth=4.0, r0=0.8, r1=1.3, gauge="algebraic")
     f = tgh.hole_forest(c, 8, 2, [3.0, 1.8, 1.4], path=((0.0, 0.0, 0.0), (0.05, 0.0, 0.0)))
     rows.append(("kerr_schild_hierarchy_moving", c, f, 4, 0.3))
+    # Kerr in harmonic coordinates (no gauge source), at rest and moving
+    c = tgh.harmonic_kerr_case(M=1.0, a=0.7, halfwidth=2.0, r0=0.9, r1=1.4)
+    rows.append(("harmonic_kerr_damped", c, tgh.gh_forest(c, 8, 2), 4, 0.0))
+    c = tgh.harmonic_kerr_case(M=1.0, a=0.7, v=0.1, halfwidth=2.0, r0=0.9, r1=1.4)
+    rows.append(("harmonic_kerr_moving", c, tgh.gh_forest(c, 8, 2), 4, 0.3))
     assert len(rows) == N_ROWS
     return rows
 

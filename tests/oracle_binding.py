@@ -43,6 +43,11 @@ class Oracle:
             "orc_set_work": (ctypes.c_int, [_VP, _DP]),
             "orc_initial_state": (ctypes.c_int, [_VP, _DP, _D]),
             "orc_stage_limit": (ctypes.c_int, [_VP, _DP, _D]),
+            "orc_set_target": (ctypes.c_int, [_VP, _DP, _D]),
+            "orc_fill_target_snapshot": (ctypes.c_int, [_VP, _DP, _D, _D]),
+            "orc_fill_target_analytic": (ctypes.c_int, [_VP, _D, _D, _D]),
+            "orc_fitted_initial_state": (ctypes.c_int, [_VP, _DP, _D, _D]),
+            "orc_copy_target": (ctypes.c_int, [_VP, _DP]),
             "orc_max_speed": (ctypes.c_int, [_VP, _DP, _D, _DP]),
             "orc_rk4_step": (ctypes.c_int, [_VP, _DP, _D, _D]),
             "orc_error_norm": (ctypes.c_int, [_VP, _DP, _D, _DP, _DP]),
@@ -218,7 +223,29 @@ class OracleProblem:
         assert st == 0, self.lib.orc_last_error(self.h)
 
     def rhs(self, du, t, matter=None):
-        self.lib.orc_rhs(self.h, _dp(du), t, _dp(matter) if matter is not None else None)
+        st = self.lib.orc_rhs(self.h, _dp(du), t, _dp(matter) if matter is not None else None)
+        assert st == 0, self.lib.orc_last_error(self.h)
+
+    # the :fitted target cache (40 fields of the owned points per block)
+    def set_target(self, tw, t_f):
+        tw = np.ascontiguousarray(tw, dtype=float)
+        assert tw.size == 2 * self.L
+        self.lib.orc_set_target(self.h, _dp(tw), t_f)
+
+    def fill_target_snapshot(self, u, t_f, r_fill):
+        self.lib.orc_fill_target_snapshot(self.h, _dp(np.ascontiguousarray(u, dtype=float)), t_f, r_fill)
+
+    def fill_target_analytic(self, t_f, r_fill, dt=0.0):
+        self.lib.orc_fill_target_analytic(self.h, t_f, r_fill, dt)
+
+    def fitted_initial_state(self, u, t, d_init=0.0):
+        self.lib.orc_fitted_initial_state(self.h, _dp(u), t, d_init)
+        return u
+
+    def target(self):
+        out = np.zeros(2 * self.L)
+        self.lib.orc_copy_target(self.h, _dp(out))
+        return out
 
     def gh_rhs(self, du, u, t, matter=None):
         self.prepare(u, t)

@@ -27,7 +27,7 @@ def _initial(tgh, P, O, case, forest, name, t):
     u = O.initial_state(O.statevector(), t)
     if name.startswith("perturbed"):
         u = u + tgh.perturbation(forest, amplitude=1e-4)
-    elif name.startswith("kerr") or name.startswith("gauge"):
+    elif name.startswith("kerr") or name.startswith("gauge") or name.startswith("harmonic"):
         u = u + tgh.perturbation(forest, amplitude=1e-6, seed=11)
     if name.endswith("pasted"):
         O.stage_limit(u, t)
@@ -98,7 +98,7 @@ def test_fill_matches_oracle(tgh, oracle, which):
     assert np.array_equal(wg, wo)
 
 
-@pytest.mark.parametrize("row", [0, 2, 6, 7, 9, 11, 14, 17, 18, 19])
+@pytest.mark.parametrize("row", [0, 2, 6, 7, 9, 11, 14, 17, 18, 19, 20, 21])
 def test_rk4_step_matches_oracle(tgh, oracle, row):
     name, case, forest, q, t = cases(tgh)[row]
     P = tgh.GHProblem(case, forest, q, margin_check=False)
@@ -183,15 +183,17 @@ def test_hole_interior_is_masked_for_speed(tgh):
 
 def test_analytic_state_is_the_oracles_bit_for_bit(tgh, oracle):
     """The device's analytic state (Dirichlet ghosts, layer and core targets) at points around a
-    resting and a moving (boosted) spinning hole and near its ring singularity: every h, Pi bit
-    for bit the oracle's. The moving hole's target rates are centred differences of this state
-    over 1.2e-5 r_0 in t, which would turn one ulp into ~1e-11. Kerr-Schild takes only
+    resting and a moving (boosted) spinning hole, in Kerr-Schild and in harmonic coordinates, and
+    near the chart's singular set: every h, Pi bit for bit the oracle's. The moving hole's target rates are centred differences of this state
+    over 1.2e-5 r_0 in t, which would turn one ulp into ~1e-11. Both charts take only
     +, -, *, / and square roots, correctly rounded on both sides; shifted Minkowski's tanh (and
     the gauge wave's sin) come from CUDA's and the C library's own functions, which may differ
     in the last bit, and psi = A (1 - tanh^2) carries that on: there, within 1e-15 of max(1, |u|)."""
     rng = np.random.default_rng(7)
     for case in (tgh.kerr_schild_case(M=1.0, a=0.7, halfwidth=2.0, r0=0.8, r1=1.3, gauge="algebraic"),
                  tgh.kerr_schild_case(M=1.0, a=0.7, v=0.1, halfwidth=2.0, r0=0.8, r1=1.3, gauge="algebraic"),
+                 tgh.harmonic_kerr_case(M=1.0, a=0.7, halfwidth=2.0, r0=0.9, r1=1.4),
+                 tgh.harmonic_kerr_case(M=1.0, a=0.7, v=0.1, halfwidth=2.0, r0=0.9, r1=1.4),
                  tgh.shifted_minkowski_case(eps_ko=0.5, gamma0=1.0, gamma2=-0.5)):
         f = tgh.gh_forest(case, 8, 2)
         P = tgh.GHProblem(case, f, 4, margin_check=False)
@@ -205,7 +207,7 @@ def test_analytic_state_is_the_oracles_bit_for_bit(tgh, oracle):
                 continue  # the core rule moves the point; the background is compared off the core
             h, Pi, _, _ = oracle.background_state(bg, t, x)
             ref = np.concatenate([h, Pi])
-            if case.background["kind"] == "kerr_schild":
+            if case.background["kind"] in ("kerr_schild", "harmonic_kerr"):
                 assert np.array_equal(got, ref), (k, x, got - ref)
             else:
                 assert np.all(np.abs(got - ref) <= 1e-15 * np.maximum(np.abs(ref), 1.0)), (k, x, got - ref)

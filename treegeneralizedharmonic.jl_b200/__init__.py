@@ -8,7 +8,8 @@ The package loads as `tgh_b200` (its directory name is not a Python identifier):
         submodule_search_locations=["<repo>/treegeneralizedharmonic.jl_b200"])
 
 Public surface, named after the reference's:
-  cases      minkowski_case, gauge_wave_case, shifted_minkowski_case, kerr_schild_case, ...
+  cases      minkowski_case, gauge_wave_case, shifted_minkowski_case, kerr_schild_case,
+             harmonic_kerr_case, ...
   forests    gh_forest, hole_forest
   problem    GHProblem with prepare, rhs, gh_rhs, settle, stage_limit, step_limit, max_speed,
              initial_state, gh_dt, rk4_step, step_batched, gh_solve, error_norm,
@@ -25,8 +26,8 @@ from . import bounds, checkpoint, refinement
 from .bounds import StateBounds, check_bounds_gate, default_bounds, default_gate, layer_spacing
 from .checkpoint import latest_checkpoint, load_checkpoint, save_checkpoint
 from .refinement import Refinement, indicator_flags, level_bounds, refine_flags
-from .cases import (Case, gauge_wave_case, horizon_min_radius, kerr_schild_case, minkowski_case,
-                    perturbed_minkowski_case, shifted_minkowski_case)
+from .cases import (Case, gauge_wave_case, harmonic_kerr_case, horizon_min_radius, kerr_schild_case,
+                    minkowski_case, perturbed_minkowski_case, shifted_minkowski_case)
 from .forest import Forest, gh_forest, hole_forest
 from .initialdata import fourier_modes, perturbation
 from .problem import GHProblem, fp64_peak_tflops
@@ -35,7 +36,7 @@ from .gradient import MaskedError, MaskedErrorStudy
 from .adjoint import MaskedErrorOfState, masked_error_adjoint
 from . import autotune
 
-__all__ = ["StateBounds", "check_bounds_gate", "default_bounds", "default_gate", "layer_spacing", "Case", "Forest", "GHProblem", "gauge_wave_case", "gh_forest", "hole_forest", "kerr_schild_case",
+__all__ = ["StateBounds", "check_bounds_gate", "default_bounds", "default_gate", "layer_spacing", "Case", "Forest", "GHProblem", "gauge_wave_case", "gh_forest", "hole_forest", "kerr_schild_case", "harmonic_kerr_case",
            "minkowski_case", "perturbed_minkowski_case", "shifted_minkowski_case", "horizon_min_radius",
            "fourier_modes", "perturbation", "fp64_peak_tflops", "load_library", "ShardedGHProblem",
            "exchange_plan", "partition", "MaskedError", "MaskedErrorStudy", "Refinement", "indicator_flags",

@@ -12,11 +12,11 @@ LIB_PATH = _HERE / "lib" / "libtgh_b200.so"
 
 (TGH_OK, TGH_ERR_ARG, TGH_ERR_NONFINITE, TGH_ERR_SPEED, TGH_ERR_RADII, TGH_ERR_TIMEOUT, TGH_ERR_CUDA, TGH_ERR_NOMEM,
  TGH_ERR_STALE) = range(9)
-BG_MINKOWSKI, BG_GAUGE_WAVE, BG_SHIFTED_MINKOWSKI, BG_KERR_SCHILD = range(4)
+BG_MINKOWSKI, BG_GAUGE_WAVE, BG_SHIFTED_MINKOWSKI, BG_KERR_SCHILD, BG_HARMONIC_KERR = range(5)
 GAUGE_NONE, GAUGE_SAMPLED, GAUGE_KERR_SCHILD = range(3)
 DAMP_CONSTANT, DAMP_GAUSSIAN = range(2)
 DISS_CONSTANT, DISS_HORIZON = range(2)
-INT_NONE, INT_DAMPED, INT_FROZEN, INT_PASTED = range(4)
+INT_NONE, INT_DAMPED, INT_FROZEN, INT_PASTED, INT_FITTED = range(5)
 PREC_FP64, PREC_MIXED = range(2)
 MASK_INTERIOR, MASK_ALL = range(2)
 TGH_PI_L1, TGH_PI_TMA = range(2)
@@ -43,7 +43,7 @@ class Config(ctypes.Structure):
                 ("eps_r1", ctypes.c_double), ("eps_rh", ctypes.c_double), ("eps_c0", D3), ("eps_v", D3),
                 ("interior", ctypes.c_int), ("int_c0", D3), ("int_v", D3), ("r0", ctypes.c_double),
                 ("r1", ctypes.c_double), ("rho_max", ctypes.c_double), ("w_ramp", ctypes.c_double),
-                ("rho_ramp", ctypes.c_double), ("precision", ctypes.c_int)]
+                ("rho_ramp", ctypes.c_double), ("precision", ctypes.c_int), ("target_rate", ctypes.c_int)]
 
 
 class Mesh(ctypes.Structure):
@@ -79,6 +79,11 @@ SIGNATURES = {
     "tgh_step_limit": (ctypes.c_int, [_VP, _VP, _D]),
     "tgh_max_speed": (ctypes.c_int, [_VP, _VP, _D, ctypes.POINTER(_D)]),
     "tgh_initial_state": (ctypes.c_int, [_VP, _VP, _D]),
+    "tgh_set_target": (ctypes.c_int, [_VP, _VP, _D]),
+    "tgh_fill_target_snapshot": (ctypes.c_int, [_VP, _VP, _D, _D]),
+    "tgh_fill_target_analytic": (ctypes.c_int, [_VP, _D, _D, _D]),
+    "tgh_fitted_initial_state": (ctypes.c_int, [_VP, _VP, _D, _D]),
+    "tgh_copy_target": (ctypes.c_int, [_VP, _VP]),
     "tgh_rk4_step": (ctypes.c_int, [_VP, _VP, _D, _D]),
     "tgh_rk4_step_blocks": (ctypes.c_int, [_VP, _VP, _D, _D]),
     "tgh_set_variant": (ctypes.c_int, [_VP, ctypes.c_int, ctypes.c_int, ctypes.c_int]),

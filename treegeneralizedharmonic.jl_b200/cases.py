@@ -28,7 +28,8 @@ class Case:
         c.q = int(q)
         bg = self.background
         kinds = {"minkowski": _abi.BG_MINKOWSKI, "gauge_wave": _abi.BG_GAUGE_WAVE,
-                 "shifted_minkowski": _abi.BG_SHIFTED_MINKOWSKI, "kerr_schild": _abi.BG_KERR_SCHILD}
+                 "shifted_minkowski": _abi.BG_SHIFTED_MINKOWSKI, "kerr_schild": _abi.BG_KERR_SCHILD,
+                 "harmonic_kerr": _abi.BG_HARMONIC_KERR}
         c.bg.kind = kinds[bg["kind"]]
         c.bg.A = bg.get("A", 0.0)
         c.bg.d = bg.get("d", 1.0)
@@ -68,8 +69,9 @@ class Case:
             c.eps_ko = float(self.eps_ko)
         if self.interior:
             it = self.interior
-            c.interior = {"damped": _abi.INT_DAMPED, "frozen": _abi.INT_FROZEN,
-                          "pasted": _abi.INT_PASTED}[it.get("variant", "damped")]
+            c.interior = {"damped": _abi.INT_DAMPED, "frozen": _abi.INT_FROZEN, "pasted": _abi.INT_PASTED,
+                          "fitted": _abi.INT_FITTED}[it.get("variant", "damped")]
+            c.target_rate = 1 if it.get("target_rate", False) else 0
             for i in range(3):
                 c.int_c0[i] = it["c0"][i]
                 c.int_v[i] = it.get("v", (0, 0, 0))[i]
@@ -108,12 +110,13 @@ def perturbed_minkowski_case(halfwidth=1.0, eps_ko=0.5, gamma0=1.0, gamma2=0.0):
 
 def kerr_schild_case(M=1.0, a=0.0, v=0.0, x0=0.0, halfwidth=8.0, r0=0.8, r1=1.3, rho_max=None,
                      variant="damped", gauge="sampled", eps_ko=0.5, gamma0=None, gamma2=0.0, w_ramp=0.5,
-                     rho_ramp=0.5, margin=8):
+                     rho_ramp=0.5, margin=8, target_rate=False):
     """A Kerr-Schild hole in a Dirichlet box with the damping layer (hole_case /
     kerr_schild_case, src/initialdata.jl:1044-1300). The hole sits at (x0 + v t, 0, 0): the
     background is translate(boost(KerrSchild(M, a), (-v, 0, 0)), (0, x0, 0, 0)). A moving hole
     needs the algebraic gauge source. The default damping is GHSO2's Gaussian: 1/M at the hole,
-    1/(10 M) far away, width 3 M."""
+    1/(10 M) far away, width 3 M. variant "fitted" relaxes the layer and core toward the problem's
+    target cache (GHProblem.fill_target_*, set_target), with target_rate feeding its rate forward."""
     if v != 0.0 and gauge == "sampled":
         raise ValueError("a moving hole's gauge source depends on time: pass gauge='algebraic'")
     bg = {"kind": "kerr_schild", "M": M, "a": a, "boost": (-v, 0.0, 0.0), "translate": (0.0, x0, 0.0, 0.0)}
@@ -125,13 +128,37 @@ def kerr_schild_case(M=1.0, a=0.0, v=0.0, x0=0.0, halfwidth=8.0, r0=0.8, r1=1.3,
     if variant is not None:
         interior = {"variant": variant, "c0": centre, "v": vel, "r0": r0, "r1": r1,
                     "rho_max": 4.0 / M if rho_max is None else rho_max, "w_ramp": w_ramp, "rho_ramp": rho_ramp,
-                    "margin": margin}
+                    "margin": margin, "target_rate": bool(target_rate)}
     ks = {"M": M, "spin": (0.0, 0.0, a), "velocity": vel}
     return Case(bg, ((-halfwidth, halfwidth),) * 3, (False, False, False), eps_ko, gamma0, gamma2, interior,
                 gauge, ks, M)
 
 
-def horizon_min_radius(M, a, v=0.0):
-    """The smallest coordinate radius of the Kerr-Schild horizon, r_+ = M + sqrt(M^2 - a^2),
-    Lorentz-contracted along the motion."""
-    return (M + math.sqrt(M * M - a * a)) * math.sqrt(1.0 - v * v)
+def harmonic_kerr_case(M=1.0, a=0.0, v=0.0, x0=0.0, halfwidth=8.0, r0=0.8, r1=1.3, rho_max=None,
+                       variant="damped", gauge="none", eps_ko=0.5, gamma0=None, gamma2=0.0, w_ramp=0.5,
+                       rho_ramp=0.5, margin=8, target_rate=False):
+    """A hole in fully harmonic Cartesian coordinates (harmonic_kerr_case,
+    src/initialdata.jl:1300-1326): the background is translate(boost(Harmonic(M, a), (-v, 0, 0)),
+    (0, x0, 0, 0)), horizon penetrating and harmonic, so H = 0 exactly and no gauge source is
+    needed, moving or not (a boost of a harmonic chart is harmonic). Every other keyword is
+    kerr_schild_case's. The chart's singular set is the disk x^2 + y^2 <= a^2, z = 0, which the
+    frozen core must contain (r0 > |a|)."""
+    if not abs(a) < M:
+        raise ValueError("the harmonic chart needs |a| < M")
+    c = kerr_schild_case(M=M, a=a, v=v, x0=x0, halfwidth=halfwidth, r0=r0, r1=r1, rho_max=rho_max,
+                         variant=variant, gauge="algebraic" if gauge == "algebraic" else "none", eps_ko=eps_ko,
+                         gamma0=gamma0, gamma2=gamma2, w_ramp=w_ramp, rho_ramp=rho_ramp, margin=margin,
+                         target_rate=target_rate)
+    c.background = dict(c.background, kind="harmonic_kerr")
+    c.gauge = gauge
+    if gauge != "algebraic":
+        c.ks_source = None
+    return c
+
+
+def horizon_min_radius(M, a, v=0.0, chart="kerr_schild"):
+    """The smallest coordinate radius of the horizon, Lorentz-contracted along the motion: the
+    spheroidal radius r_+ = M + sqrt(M^2 - a^2) in Kerr-Schild coordinates, r_+ - M =
+    sqrt(M^2 - a^2) in the harmonic chart (on the spin axis)."""
+    r = math.sqrt(M * M - a * a) + (M if chart == "kerr_schild" else 0.0)
+    return r * math.sqrt(1.0 - v * v)

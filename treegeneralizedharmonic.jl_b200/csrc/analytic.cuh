@@ -119,6 +119,18 @@ TGH_HD void rn_kerr_schild(double M, double a, const RD x[4], RD g[4][4]) {
     for (int j = 0; j < 4; ++j) g[i][j] = RD(i == j ? etad(i) : 0.0) + RD(2.0) * H * l[i] * l[j];
 }
 
+// the rounded duals for the templated closed forms of physics.cuh (found by argument lookup)
+TGH_HD RD dsqrt(const RD& a) { return rsqrt_n(a); }
+TGH_HD void ks_rest(double M, double a, const RD* x, RD g[4][4]) { rn_kerr_schild(M, a, x, g); }
+
+// a hole's metric in its rest frame: Kerr-Schild, or Kerr in harmonic coordinates
+TGH_HD void rn_hole_rest(const Case& c, const RD x[4], RD g[4][4]) {
+  if (c.bg.kind == TGH_BG_HARMONIC_KERR)
+    harmonic_kerr_rest<RD>(c.bg.M, c.bg.a, x, g);
+  else
+    rn_kerr_schild(c.bg.M, c.bg.a, x, g);
+}
+
 // the case's metric g_ab with its first derivatives at xin = (t, x, y, z)
 TGH_HD void rn_metric(const Case& c, const RD xin[4], RD g[4][4]) {
   RD x[4];
@@ -138,9 +150,9 @@ TGH_HD void rn_metric(const Case& c, const RD xin[4], RD g[4][4]) {
     g[0][1] = -psi;
     g[1][0] = -psi;
     g[1][1] = RD(1.0) - psi * psi;
-  } else if (c.bg.kind == TGH_BG_KERR_SCHILD) {
+  } else if (c.bg.kind == TGH_BG_KERR_SCHILD || c.bg.kind == TGH_BG_HARMONIC_KERR) {
     if (!c.boosted) {
-      rn_kerr_schild(c.bg.M, c.bg.a, x, g);
+      rn_hole_rest(c, x, g);
       return;
     }
     RD xr[4], gr[4][4];
@@ -151,7 +163,7 @@ TGH_HD void rn_metric(const Case& c, const RD xin[4], RD g[4][4]) {
       for (int j = 1; j < 4; ++j) s = s + RD(c.L[i][j]) * x[j];
       xr[i] = s;
     }
-    rn_kerr_schild(c.bg.M, c.bg.a, xr, gr);
+    rn_hole_rest(c, xr, gr);
     // g_ab = sum_cd (L_ca L_db) g_rest_cd, c outer, d inner
 #pragma unroll
     for (int a = 0; a < 4; ++a)

@@ -225,6 +225,84 @@ static __global__ void fill_prolong_kernel(const ProlongPt* __restrict__ pts, in
       prolong_value<P>(work + (long)p.src_b * NV * g.Wv + (long)v * g.Wv + p.src_w, p.odd, g);
 }
 
+// The prolongation sum-factorised over tiles: the prolonged points of one fine block whose
+// stencils lie in one coarse block, cut into boxes of 8 x 8 x 8 fine points aligned to the
+// block's corner. A point's value is the per-point order above - for each coarse z, for each
+// coarse y, the x sum; the y sum of those; the z sum - and every partial sum of that order
+// depends only on the fine x (the x sums), on the fine x and y (the y sums) and the coarse rows
+// it is taken over, so the tile forms each partial sum once, in shared memory, and all its
+// points read them: stage X over (fine x, coarse y, coarse z), stage Y over (fine x, fine y,
+// coarse z), stage Z at the listed points. Rounding and order per point are the per-point
+// kernel's, operation for operation, so both give the same bits.
+struct ProlongTile {
+  int dst_b, src_b;
+  short i0, j0, k0;     // the fine working-array coordinates of the tile's origin (may lie below 0)
+  short cxb, cyb, czb;  // coarse working-array coordinate of the centre of fine offset 0
+  short ylo, zlo;       // the coarse rows stage X covers: [ylo, ylo + cyn) x [zlo, zlo + czn)
+  unsigned char cyn, czn;
+  unsigned char par;    // bit d: the fine lattice index of the origin is odd along axis d
+  unsigned char nfx, nfy;
+  unsigned char pad;
+  int fxs, fys;         // the fine x (y) offsets holding listed points, 3 bits each, nfx (nfy) of them
+  int p0, np;           // the listed points: pts[p0 .. p0 + np), fx | fy << 3 | fz << 6
+};
+
+template <int P>
+__device__ __forceinline__ double lagrange_sum(const double* v, int stride) {
+  constexpr ProlongWeights<P> W = prolong_weights<P>();
+  double s = __dmul_rn(W.v[0], v[0]);
+#pragma unroll
+  for (int k = 1; k < P; ++k) s = __dadd_rn(s, __dmul_rn(W.v[k], v[k * stride]));
+  return s;
+}
+
+// One CTA per tile, its threads on one variable at a time (the two stages' arrays are one
+// variable's, at most 19.7 KB at P = 10, so that several CTAs share an SM and hide the stages'
+// load and reduction latency).
+constexpr int PROLONG_TILE_THREADS = 128;
+
+template <int P>
+static __global__ void __launch_bounds__(PROLONG_TILE_THREADS, 8)
+    fill_prolong_tile_kernel(const ProlongTile* __restrict__ tiles, const unsigned short* __restrict__ pts,
+                             double* __restrict__ work, Geo g) {
+  constexpr int C = P + 4, H = P / 2 - 1;
+  __shared__ double X[8 * C * C];
+  __shared__ double Y[8 * 8 * C];
+  const ProlongTile T = tiles[blockIdx.x];
+  const int px = T.par & 1, py = (T.par >> 1) & 1, pz = (T.par >> 2) & 1;
+  const long sy = g.Wx, sz = (long)g.Wx * g.Wd;
+  const int nX = T.nfx * T.cyn * T.czn, nY = T.nfx * T.nfy * T.czn;
+  for (int v = 0; v < NV; ++v) {
+    const double* src = work + (long)T.src_b * NV * g.Wv + (long)v * g.Wv;
+    // stage X: the x sum of every coarse row (y, z) at every listed fine x
+    for (int e = threadIdx.x; e < nX; e += PROLONG_TILE_THREADS) {
+      const int cyi = e % T.cyn, r = e / T.cyn, czi = r % T.czn, kx = r / T.czn;
+      const int fx = (T.fxs >> (3 * kx)) & 7, nx = px + fx;
+      const double* row = src + (T.cxb + (nx >> 1)) + sy * (T.ylo + cyi) + sz * (T.zlo + czi);
+      X[(fx * C + czi) * C + cyi] = (nx & 1) ? lagrange_sum<P>(row - H, 1) : row[0];
+    }
+    __syncthreads();
+    // stage Y: the y sum over those rows at every listed (fine x, fine y)
+    for (int e = threadIdx.x; e < nY; e += PROLONG_TILE_THREADS) {
+      const int czi = e % T.czn, r = e / T.czn, ky = r % T.nfy, kx = r / T.nfy;
+      const int fx = (T.fxs >> (3 * kx)) & 7, fy = (T.fys >> (3 * ky)) & 7, ny = py + fy;
+      const double* col = X + (fx * C + czi) * C + (T.cyb + (ny >> 1) - T.ylo);
+      Y[(fx * 8 + fy) * C + czi] = (ny & 1) ? lagrange_sum<P>(col - H, 1) : col[0];
+    }
+    __syncthreads();
+    // stage Z: the z sum at the listed points, written into the fine block (the next
+    // variable's stage X writes X only after every thread has passed the barrier above, and its
+    // stage Y writes Y only after the barrier that ends that stage X)
+    double* dst = work + (long)T.dst_b * NV * g.Wv + (long)v * g.Wv;
+    for (int e = threadIdx.x; e < T.np; e += PROLONG_TILE_THREADS) {
+      const int c = pts[T.p0 + e];
+      const int fx = c & 7, fy = (c >> 3) & 7, fz = (c >> 6) & 7, nz = pz + fz;
+      const double* col = Y + (fx * 8 + fy) * C + (T.czb + (nz >> 1) - T.zlo);
+      dst[(T.i0 + fx) + sy * (T.j0 + fy) + sz * (T.k0 + fz)] = (nz & 1) ? lagrange_sum<P>(col - H, 1) : col[0];
+    }
+  }
+}
+
 // plain-form RK4 stage updates over the whole state vector (each one fused multiply-add):
 //  kind 0: acc = u + cb k, y = u + ca k   kind 1: acc = acc + cb k, y = u + ca k
 //  kind 2: u = acc + cb k
@@ -367,6 +445,81 @@ static __global__ void exact_state_kernel(double* __restrict__ u, const double* 
 #pragma unroll
   for (int v = 0; v < NV; ++v) q[v * g.S] = v20[v];
 }
+
+// The :fitted target cache's fills (40 fields per block: the target A, then its slope S), at every
+// owned point with r < r_fill about the interior's centre at t_f, zero elsewhere: with u, the
+// snapshot target (snapshot_target_kernel!, src/fit.jl:1189-1212: A = u, S = 0); without, the
+// case's analytic state standing in for the fit of fit_target_kernel! (src/fit.jl:1070-1116): A
+// at t_f (core rule included) and, with dt > 0, S = (A(t_f + dt) - A(t_f - dt)) / (2 dt) as the
+// product with 1 / (2 dt). One analytic evaluation per launch and point: phase 0 writes A (and
+// S = 0), phase 1 parks A(t_f + dt) in the S fields, phase 2 turns them into the slope with
+// A(t_f - dt); the region is always the one at t_f.
+static __global__ void fill_target_kernel(double* __restrict__ tw, const double* __restrict__ u,
+                                          const double* __restrict__ blk, Geo g, long npts, const Case cs,
+                                          double t_f, double r_fill, double dt, int phase) {
+  const long p = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= npts) return;
+  const int b = (int)(p / g.S);
+  const long ip = p - (long)b * g.S;
+  const int k = (int)(ip / ((long)g.N1 * g.N1)), j = (int)((ip / g.N1) % g.N1), i = (int)(ip % g.N1);
+  double x[3];
+  point_pos(blk, b, i, j, k, x);
+  double* o = tw + (long)b * 2 * NV * g.S + ip;
+  if (!(interior_radius(cs, t_f, x) < r_fill)) {
+    if (phase == 0)
+      for (int v = 0; v < 2 * NV; ++v) o[v * g.S] = 0.0;
+    return;
+  }
+  if (u) {
+    const double* q = u + (long)b * NV * g.S + ip;
+    for (int v = 0; v < NV; ++v) {
+      o[v * g.S] = q[v * g.S];
+      o[(NV + v) * g.S] = 0.0;
+    }
+    return;
+  }
+  double a[NV];
+  if (phase == 0) {
+    exact_state(cs, t_f, x, a);
+    for (int v = 0; v < NV; ++v) {
+      o[v * g.S] = a[v];
+      o[(NV + v) * g.S] = 0.0;
+    }
+  } else if (phase == 1) {
+    exact_state(cs, TGH_RADD(t_f, dt), x, a);
+    for (int v = 0; v < NV; ++v) o[(NV + v) * g.S] = a[v];
+  } else {
+    exact_state(cs, TGH_RSUB(t_f, dt), x, a);
+    const double id = TGH_RDIV(1.0, TGH_RMUL(2.0, dt));
+    for (int v = 0; v < NV; ++v) o[(NV + v) * g.S] = TGH_RMUL(id, TGH_RSUB(o[(NV + v) * g.S], a[v]));
+  }
+}
+
+// fitted_state_kernel! (src/fit.jl:1247-1285) without the blend: the background's state where
+// r >= r_1 - d_init, below it the cached target at t, A + (t - t_f) S (each operation rounded, as
+// the oracle forms it)
+static __global__ void fitted_state_kernel(double* __restrict__ u, const double* __restrict__ blk, Geo g, long npts,
+                                           const Case cs, double t, double d_init) {
+  const long p = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= npts) return;
+  const int b = (int)(p / g.S);
+  const long ip = p - (long)b * g.S;
+  const int k = (int)(ip / ((long)g.N1 * g.N1)), j = (int)((ip / g.N1) % g.N1), i = (int)(ip % g.N1);
+  double x[3];
+  point_pos(blk, b, i, j, k, x);
+  double* q = u + (long)b * NV * g.S + ip;
+  if (interior_radius(cs, t, x) >= TGH_RSUB(cs.r1, d_init)) {
+    double v20[NV];
+    rn_background_state(cs, t, x, v20, v20 + NC);
+    for (int v = 0; v < NV; ++v) q[v * g.S] = v20[v];
+    return;
+  }
+  const double* tw = cs.tw + (long)b * 2 * NV * g.S + ip;
+  const double dt = TGH_RSUB(t, *cs.tf);
+  for (int v = 0; v < NV; ++v) q[v * g.S] = TGH_RADD(tw[v * g.S], TGH_RMUL(dt, tw[(NV + v) * g.S]));
+}
+
+static __global__ void set_scalar_kernel(double* dst, double v) { *dst = v; }
 
 // the sampled gauge source at every owned point, through the core rule (src/gauge.jl:156-170)
 static __global__ void sample_gauge_kernel(double* __restrict__ H, const double* __restrict__ blk, Geo g, long npts,

@@ -151,6 +151,12 @@ struct Case {
   double eps, eout, ein, er1, erh, ec0[3], ev[3];
   int interior;
   double ic0[3], iv[3], r0, r1, rho_max, w_ramp, rho_ramp;
+  // :fitted: the target cache (per block 40 fields of the owned points: the target A, the packed
+  // (h, Pi), then its slope S), the fill time t_f (one double in device memory, so that a captured
+  // step graph reads the current one) and whether the target's rate is fed forward
+  const double* tw;
+  const double* tf;
+  int trate;
 };
 
 // g_ab at a spacetime point x = (t, x, y, z), in any scalar type S
@@ -176,6 +182,82 @@ template <class S> TGH_HD void kerr_schild_rest(double M, double a, const S* x, 
   }
 }
 
+template <class S> TGH_HD void ks_rest(double M, double a, const S* x, S g[4][4]) { kerr_schild_rest(M, a, x, g); }
+
+// Kerr (M, a) in horizon-penetrating harmonic coordinates in its rest frame (t = x[0]; the
+// metric does not depend on t): the Kerr-Schild metric pulled back, g = J^T g_KS J, along
+//   X + i Y = w (x + i y),  Z = (r / r_H) z,  T = t + 2 M ln(r_H + sqrt(M^2 - a^2)),
+//   w = (r + i a) / (r_H + i a),  r = r_H + M,
+// r_H the spheroidal radius of (x, y, z) with parameter a (the Kerr-Schild quartic). Both charts
+// share the Kerr-Schild angle; the harmonic radius is the Boyer-Lindquist radius minus M, and the
+// harmonic time t_BL + 2 M r_+ int dr / Delta is regular on the future horizon. J comes in closed
+// form from d r_H / d x^i = r_H (x_i r_H^2 + a^2 z delta_iz) / (r_H^4 + a^2 z^2), so the metric's
+// derivatives come from S's own (forward-mode numbers). Every coordinate function is harmonic
+// (H_a = 0); at a = 0 this is the harmonic Schwarzschild metric g_tt = -(r - M)/(r + M),
+// g_tr = 4 M^2 / (r + M)^2. The operations are the oracle's, one by one (with a rounded S the
+// result is the oracle's bit for bit).
+template <class S> TGH_HD void harmonic_kerr_rest(double M, double a, const S* x, S g[4][4]) {
+  const S X = x[1], Y = x[2], Z = x[3];
+  const S rho2 = X * X + Y * Y + Z * Z;
+  const S a2 = cst<S>(TGH_RMUL(a, a));
+  const S half = cst<S>(0.5) * (rho2 - a2);
+  const S r2 = half + dsqrt(half * half + a2 * Z * Z);
+  const S rh = dsqrt(r2);
+  const S q = r2 * r2 + a2 * Z * Z;
+  const S dr[3] = {rh * (X * r2) / q, rh * (Y * r2) / q, rh * (Z * r2 + a2 * Z) / q};
+  const S r = rh + cst<S>(M);
+  const S D = r2 + a2;
+  const S wr = (r * rh + a2) / D;
+  const S wi = cst<S>(-TGH_RMUL(a, M)) / D;
+  const S D2 = D * D;
+  const S dwr = cst<S>(-M) * (r2 - a2) / D2;
+  const S dwi = cst<S>(TGH_RMUL(TGH_RMUL(2.0, M), a)) * rh / D2;
+  const S px = X * dwr - Y * dwi;
+  const S py = X * dwi + Y * dwr;
+  const S zr = r / rh;
+  const S zd = cst<S>(-M) * Z / r2;
+  const S tr = cst<S>(TGH_RMUL(2.0, M)) / (rh + cst<S>(TGH_RSQRT(TGH_RSUB(TGH_RMUL(M, M), TGH_RMUL(a, a)))));
+  const S xk[4] = {x[0], wr * X - wi * Y, wr * Y + wi * X, zr * Z};
+  S J[4][4];
+  J[0][0] = cst<S>(1.0);
+  J[1][0] = J[2][0] = J[3][0] = cst<S>(0.0);
+#pragma unroll
+  for (int j = 0; j < 3; ++j) {
+    J[0][j + 1] = tr * dr[j];
+    J[1][j + 1] = px * dr[j];
+    J[2][j + 1] = py * dr[j];
+    J[3][j + 1] = zd * dr[j];
+  }
+  J[1][1] = wr + J[1][1];
+  J[1][2] = J[1][2] - wi;
+  J[2][1] = wi + J[2][1];
+  J[2][2] = wr + J[2][2];
+  J[3][3] = zr + J[3][3];
+  S gk[4][4];
+  ks_rest(M, a, xk, gk);
+#pragma unroll
+  for (int p = 0; p < 4; ++p)
+#pragma unroll
+    for (int s = 0; s < 4; ++s) {
+      S acc = cst<S>(0.0);
+#pragma unroll
+      for (int A = 0; A < 4; ++A) {
+        S t = J[0][s] * gk[A][0];
+#pragma unroll
+        for (int B = 1; B < 4; ++B) t = t + J[B][s] * gk[A][B];
+        acc = acc + J[A][p] * t;
+      }
+      g[p][s] = acc;
+    }
+}
+
+template <class S> TGH_HD void hole_rest(const Case& c, const S* x, S g[4][4]) {
+  if (c.bg.kind == TGH_BG_HARMONIC_KERR)
+    harmonic_kerr_rest(c.bg.M, c.bg.a, x, g);
+  else
+    kerr_schild_rest(c.bg.M, c.bg.a, x, g);
+}
+
 template <class S> TGH_HD void metric(const Case& c, const S* xin, S g[4][4]) {
   S x[4];
 #pragma unroll
@@ -194,16 +276,16 @@ template <class S> TGH_HD void metric(const Case& c, const S* xin, S g[4][4]) {
     g[0][1] = -psi;
     g[1][0] = -psi;
     g[1][1] = cst<S>(1.0) - psi * psi;
-  } else if (c.bg.kind == TGH_BG_KERR_SCHILD) {
+  } else if (c.bg.kind == TGH_BG_KERR_SCHILD || c.bg.kind == TGH_BG_HARMONIC_KERR) {
     if (!c.boosted) {
-      kerr_schild_rest(c.bg.M, c.bg.a, x, g);
+      hole_rest(c, x, g);
     } else {
       S xr[4], gr[4][4];
 #pragma unroll
       for (int i = 0; i < 4; ++i)
         xr[i] = cst<S>(c.L[i][0]) * x[0] + cst<S>(c.L[i][1]) * x[1] + cst<S>(c.L[i][2]) * x[2] +
                 cst<S>(c.L[i][3]) * x[3];
-      kerr_schild_rest(c.bg.M, c.bg.a, xr, gr);
+      hole_rest(c, xr, gr);
 #pragma unroll
       for (int a = 0; a < 4; ++a)
 #pragma unroll

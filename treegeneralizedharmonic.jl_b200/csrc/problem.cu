@@ -72,6 +72,11 @@ struct tgh_problem {
   // device buffers
   double* work = nullptr;     // the ghosted working array (also W0 of the batched form)
   double* Hsrc = nullptr;
+  // :fitted: the target cache (per own block 40 fields of the owned points), its fill time on the
+  // device, and whether a fill or a set has happened since creation
+  double* tw = nullptr;
+  double* tf = nullptr;
+  bool target_set = false;
   double* blk = nullptr;      // per block: domain lo (3), h, integer corner (3), pad
   uint8_t* primary = nullptr; // per owned point: 1 where this block holds the primary copy
   CopyRun* runs = nullptr;
@@ -91,6 +96,11 @@ struct tgh_problem {
   bool capturing = false;
   std::vector<ProlongPt*> prol;  // per level 1..maxlevel
   std::vector<int> nprol;
+  // the same prolongation as tiles of 8^3 fine points (fill_prolong_tile_kernel), per level;
+  // ntile[l] < 0: the level's points do not tile (the per-point kernel runs)
+  std::vector<ProlongTile*> ptile;
+  std::vector<unsigned short*> ptpts;
+  std::vector<int> ntile;
   unsigned long long* scratch = nullptr;  // speed reduction: max bits, non-finite count
   unsigned long long* bcounts = nullptr;  // the range projection's counts: fired, non-finite, max r bits
   // the range projection the limiters apply (set by tgh_set_bounds), and its accounting
@@ -239,7 +249,7 @@ static Case make_case(const tgh_config& c) {
   k.bg = c.bg;
   const double* u = c.bg.boost;
   const double u2 = u[0] * u[0] + u[1] * u[1] + u[2] * u[2];
-  k.boosted = (c.bg.kind == TGH_BG_KERR_SCHILD && u2 > 0.0) ? 1 : 0;
+  k.boosted = ((c.bg.kind == TGH_BG_KERR_SCHILD || c.bg.kind == TGH_BG_HARMONIC_KERR) && u2 > 0.0) ? 1 : 0;
   const double gam = 1.0 / std::sqrt(1.0 - u2);
   for (int i = 0; i < 4; ++i)
     for (int j = 0; j < 4; ++j) k.L[i][j] = i == j ? 1.0 : 0.0;
@@ -438,6 +448,8 @@ static bool plan_rank(const tgh_problem* p, int r, bool entries, HostPlan& hp, s
 // The plan of this problem's rank on the device, with the exchange lists: what this rank
 // receives into its halo (its own requests) and what it sends (every other rank's requests
 // to it, found by planning that rank's leaves: both sides derive the same sorted list).
+static bool tile_prolongation(const tgh_problem* p, const HostPlan& hp, const std::vector<ProlongPt>& pts,
+                              std::vector<ProlongTile>& tiles, std::vector<unsigned short>& codes);
 static int build_plan(tgh_problem* p) {
   HostPlan hp;
   std::string err;
@@ -502,13 +514,142 @@ static int build_plan(tgh_problem* p) {
     if (!prol[l].empty())
       CK(cudaMemcpy(p->prol[l], prol[l].data(), prol[l].size() * sizeof(ProlongPt), cudaMemcpyHostToDevice));
   }
+  p->ptile.assign(p->maxlevel + 1, nullptr);
+  p->ptpts.assign(p->maxlevel + 1, nullptr);
+  p->ntile.assign(p->maxlevel + 1, -1);
+  for (int l = 1; l <= p->maxlevel; ++l) {
+    std::vector<ProlongTile> tiles;
+    std::vector<unsigned short> codes;
+    if (prol[l].empty() || !tile_prolongation(p, hp, prol[l], tiles, codes)) continue;
+    p->ntile[l] = (int)tiles.size();
+    CK(cudaMalloc(&p->ptile[l], tiles.size() * sizeof(ProlongTile)));
+    CK(cudaMemcpy(p->ptile[l], tiles.data(), tiles.size() * sizeof(ProlongTile), cudaMemcpyHostToDevice));
+    CK(cudaMalloc(&p->ptpts[l], codes.size() * sizeof(unsigned short)));
+    CK(cudaMemcpy(p->ptpts[l], codes.data(), codes.size() * sizeof(unsigned short), cudaMemcpyHostToDevice));
+  }
   CK(cudaMalloc(&p->primary, (size_t)p->npts));
   CK(cudaMemcpy(p->primary, prim.data(), (size_t)p->npts, cudaMemcpyHostToDevice));
   return TGH_OK;
 }
 
+// The tiles of one level's prolonged points (fill_prolong_tile_kernel): the points of one fine
+// block whose stencils lie in one coarse block, grouped by the 8^3 box of fine offsets from the
+// block's corner that holds them. Per tile the coarse centre of fine offset 0 and the coarse rows
+// its points' y and z stencils cover. The coarse centre of a point is its stencil base plus P/2 - 1
+// along an interpolating axis. False (the per-point kernel then runs) when a tile's points do not
+// share one mapping from fine offsets to coarse centres (a periodic wrap inside a tile) or its rows
+// exceed the kernel's shared arrays.
+static bool tile_prolongation(const tgh_problem* p, const HostPlan& hp, const std::vector<ProlongPt>& pts,
+                              std::vector<ProlongTile>& tiles, std::vector<unsigned short>& codes) {
+  const int P = p->q + 2, H = P / 2 - 1, C = P + 4, Wx = p->Wx, Wd = p->Wd, G = p->G;
+  if ((long)p->nwb >= (1L << 20)) return false;
+  auto fdiv8 = [](int r) { return r >= 0 ? r / 8 : -((-r + 7) / 8); };
+  struct Acc {
+    ProlongTile t;
+    int ylo, yhi, zlo, zhi, fxm, fym;
+    std::vector<unsigned short> c;
+  };
+  std::unordered_map<unsigned long long, int> index;
+  std::vector<Acc> acc;
+  for (const ProlongPt& q : pts) {
+    const int fi[3] = {q.dst_w % Wx, (q.dst_w / Wx) % Wd, q.dst_w / (Wx * Wd)};
+    const int sb[3] = {q.src_w % Wx, (q.src_w / Wx) % Wd, q.src_w / (Wx * Wd)};
+    int t[3], f[3], par[3], ctr[3];
+    for (int d = 0; d < 3; ++d) {
+      const int r = fi[d] - G;
+      t[d] = fdiv8(r);
+      f[d] = r - 8 * t[d];
+      const int odd = (q.odd >> d) & 1;
+      par[d] = (odd + f[d]) & 1;  // the parity of the tile origin's fine lattice index
+      ctr[d] = sb[d] + (odd ? H : 0);
+    }
+    const unsigned long long key = (unsigned long long)q.dst_b << 44 | (unsigned long long)q.src_b << 24 |
+                                   (unsigned long long)(t[0] + 8) << 16 | (unsigned long long)(t[1] + 8) << 8 |
+                                   (unsigned long long)(t[2] + 8);
+    if (t[0] + 8 < 0 || t[0] + 8 > 255 || t[1] + 8 < 0 || t[1] + 8 > 255 || t[2] + 8 < 0 || t[2] + 8 > 255) return false;
+    auto it = index.find(key);
+    int a;
+    if (it == index.end()) {
+      a = (int)acc.size();
+      index.emplace(key, a);
+      Acc n{};
+      n.t.dst_b = q.dst_b;
+      n.t.src_b = q.src_b;
+      n.t.i0 = (short)(8 * t[0] + G);
+      n.t.j0 = (short)(8 * t[1] + G);
+      n.t.k0 = (short)(8 * t[2] + G);
+      n.t.par = (unsigned char)(par[0] | par[1] << 1 | par[2] << 2);
+      n.t.cxb = (short)(ctr[0] - ((par[0] + f[0]) >> 1));
+      n.t.cyb = (short)(ctr[1] - ((par[1] + f[1]) >> 1));
+      n.t.czb = (short)(ctr[2] - ((par[2] + f[2]) >> 1));
+      n.ylo = n.zlo = 1 << 30;
+      n.yhi = n.zhi = -(1 << 30);
+      acc.push_back(std::move(n));
+    } else {
+      a = it->second;
+    }
+    Acc& A = acc[a];
+    const short cb[3] = {A.t.cxb, A.t.cyb, A.t.czb};
+    for (int d = 0; d < 3; ++d)
+      if (((A.t.par >> d) & 1) != par[d] || cb[d] + ((par[d] + f[d]) >> 1) != ctr[d]) return false;
+    const int oy = (q.odd >> 1) & 1, oz = (q.odd >> 2) & 1;
+    A.ylo = std::min(A.ylo, ctr[1] - (oy ? H : 0));
+    A.yhi = std::max(A.yhi, ctr[1] + (oy ? P / 2 : 0));
+    A.zlo = std::min(A.zlo, ctr[2] - (oz ? H : 0));
+    A.zhi = std::max(A.zhi, ctr[2] + (oz ? P / 2 : 0));
+    A.fxm |= 1 << f[0];
+    A.fym |= 1 << f[1];
+    A.c.push_back((unsigned short)(f[0] | f[1] << 3 | f[2] << 6));
+  }
+  tiles.reserve(acc.size());
+  codes.reserve(pts.size());
+  for (Acc& A : acc) {
+    const int cyn = A.yhi - A.ylo + 1, czn = A.zhi - A.zlo + 1;
+    if (cyn > C || czn > C) return false;
+    // every coarse value stage X reads lies in the coarse block's working array
+    if (A.ylo < 0 || A.yhi >= Wd || A.zlo < 0 || A.zhi >= Wd) return false;
+    for (int x = 0; x < 8; ++x) {
+      if (!(A.fxm >> x & 1)) continue;
+      const int nx = (A.t.par & 1) + x, c = A.t.cxb + (nx >> 1);
+      if ((nx & 1) ? (c - H < 0 || c - H + P > Wd) : (c < 0 || c >= Wd)) return false;
+    }
+    A.t.ylo = (short)A.ylo;
+    A.t.zlo = (short)A.zlo;
+    A.t.cyn = (unsigned char)cyn;
+    A.t.czn = (unsigned char)czn;
+    int n = 0;
+    A.t.fxs = 0;
+    for (int x = 0; x < 8; ++x)
+      if (A.fxm >> x & 1) A.t.fxs |= x << (3 * n++);
+    A.t.nfx = (unsigned char)n;
+    n = 0;
+    A.t.fys = 0;
+    for (int y = 0; y < 8; ++y)
+      if (A.fym >> y & 1) A.t.fys |= y << (3 * n++);
+    A.t.nfy = (unsigned char)n;
+    A.t.p0 = (int)codes.size();
+    A.t.np = (int)A.c.size();
+    codes.insert(codes.end(), A.c.begin(), A.c.end());
+    tiles.push_back(A.t);
+  }
+  (void)hp;
+  return true;
+}
+
 // Level l's prolongation into `work` (the weights of order P are compile-time constants).
 static cudaError_t launch_prolong(tgh_problem* p, int l, double* work) {
+  if (l < (int)p->ntile.size() && p->ntile[l] > 0) {
+    const int n = p->ntile[l];
+    const ProlongTile* t = p->ptile[l];
+    const unsigned short* c = p->ptpts[l];
+    switch (p->q + 2) {
+      case 4: fill_prolong_tile_kernel<4><<<n, PROLONG_TILE_THREADS, 0, p->stream>>>(t, c, work, p->geo); break;
+      case 6: fill_prolong_tile_kernel<6><<<n, PROLONG_TILE_THREADS, 0, p->stream>>>(t, c, work, p->geo); break;
+      case 8: fill_prolong_tile_kernel<8><<<n, PROLONG_TILE_THREADS, 0, p->stream>>>(t, c, work, p->geo); break;
+      default: fill_prolong_tile_kernel<10><<<n, PROLONG_TILE_THREADS, 0, p->stream>>>(t, c, work, p->geo); break;
+    }
+    return cudaGetLastError();
+  }
   const int T = 256;
   const long n = (long)p->nprol[l] * NV;
   switch (p->q + 2) {
@@ -641,7 +782,17 @@ static int interior_blocks(tgh_problem* p, tgh_problem::BlockList& L, double tlo
 
 // One right-hand side over all blocks on the problem's stream: the interior's points (a problem
 // with an interior, over the blocks of the list in use), the head kernel, then the Pi kernel.
+// a :fitted interior relaxes toward the target cache, which must have been filled or set
+// (GHProblem refuses a :fitted interior without its target, src/evolution.jl:1132-1136)
+static int fitted_ready(tgh_problem* p) {
+  if (p->cfg.interior == TGH_INT_FITTED && !p->target_set)
+    return fail(p, TGH_ERR_ARG, "a :fitted interior relaxes toward the target cache: fill or set it first "
+                                "(tgh_set_target, tgh_fill_target_snapshot, tgh_fill_target_analytic)");
+  return TGH_OK;
+}
+
 static int launch_interior(tgh_problem* p, const RhsArgs& a, int mode, cudaStream_t s) {
+  if (int st = fitted_ready(p)) return st;
   const tgh_problem::BlockList* L = p->ilist_use;
   if (!L) {
     // a direct launch: the list for this t
@@ -851,6 +1002,12 @@ static int setup_host(tgh_problem* p, const tgh_config* cfg, const tgh_mesh* m, 
   p->Wv = (long)p->Wx * p->Wd * p->Wd;
   p->npts = p->S * p->nb;
   p->geo = Geo{p->N1, p->Wd, p->G, p->Wx, p->S, p->Wv};
+  if (cfg->bg.kind < TGH_BG_MINKOWSKI || cfg->bg.kind > TGH_BG_HARMONIC_KERR)
+    return fail(p, TGH_ERR_ARG, "unknown background kind");
+  if (cfg->interior < TGH_INT_NONE || cfg->interior > TGH_INT_FITTED)
+    return fail(p, TGH_ERR_ARG, "unknown interior variant");
+  if (cfg->bg.kind == TGH_BG_HARMONIC_KERR && !(std::fabs(cfg->bg.a) < cfg->bg.M))
+    return fail(p, TGH_ERR_ARG, "the harmonic chart needs |a| < M (its time function has a log at r_-)");
   p->cs = make_case(*cfg);
   p->diss = cfg->dissipation == TGH_DISS_CONSTANT ? cfg->eps_ko != 0.0 : !(cfg->eps_out == 0.0 && cfg->eps_in == 0.0);
   p->intr = cfg->interior != TGH_INT_NONE;
@@ -867,7 +1024,8 @@ static int setup_host(tgh_problem* p, const tgh_config* cfg, const tgh_mesh* m, 
       const double hmin = std::ldexp(p->h0, -p->maxlevel);
       if (cfg->r1 - cfg->r0 < 2.0 * (p->G + 1) * hmin)
         return fail(p, TGH_ERR_RADII, "the damping layer is too thin: r_1 - r_0 < 2(G+1)h");
-      if (cfg->bg.kind == TGH_BG_KERR_SCHILD && cfg->r0 <= std::fabs(cfg->bg.a))
+      if ((cfg->bg.kind == TGH_BG_KERR_SCHILD || cfg->bg.kind == TGH_BG_HARMONIC_KERR) &&
+          cfg->r0 <= std::fabs(cfg->bg.a))
         return fail(p, TGH_ERR_RADII, "the frozen core does not contain the chart's singular disk |x| <= |a|");
     }
   }
@@ -880,7 +1038,8 @@ static int setup_host(tgh_problem* p, const tgh_config* cfg, const tgh_mesh* m, 
 static bool stationary(const tgh_config& c) {
   const double* u = c.bg.boost;
   const bool bg = c.bg.kind == TGH_BG_MINKOWSKI || c.bg.kind == TGH_BG_SHIFTED_MINKOWSKI ||
-                  (c.bg.kind == TGH_BG_KERR_SCHILD && u[0] == 0.0 && u[1] == 0.0 && u[2] == 0.0);
+                  ((c.bg.kind == TGH_BG_KERR_SCHILD || c.bg.kind == TGH_BG_HARMONIC_KERR) && u[0] == 0.0 &&
+                   u[1] == 0.0 && u[2] == 0.0);
   const bool core = c.interior == TGH_INT_NONE || (c.int_v[0] == 0.0 && c.int_v[1] == 0.0 && c.int_v[2] == 0.0);
   return bg && core;
 }
@@ -922,6 +1081,16 @@ static int setup_device(tgh_problem* p) {
     sample_gauge_kernel<<<grid_for(p->npts, 64), 64, 0, p->stream>>>(p->Hsrc, p->blk, p->geo, p->npts, p->cs, 0.0);
     CK(cudaGetLastError());
   }
+  if (cfg->interior == TGH_INT_FITTED) {
+    const size_t L = (size_t)p->S * 2 * NV * p->nb;
+    CK(cudaMalloc(&p->tw, L * sizeof(double)));
+    CK(cudaMemsetAsync(p->tw, 0, L * sizeof(double), p->stream));
+    CK(cudaMalloc(&p->tf, sizeof(double)));
+    CK(cudaMemsetAsync(p->tf, 0, sizeof(double), p->stream));
+    p->cs.tw = p->tw;
+    p->cs.tf = p->tf;
+    p->cs.trate = cfg->target_rate != 0;
+  }
   CK(cudaStreamSynchronize(p->stream));
   return TGH_OK;
 }
@@ -947,7 +1116,7 @@ void tgh_problem_destroy(tgh_problem* p) {
     if (x.send) cudaFree(x.send);
     if (x.recv) cudaFree(x.recv);
   }
-  void* bufs[] = {p->work, p->Hsrc, p->blk, p->primary, p->runs, p->gpts, p->hooks, p->hook_cache, p->scratch,
+  void* bufs[] = {p->work, p->Hsrc, p->tw, p->tf, p->blk, p->primary, p->runs, p->gpts, p->hooks, p->hook_cache, p->scratch,
                   p->bcounts, p->dev_err, p->ilist.dev, p->ilist_graph.dev,
                   p->part, p->coef, p->diag, p->dpart, p->ind, p->ind_tol, p->ind_counts, p->ind_boxes,
                   p->k, p->acc, p->y, p->u0, p->W1, p->W2, p->bacc, p->twork, p->kt, p->acct, p->yt,
@@ -956,6 +1125,10 @@ void tgh_problem_destroy(tgh_problem* p) {
   for (void* b : bufs)
     if (b) cudaFree(b);
   for (auto* pp : p->prol)
+    if (pp) cudaFree(pp);
+  for (auto* pp : p->ptile)
+    if (pp) cudaFree(pp);
+  for (auto* pp : p->ptpts)
     if (pp) cudaFree(pp);
   delete p;
 }
@@ -1345,6 +1518,64 @@ int tgh_initial_state(tgh_problem* p, double* u, double t) {
   return stage_limit_impl(p, u, t);
 }
 
+// ---- the :fitted target cache ----
+
+static int fitted_check(tgh_problem* p) {
+  if (!p) return TGH_ERR_ARG;
+  if (p->cfg.interior != TGH_INT_FITTED) return fail(p, TGH_ERR_ARG, "the problem's interior is not :fitted");
+  return TGH_OK;
+}
+
+int tgh_set_target(tgh_problem* p, const double* tw, double t_f) {
+  if (int s = fitted_check(p)) return s;
+  if (!tw || !std::isfinite(t_f)) return fail(p, TGH_ERR_ARG, "tgh_set_target needs a cache and a finite t_f");
+  CK(cudaMemcpyAsync(p->tw, tw, (size_t)p->S * 2 * NV * p->nb * sizeof(double), cudaMemcpyDeviceToDevice, p->stream));
+  set_scalar_kernel<<<1, 1, 0, p->stream>>>(p->tf, t_f);
+  CK(cudaGetLastError());
+  p->target_set = true;
+  return TGH_OK;
+}
+
+static int fill_target_impl(tgh_problem* p, const double* u, double t_f, double r_fill, double dt) {
+  if (int s = fitted_check(p)) return s;
+  if (!std::isfinite(t_f) || !(r_fill >= 0.0) || !(dt >= 0.0))
+    return fail(p, TGH_ERR_ARG, "the fill needs a finite t_f, r_fill >= 0 and dt >= 0");
+  const int phases = (!u && dt > 0.0) ? 3 : 1;
+  for (int ph = 0; ph < phases; ++ph)
+    fill_target_kernel<<<grid_for(p->npts, 128), 128, 0, p->stream>>>(p->tw, u, p->blk, p->geo, p->npts, p->cs,
+                                                                      t_f, r_fill, dt, ph);
+  set_scalar_kernel<<<1, 1, 0, p->stream>>>(p->tf, t_f);
+  CK(cudaGetLastError());
+  p->target_set = true;
+  return TGH_OK;
+}
+
+int tgh_fill_target_snapshot(tgh_problem* p, const double* u, double t_f, double r_fill) {
+  if (!u) return fail(p, TGH_ERR_ARG, "the snapshot target needs a state");
+  return fill_target_impl(p, u, t_f, r_fill, 0.0);
+}
+
+int tgh_fill_target_analytic(tgh_problem* p, double t_f, double r_fill, double dt) {
+  return fill_target_impl(p, nullptr, t_f, r_fill, dt);
+}
+
+int tgh_fitted_initial_state(tgh_problem* p, double* u, double t, double d_init) {
+  if (int s = fitted_check(p)) return s;
+  if (int s = fitted_ready(p)) return s;
+  if (!u || !(d_init >= 0.0 && d_init <= p->cfg.r1 - p->cfg.r0))
+    return fail(p, TGH_ERR_ARG, "the fitted initial state needs a state and 0 <= d_init <= r_1 - r_0");
+  fitted_state_kernel<<<grid_for(p->npts, 128), 128, 0, p->stream>>>(u, p->blk, p->geo, p->npts, p->cs, t, d_init);
+  CK(cudaGetLastError());
+  return TGH_OK;
+}
+
+int tgh_copy_target(tgh_problem* p, double* out) {
+  if (int s = fitted_check(p)) return s;
+  if (!out) return fail(p, TGH_ERR_ARG, "tgh_copy_target needs a destination");
+  CK(cudaMemcpyAsync(out, p->tw, (size_t)p->S * 2 * NV * p->nb * sizeof(double), cudaMemcpyDeviceToDevice, p->stream));
+  return TGH_OK;
+}
+
 int tgh_max_speed(tgh_problem* p, const double* u, double t, double* lambda) {
   CK(cudaMemsetAsync(p->scratch, 0, 2 * sizeof(unsigned long long), p->stream));
   speed_kernel<<<grid_for(p->npts, 128), 128, 0, p->stream>>>(u, p->blk, p->geo, p->npts, p->cs, t, p->scratch);
@@ -1565,6 +1796,7 @@ int tgh_step_batched(tgh_problem* p, double* u, double t, double dt, int nsteps)
   if (p->cfg.interior == TGH_INT_PASTED)
     return fail(p, TGH_ERR_ARG, "the batched form has no :pasted limiter; use tgh_rk4_step");
   if (p->has_bounds) return fail(p, TGH_ERR_ARG, "the batched form has no range projection; use tgh_rk4_step");
+  if (int st = fitted_ready(p)) return st;
   int s = batched_buffers(p);
   if (s) return s;
   // the state into W0's owned points (and ghosts), outside the graph
@@ -1730,6 +1962,7 @@ int tgh_shard_begin(tgh_problem* p, const double* u) {
   if (p->cfg.interior == TGH_INT_PASTED)
     return fail(p, TGH_ERR_ARG, "the batched form has no :pasted limiter; use tgh_rk4_step");
   if (p->has_bounds) return fail(p, TGH_ERR_ARG, "the batched form has no range projection; use tgh_rk4_step");
+  if (int st = fitted_ready(p)) return st;
   int s = batched_buffers(p);
   if (s) return s;
   work_overwritten(p, "the sharded step");
@@ -1872,7 +2105,7 @@ static int tangent_check(tgh_problem* p, int dir) {
   if (dir < TAN_STATE || dir > TAN_DAMP_NEAR) return fail(p, TGH_ERR_ARG, "unknown tangent direction");
   if (p->nranks > 1) return fail(p, TGH_ERR_ARG, "the tangent-linear form runs on one rank");
   if (p->mixed) return fail(p, TGH_ERR_ARG, "the tangent-linear form is FP64");
-  if (p->intr && (core_follows(p->cs) || p->cfg.interior == TGH_INT_PASTED))
+  if (p->intr && (core_follows(p->cs) || p->cfg.interior == TGH_INT_PASTED || p->cfg.interior == TGH_INT_FITTED))
     return fail(p, TGH_ERR_ARG, "the tangent-linear form takes a static :damped or :frozen interior");
   const size_t L = tgh_state_length(p), Lw = work_doubles(p);
   if (!p->twork) {
@@ -1972,7 +2205,7 @@ int tgh_tangent_error_norm(tgh_problem* p, const double* u, const double* ut, do
 static int adjoint_check(tgh_problem* p) {
   if (p->nranks > 1) return fail(p, TGH_ERR_ARG, "the adjoint form runs on one rank");
   if (p->mixed) return fail(p, TGH_ERR_ARG, "the adjoint form is FP64");
-  if (p->intr && (core_follows(p->cs) || p->cfg.interior == TGH_INT_PASTED))
+  if (p->intr && (core_follows(p->cs) || p->cfg.interior == TGH_INT_PASTED || p->cfg.interior == TGH_INT_FITTED))
     return fail(p, TGH_ERR_ARG, "the adjoint form takes a static :damped or :frozen interior");
   if (p->has_bounds) return fail(p, TGH_ERR_ARG, "the adjoint form does not differentiate the range projection");
   const size_t L = tgh_state_length(p);

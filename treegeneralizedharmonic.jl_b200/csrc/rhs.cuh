@@ -437,6 +437,38 @@ __global__ void __launch_bounds__(128) interior_kernel(const Case cs, const RhsA
     else es.put(v, val);
   };
   const bool frozen = cs.interior == TGH_INT_PASTED ? r < cs.r1 : r < cs.r0;
+  if (cs.interior == TGH_INT_FITTED) {
+    // the :fitted branches (src/evolution.jl:528-548, 619-653): the target A + (t - t_f) S read
+    // from the cache at the point (two loads a variable), its rate S fed forward with
+    // target_rate; the core relaxes at rho_max, the layer's parts are parked as above
+    const double* tw = cs.tw + (long)q.b * (2 * NV) * S + q.ip;
+    const double dt = A.t - *cs.tf;
+    if (frozen) {
+      const double rc = cs.rho_max;
+      for (int v = 0; v < NV; ++v) {
+        const double sl = tw[(NV + v) * S];
+        const double tg = tw[v * S] + dt * sl;
+        put(v, cs.trate ? sl - rc * (wk[v * sv] - tg) : -(rc * (wk[v * sv] - tg)));
+      }
+      return;
+    }
+    double w, rho;
+    layer_profiles(cs, r, w, rho);
+    const double om = 1.0 - w;
+    double* dD = MODE == MODE_DU ? ed.d : cfo + CF_DTH0 * A.npts;
+    double* dT = MODE == MODE_DU ? ed.d + NC * S : es.nx + NC * sv;
+    const long sD = MODE == MODE_DU ? S : A.npts, sT = MODE == MODE_DU ? S : sv;
+    for (int v = 0; v < NV; ++v) {
+      const double sl = tw[(NV + v) * S];
+      const double tg = tw[v * S] + dt * sl;
+      const double val = cs.trate ? om * sl - rho * (wk[v * sv] - tg) : -(rho * (wk[v * sv] - tg));
+      if (v < NC)
+        dD[v * sD] = val;
+      else
+        dT[(v - NC) * sT] = val;
+    }
+    return;
+  }
   if (!frozen) {
     double w, rho;
     layer_profiles(cs, r, w, rho);

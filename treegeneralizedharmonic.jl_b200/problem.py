@@ -142,6 +142,44 @@ class GHProblem:
         self._check(self.lib.tgh_initial_state(self._h, _ptr(u), float(t)))
         return u
 
+    # ---- the :fitted target cache (src/fit.jl:1030-1285) ----
+
+    def target_length(self):
+        """Doubles in the target cache: 40 fields of (N+1)^3 owned points per block."""
+        return 2 * self.state_length
+
+    def default_fill_radius(self):
+        """r_fill of fill_target! for the sphere interior: r_1 plus the finest spacing (the layer's
+        outer radius plus one cell, src/fit.jl:1147)."""
+        it = self.case.interior
+        return it["r1"] + self.forest.h0 / 2 ** int(self.forest.level.max())
+
+    def set_target(self, tw, t_f):
+        """The cache from a device array of target_length() doubles (A then S per block)."""
+        self._check(self.lib.tgh_set_target(self._h, _ptr(tw), float(t_f)))
+
+    def fill_target_snapshot(self, u, t_f, r_fill=None):
+        """fill_snapshot!: A = u, S = 0 inside r_fill at t_f, zero elsewhere."""
+        r = self.default_fill_radius() if r_fill is None else float(r_fill)
+        self._check(self.lib.tgh_fill_target_snapshot(self._h, _ptr(u), float(t_f), r))
+
+    def fill_target_analytic(self, t_f, r_fill=None, dt=0.0):
+        """The case's analytic state at t_f in place of a fit, S its centred difference over dt."""
+        r = self.default_fill_radius() if r_fill is None else float(r_fill)
+        self._check(self.lib.tgh_fill_target_analytic(self._h, float(t_f), r, float(dt)))
+
+    def fitted_initial_state(self, u, t, d_init=0.0):
+        """fitted_state_kernel! without the blend: the background outside r_1 - d_init, the cached
+        target inside."""
+        self._check(self.lib.tgh_fitted_initial_state(self._h, _ptr(u), float(t), float(d_init)))
+        return u
+
+    def target(self):
+        """A copy of the target cache (a device tensor of target_length() doubles)."""
+        out = torch.empty(self.target_length(), dtype=torch.float64, device="cuda")
+        self._check(self.lib.tgh_copy_target(self._h, _ptr(out)))
+        return out
+
     def gh_dt(self, u, cfl=0.25, t=0.0):
         """cfl * h_min / lambda_max (src/evolution.jl:1509-1519)."""
         hmin = self.forest.h0 / 2 ** (self.forest.nlevels - 1)

@@ -80,15 +80,16 @@ def block_extent(forest, b):
 
 
 def horizon_radii(case):
-    """(r_h,min, r_h,max): the smallest and largest coordinate radius of the Kerr-Schild horizon
+    """(r_h,min, r_h,max): the smallest and largest coordinate radius of the hole's horizon
     about the hole's center (src/interior.jl:756-800). A boost contracts the rest frame's
     horizon ellipsoid x^T A x = 1 along the velocity; the smallest radius is then
     1 / sqrt(largest eigenvalue of L A L), L the boost's spatial matrix."""
     bg = case.background
-    if bg.get("kind") != "kerr_schild":
-        raise ValueError("the level floor needs a hole: a Kerr-Schild background")
+    if bg.get("kind") not in ("kerr_schild", "harmonic_kerr"):
+        raise ValueError("the level floor needs a hole: a Kerr-Schild or harmonic Kerr background")
     M, a = bg["M"], bg.get("a", 0.0)
-    r_min = M + math.sqrt(M * M - a * a)
+    # the horizon's spheroidal radius: r_+ in Kerr-Schild, r_+ - M in the harmonic chart
+    r_min = (M if bg["kind"] == "kerr_schild" else 0.0) + math.sqrt(M * M - a * a)
     r_max = math.sqrt(r_min * r_min + a * a)
     v = np.array(bg.get("boost", (0.0, 0.0, 0.0)), dtype=float)
     b2 = float(v @ v)
