@@ -238,12 +238,13 @@ struct ProlongTile {
   int dst_b, src_b;
   short i0, j0, k0;     // the fine working-array coordinates of the tile's origin (may lie below 0)
   short cxb, cyb, czb;  // coarse working-array coordinate of the centre of fine offset 0
+  short xlo, xhi;       // the coarse x its listed points' stencils read
   short ylo, zlo;       // the coarse rows stage X covers: [ylo, ylo + cyn) x [zlo, zlo + czn)
   unsigned char cyn, czn;
   unsigned char par;    // bit d: the fine lattice index of the origin is odd along axis d
-  unsigned char nfx, nfy;
-  unsigned char pad;
-  int fxs, fys;         // the fine x (y) offsets holding listed points, 3 bits each, nfx (nfy) of them
+  unsigned char fxm, fym;  // the fine x (y) offsets holding listed points, a bit each
+  unsigned char nfx;
+  int fxs;              // the same fine x offsets as a list, 3 bits each
   int p0, np;           // the listed points: pts[p0 .. p0 + np), fx | fy << 3 | fz << 6
 };
 
@@ -256,38 +257,70 @@ __device__ __forceinline__ double lagrange_sum(const double* v, int stride) {
   return s;
 }
 
-// One CTA per tile, its threads on one variable at a time (the two stages' arrays are one
-// variable's, at most 19.7 KB at P = 10, so that several CTAs share an SM and hide the stages'
-// load and reduction latency).
+// The partial sums along one axis at the 8 fine offsets of a tile from P + 3 consecutive coarse
+// values v (v[0] at the centre of fine offset 0 minus P/2 - 1): offset f, with the origin's parity
+// PAR, sits at coarse centre (PAR + f) >> 1 and interpolates where PAR + f is odd. Only the offsets
+// in `mask` are written (out[f * stride]); every index is a compile-time constant.
+template <int P, int PAR>
+__device__ __forceinline__ void tile_axis_sums(const double* v, unsigned mask, double* out, int stride) {
+  constexpr int H = P / 2 - 1;
+#pragma unroll
+  for (int f = 0; f < 8; ++f) {
+    if (!((mask >> f) & 1)) continue;
+    const int c = H + ((PAR + f) >> 1);
+    out[f * stride] = ((PAR + f) & 1) ? lagrange_sum<P>(v + c - H, 1) : v[c];
+  }
+}
+
+// One CTA per tile, its threads on one variable at a time: stage X a thread per coarse row (y, z),
+// the row's P + 3 coarse values loaded once and every listed fine x formed from them; stage Y a
+// thread per (fine x, coarse z), the column's P + 3 x sums read once; stage Z a thread per listed
+// point. The shared arrays' rows have an odd pitch (no bank conflicts between neighbouring
+// threads); at most 19.7 KB at P = 10.
 constexpr int PROLONG_TILE_THREADS = 128;
 
 template <int P>
 static __global__ void __launch_bounds__(PROLONG_TILE_THREADS, 8)
     fill_prolong_tile_kernel(const ProlongTile* __restrict__ tiles, const unsigned short* __restrict__ pts,
                              double* __restrict__ work, Geo g) {
-  constexpr int C = P + 4, H = P / 2 - 1;
-  __shared__ double X[8 * C * C];
-  __shared__ double Y[8 * 8 * C];
+  constexpr int C = P + 4, CP = C | 1, H = P / 2 - 1, NVAL = P + 3;
+  __shared__ double X[8 * CP * CP];  // [fx][cz][cy]
+  __shared__ double Y[8 * 8 * CP];   // [fy][fx][cz]
   const ProlongTile T = tiles[blockIdx.x];
   const int px = T.par & 1, py = (T.par >> 1) & 1, pz = (T.par >> 2) & 1;
   const long sy = g.Wx, sz = (long)g.Wx * g.Wd;
-  const int nX = T.nfx * T.cyn * T.czn, nY = T.nfx * T.nfy * T.czn;
+  const int nrow = T.cyn * T.czn, ncol = T.nfx * T.czn;
   for (int v = 0; v < NV; ++v) {
     const double* src = work + (long)T.src_b * NV * g.Wv + (long)v * g.Wv;
-    // stage X: the x sum of every coarse row (y, z) at every listed fine x
-    for (int e = threadIdx.x; e < nX; e += PROLONG_TILE_THREADS) {
-      const int cyi = e % T.cyn, r = e / T.cyn, czi = r % T.czn, kx = r / T.czn;
-      const int fx = (T.fxs >> (3 * kx)) & 7, nx = px + fx;
-      const double* row = src + (T.cxb + (nx >> 1)) + sy * (T.ylo + cyi) + sz * (T.zlo + czi);
-      X[(fx * C + czi) * C + cyi] = (nx & 1) ? lagrange_sum<P>(row - H, 1) : row[0];
+    // stage X: per coarse row (y, z) the x sums at every listed fine x
+    for (int e = threadIdx.x; e < nrow; e += PROLONG_TILE_THREADS) {
+      const int cyi = e % T.cyn, czi = e / T.cyn;
+      const int x0 = T.cxb - H;
+      const double* row = src + x0 + sy * (T.ylo + cyi) + sz * (T.zlo + czi);
+      double val[NVAL];
+#pragma unroll
+      for (int k = 0; k < NVAL; ++k) val[k] = (x0 + k >= T.xlo && x0 + k <= T.xhi) ? row[k] : 0.0;
+      double* out = X + czi * CP + cyi;
+      if (px)
+        tile_axis_sums<P, 1>(val, T.fxm, out, CP * CP);
+      else
+        tile_axis_sums<P, 0>(val, T.fxm, out, CP * CP);
     }
     __syncthreads();
-    // stage Y: the y sum over those rows at every listed (fine x, fine y)
-    for (int e = threadIdx.x; e < nY; e += PROLONG_TILE_THREADS) {
-      const int czi = e % T.czn, r = e / T.czn, ky = r % T.nfy, kx = r / T.nfy;
-      const int fx = (T.fxs >> (3 * kx)) & 7, fy = (T.fys >> (3 * ky)) & 7, ny = py + fy;
-      const double* col = X + (fx * C + czi) * C + (T.cyb + (ny >> 1) - T.ylo);
-      Y[(fx * 8 + fy) * C + czi] = (ny & 1) ? lagrange_sum<P>(col - H, 1) : col[0];
+    // stage Y: per (listed fine x, coarse z) the y sums at every listed fine y
+    for (int e = threadIdx.x; e < ncol; e += PROLONG_TILE_THREADS) {
+      const int czi = e % T.czn, kx = e / T.czn;
+      const int fx = (T.fxs >> (3 * kx)) & 7;
+      const int y0 = T.cyb - H - T.ylo;  // column index of val[0]
+      const double* col = X + (fx * CP + czi) * CP;
+      double val[NVAL];
+#pragma unroll
+      for (int k = 0; k < NVAL; ++k) val[k] = (y0 + k >= 0 && y0 + k < T.cyn) ? col[y0 + k] : 0.0;
+      double* out = Y + fx * CP + czi;
+      if (py)
+        tile_axis_sums<P, 1>(val, T.fym, out, 8 * CP);
+      else
+        tile_axis_sums<P, 0>(val, T.fym, out, 8 * CP);
     }
     __syncthreads();
     // stage Z: the z sum at the listed points, written into the fine block (the next
@@ -297,7 +330,7 @@ static __global__ void __launch_bounds__(PROLONG_TILE_THREADS, 8)
     for (int e = threadIdx.x; e < T.np; e += PROLONG_TILE_THREADS) {
       const int c = pts[T.p0 + e];
       const int fx = c & 7, fy = (c >> 3) & 7, fz = (c >> 6) & 7, nz = pz + fz;
-      const double* col = Y + (fx * 8 + fy) * C + (T.czb + (nz >> 1) - T.zlo);
+      const double* col = Y + (fy * 8 + fx) * CP + (T.czb + (nz >> 1) - T.zlo);
       dst[(T.i0 + fx) + sy * (T.j0 + fy) + sz * (T.k0 + fz)] = (nz & 1) ? lagrange_sum<P>(col - H, 1) : col[0];
     }
   }

@@ -546,7 +546,7 @@ static bool tile_prolongation(const tgh_problem* p, const HostPlan& hp, const st
   auto fdiv8 = [](int r) { return r >= 0 ? r / 8 : -((-r + 7) / 8); };
   struct Acc {
     ProlongTile t;
-    int ylo, yhi, zlo, zhi, fxm, fym;
+    int xlo, xhi, ylo, yhi, zlo, zhi, fxm, fym;
     std::vector<unsigned short> c;
   };
   std::unordered_map<unsigned long long, int> index;
@@ -582,8 +582,8 @@ static bool tile_prolongation(const tgh_problem* p, const HostPlan& hp, const st
       n.t.cxb = (short)(ctr[0] - ((par[0] + f[0]) >> 1));
       n.t.cyb = (short)(ctr[1] - ((par[1] + f[1]) >> 1));
       n.t.czb = (short)(ctr[2] - ((par[2] + f[2]) >> 1));
-      n.ylo = n.zlo = 1 << 30;
-      n.yhi = n.zhi = -(1 << 30);
+      n.xlo = n.ylo = n.zlo = 1 << 30;
+      n.xhi = n.yhi = n.zhi = -(1 << 30);
       acc.push_back(std::move(n));
     } else {
       a = it->second;
@@ -592,7 +592,9 @@ static bool tile_prolongation(const tgh_problem* p, const HostPlan& hp, const st
     const short cb[3] = {A.t.cxb, A.t.cyb, A.t.czb};
     for (int d = 0; d < 3; ++d)
       if (((A.t.par >> d) & 1) != par[d] || cb[d] + ((par[d] + f[d]) >> 1) != ctr[d]) return false;
-    const int oy = (q.odd >> 1) & 1, oz = (q.odd >> 2) & 1;
+    const int ox = q.odd & 1, oy = (q.odd >> 1) & 1, oz = (q.odd >> 2) & 1;
+    A.xlo = std::min(A.xlo, ctr[0] - (ox ? H : 0));
+    A.xhi = std::max(A.xhi, ctr[0] + (ox ? P / 2 : 0));
     A.ylo = std::min(A.ylo, ctr[1] - (oy ? H : 0));
     A.yhi = std::max(A.yhi, ctr[1] + (oy ? P / 2 : 0));
     A.zlo = std::min(A.zlo, ctr[2] - (oz ? H : 0));
@@ -607,12 +609,9 @@ static bool tile_prolongation(const tgh_problem* p, const HostPlan& hp, const st
     const int cyn = A.yhi - A.ylo + 1, czn = A.zhi - A.zlo + 1;
     if (cyn > C || czn > C) return false;
     // every coarse value stage X reads lies in the coarse block's working array
-    if (A.ylo < 0 || A.yhi >= Wd || A.zlo < 0 || A.zhi >= Wd) return false;
-    for (int x = 0; x < 8; ++x) {
-      if (!(A.fxm >> x & 1)) continue;
-      const int nx = (A.t.par & 1) + x, c = A.t.cxb + (nx >> 1);
-      if ((nx & 1) ? (c - H < 0 || c - H + P > Wd) : (c < 0 || c >= Wd)) return false;
-    }
+    if (A.xlo < 0 || A.xhi >= Wd || A.ylo < 0 || A.yhi >= Wd || A.zlo < 0 || A.zhi >= Wd) return false;
+    A.t.xlo = (short)A.xlo;
+    A.t.xhi = (short)A.xhi;
     A.t.ylo = (short)A.ylo;
     A.t.zlo = (short)A.zlo;
     A.t.cyn = (unsigned char)cyn;
@@ -622,11 +621,8 @@ static bool tile_prolongation(const tgh_problem* p, const HostPlan& hp, const st
     for (int x = 0; x < 8; ++x)
       if (A.fxm >> x & 1) A.t.fxs |= x << (3 * n++);
     A.t.nfx = (unsigned char)n;
-    n = 0;
-    A.t.fys = 0;
-    for (int y = 0; y < 8; ++y)
-      if (A.fym >> y & 1) A.t.fys |= y << (3 * n++);
-    A.t.nfy = (unsigned char)n;
+    A.t.fxm = (unsigned char)A.fxm;
+    A.t.fym = (unsigned char)A.fym;
     A.t.p0 = (int)codes.size();
     A.t.np = (int)A.c.size();
     codes.insert(codes.end(), A.c.begin(), A.c.end());
