@@ -171,14 +171,28 @@ def cpu_model():
     return "unknown"
 
 
+def simd_oracle(case, forest):
+    """The oracle build with the host's widest SIMD lanes (AVX-512: 8 doubles, else AVX2: 4), every
+    host thread, and a problem on it whose right-hand side runs on those lanes, as the reference's
+    CPU kernel does (src/lanes.jl)."""
+    sys.path.insert(0, str(ROOT / "tests"))
+    import oracle_binding  # noqa: E402  (test infrastructure, loaded for the baseline only)
+    orc = oracle_binding.Oracle.load_widest()
+    orc.lib.orc_set_threads(os.cpu_count() or 1)
+    O = orc.problem(case, forest, 4)
+    O.set_simd_width(orc.lanes())
+    return orc, O
+
+
+def simd_label(orc):
+    n = orc.lanes()
+    return f"{n} FP64 lanes along x ({'AVX-512' if n == 8 else 'AVX2'}), groups straddling the interior point by point"
+
+
 def cpu_baseline(tgh, sample_case, sample_forest, perturbed, seconds=10.0, max_steps=40):
     """The oracle's RK4 step (the C++ restatement of the reference's CPU path) on a bounded
     sample of the workload, with every host thread: steps until about `seconds` of work."""
-    sys.path.insert(0, str(ROOT / "tests"))
-    import oracle_binding  # noqa: E402  (test infrastructure, loaded for the baseline only)
-    orc = oracle_binding.Oracle.load()
-    orc.lib.orc_set_threads(os.cpu_count() or 1)
-    O = orc.problem(sample_case, sample_forest, 4)
+    orc, O = simd_oracle(sample_case, sample_forest)
     u = O.initial_state(O.statevector(), 0.0)
     if perturbed:
         u = u + tgh.perturbation(sample_forest, amplitude=1e-4)
@@ -203,7 +217,7 @@ def cpu_baseline(tgh, sample_case, sample_forest, perturbed, seconds=10.0, max_s
     monitors = {"gh_constraint_ms": (t2 - t1) * 1e3, "adm_constraint_ms": (t3 - t2) * 1e3,
                 "points": npts, "unit": "ms per call on the sample"}
     return {"value": pts / el, "unit": "point-updates/s", "cores": int(orc.lib.orc_get_threads()), "kind": "port",
-            "cpu_model": cpu_model(),
+            "cpu_model": cpu_model(), "simd": simd_label(orc),
             "sample": f"{sample_forest.nblocks} blocks of {sample_forest.N}^3 of the same configuration, "
                       f"{steps} RK4 step(s), {el:.2f} s",
             "monitors": monitors}
@@ -215,11 +229,7 @@ def run_reference(args):
         return 0
     tgh = load_package()
     case, forest, scase, sforest, cfg, gauge, perturbed = workload(tgh, args.workload)
-    sys.path.insert(0, str(ROOT / "tests"))
-    import oracle_binding  # noqa: E402
-    orc = oracle_binding.Oracle.load()
-    orc.lib.orc_set_threads(os.cpu_count() or 1)
-    O = orc.problem(scase, sforest, 4)
+    orc, O = simd_oracle(scase, sforest)
     u = O.initial_state(O.statevector(), 0.0)
     if perturbed:
         u = u + tgh.perturbation(sforest, amplitude=1e-4)
@@ -238,7 +248,7 @@ def run_reference(args):
            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
            "config": cfg,
            "cpu_baseline": {"value": val, "unit": "point-updates/s", "cores": cores, "kind": "port",
-                            "cpu_model": cpu_model(),
+                            "cpu_model": cpu_model(), "simd": simd_label(orc),
                             "sample": f"each step: one RK4 step of {sforest.nblocks} blocks of {sforest.N}^3 of the "
                                       "same configuration (the reference is Julia and cannot run here; this is "
                                       "the C++ restatement of its CPU path)"},

@@ -34,6 +34,7 @@
 
 #include "adm_streamed.hpp"
 #include "bounds.hpp"
+#include "lanes.hpp"
 #include "physics.hpp"
 #include "pointwise.hpp"
 #include "spacetime.hpp"
@@ -57,6 +58,7 @@ struct Problem {
   KSSource ks;
   bool diss = false;
   std::vector<double> work, Hsrc;
+  int simd = 1;  // points the right-hand side evaluates at once along x: 1 or ORC_SIMD_W
   std::vector<double> ustate;  // the state the last prepare scattered
   double t_prep = 0.0;
   // the :fitted target cache (src/fit.jl:1030-1055): per block 40 fields of the owned points, the
@@ -234,8 +236,8 @@ struct PointCtx {
 template <class T = double>
 static inline T axis_stencil(const std::vector<double>& w, const double* wk, size_t base, long stride) {
   const int n = (int)w.size(), r = (n - 1) / 2;
-  T s = T(w[0]) * T(wk[base + (long)(-r) * stride]);
-  for (int k = 1; k < n; ++k) s = s + T(w[k]) * T(wk[base + (long)(k - r) * stride]);
+  T s = T(w[0]) * ldw<T>(wk + base + (long)(-r) * stride);
+  for (int k = 1; k < n; ++k) s = s + T(w[k]) * ldw<T>(wk + base + (long)(k - r) * stride);
   return s;
 }
 template <class T = double>
@@ -243,8 +245,8 @@ static inline T mixed_stencil(const std::vector<double>& w, const double* wk, si
   const int n = (int)w.size(), r = (n - 1) / 2;
   T outer = T(0.0);
   for (int a = 0; a < n; ++a) {
-    T inner = T(w[0]) * T(wk[base + (long)(a - r) * s1 + (long)(-r) * s2]);
-    for (int e = 1; e < n; ++e) inner = inner + T(w[e]) * T(wk[base + (long)(a - r) * s1 + (long)(e - r) * s2]);
+    T inner = T(w[0]) * ldw<T>(wk + base + (long)(a - r) * s1 + (long)(-r) * s2);
+    for (int e = 1; e < n; ++e) inner = inner + T(w[e]) * ldw<T>(wk + base + (long)(a - r) * s1 + (long)(e - r) * s2);
     outer = a == 0 ? T(w[0]) * inner : outer + T(w[a]) * inner;
   }
   return outer;
@@ -260,8 +262,8 @@ static void gauge_at_point(const Problem& P, int b, const int I[3], const T* h, 
     }
   } else if (P.cfg.gauge == TGH_GAUGE_SAMPLED) {
     size_t o = (size_t)b * NV * P.npt_state() + I[0] + P.N1 * (I[1] + (size_t)P.N1 * I[2]);
-    for (int a = 0; a < 4; ++a) Hl[a] = T(P.Hsrc[o + a * P.npt_state()]);
-    for (int k = 0; k < 16; ++k) dHl[k % 4][k / 4] = T(P.Hsrc[o + (4 + k) * P.npt_state()]);
+    for (int a = 0; a < 4; ++a) Hl[a] = ldw<T>(P.Hsrc.data() + o + a * P.npt_state());
+    for (int k = 0; k < 16; ++k) dHl[k % 4][k / 4] = ldw<T>(P.Hsrc.data() + o + (4 + k) * P.npt_state());
   } else {
     algebraic_gauge_source<T>(P.ks, h, dth, dh, Hl, dHl);
   }
@@ -274,13 +276,29 @@ static void rhs_at_point(const Problem& P, const PointCtx& c, int b, const int I
   const double h = P.spacing(P.level[b]);
   const T inv_h = T(1.0) / T(h);
   const T inv_h2 = inv_h * inv_h;
-  const T g0 = T(P.pr.damping_rate(t, x));
-  const T eh = T(P.pr.dissipation_rate(t, x)) * inv_h;
+  // the profiles at each point of the group (one point, or a group's lanes along x)
+  auto lane_x = [&](int l, double xl[3]) {
+    int64_t n[3] = {(int64_t)P.corner[3 * b] + I[0] + l, (int64_t)P.corner[3 * b + 1] + I[1],
+                    (int64_t)P.corner[3 * b + 2] + I[2]};
+    P.position(P.level[b], n, xl);
+  };
+  const T g0 = PerLane<T>::make([&](int l) {
+    double xl[3];
+    if (l == 0) return P.pr.damping_rate(t, x);
+    lane_x(l, xl);
+    return P.pr.damping_rate(t, xl);
+  });
+  const T eh = PerLane<T>::make([&](int l) {
+    double xl[3];
+    if (l == 0) return P.pr.dissipation_rate(t, x);
+    lane_x(l, xl);
+    return P.pr.dissipation_rate(t, xl);
+  }) * inv_h;
   const double* wk = c.wk;
   T hv[NC], Pv[NC], dhs[3][NC];
   for (int v = 0; v < NC; ++v) {
-    hv[v] = T(wk[c.var + v * c.sv]);
-    Pv[v] = T(wk[c.var + (NC + v) * c.sv]);
+    hv[v] = ldw<T>(wk + c.var + v * c.sv);
+    Pv[v] = ldw<T>(wk + c.var + (NC + v) * c.sv);
   }
   for (int d = 0; d < 3; ++d)
     for (int v = 0; v < NC; ++v) dhs[d][v] = inv_h * axis_stencil<T>(P.st.w1, wk, c.var + v * c.sv, c.st[d]);
@@ -322,7 +340,7 @@ static void rhs_at_point(const Problem& P, const PointCtx& c, int b, const int I
   // gh_rhs_pi, one component at a time (src/evolution.jl:324-354)
   for (int v = 0; v < NC; ++v) {
     size_t bh = c.var + v * c.sv, bP = bh + NC * c.sv;
-    T Pi_v = T(wk[bP]);
+    T Pi_v = ldw<T>(wk + bP);
     T d1 = inv_h * axis_stencil<T>(P.st.w1, wk, bh, c.st[0]);
     T d2 = inv_h * axis_stencil<T>(P.st.w1, wk, bh, c.st[1]);
     T d3 = inv_h * axis_stencil<T>(P.st.w1, wk, bh, c.st[2]);
@@ -436,8 +454,61 @@ static void rhs_point(const Problem& P, int b, const int I[3], double t, const d
   }
 }
 
+// A group of W points along x on SIMD lanes (gh_rhs_lanes!, src/evolution.jl:698-790): F on the
+// lanes where the interior does not act at any of them (no hole, or every point at r >= r_1)
+// and there is no matter term; otherwise point by point through rhs_point, branch for branch.
+static void rhs_group(const Problem& P, int b, int i0, int j, int k, double t, const double* matter, double* du) {
+  constexpr int W = ORC_SIMD_W;
+  typedef Lane<W> V;
+  const size_t S = P.npt_state();
+  bool lanes = matter == nullptr;
+  double x[W][3];
+  for (int l = 0; l < W; ++l) {
+    int64_t n[3] = {(int64_t)P.corner[3 * b] + i0 + l, (int64_t)P.corner[3 * b + 1] + j,
+                    (int64_t)P.corner[3 * b + 2] + k};
+    P.position(P.level[b], n, x[l]);
+    if (P.in.variant != TGH_INT_NONE && !P.in.is_outside(P.in.radius(t, x[l]))) lanes = false;
+  }
+  const size_t o = (size_t)b * NV * S + i0 + P.N1 * (j + (size_t)P.N1 * k);
+  if (!lanes) {
+    double out[NV];
+    for (int l = 0; l < W; ++l) {
+      int I[3] = {i0 + l, j, k};
+      rhs_point(P, b, I, t, matter, out);
+      for (int v = 0; v < NV; ++v) du[o + l + v * S] = out[v];
+    }
+    return;
+  }
+  PointCtx c;
+  c.wk = P.work.data() + (size_t)b * NV * P.npt_work();
+  c.sv = P.npt_work();
+  c.st[0] = 1;
+  c.st[1] = P.W;
+  c.st[2] = P.W * P.W;
+  c.var = (size_t)(i0 + P.G) + P.W * ((size_t)(j + P.G) + (size_t)P.W * (k + P.G));
+  int I[3] = {i0, j, k};
+  V F[NV];
+  rhs_at_point<V>(P, c, b, I, x[0], t, nullptr, F, F + NC);
+  for (int v = 0; v < NV; ++v)
+    for (int l = 0; l < W; ++l) du[o + l + v * S] = F[v].v[l];
+}
+
 static void rhs(Problem& P, double* du, double t, const double* matter) {
   const size_t S = P.npt_state();
+  if (P.simd > 1 && P.N1 >= ORC_SIMD_W) {
+    // the groups of a row: every W-th point from the first as far as a whole group fits, and
+    // the group ending at the row's last point (is_lane_leader, src/lanes.jl:108-117)
+    const int last = P.N1 - ORC_SIMD_W;
+#pragma omp parallel for schedule(dynamic) collapse(2)
+    for (int b = 0; b < P.nb; ++b)
+      for (int k = 0; k < P.N1; ++k)
+        for (int j = 0; j < P.N1; ++j) {
+          int i0 = 0;
+          for (; i0 <= last; i0 += ORC_SIMD_W) rhs_group(P, b, i0, j, k, t, matter, du);
+          if (i0 - ORC_SIMD_W != last) rhs_group(P, b, last, j, k, t, matter, du);
+        }
+    return;
+  }
 #pragma omp parallel for schedule(dynamic) collapse(2)
   for (int b = 0; b < P.nb; ++b)
     for (int k = 0; k < P.N1; ++k) {
@@ -1086,6 +1157,12 @@ const char* orc_last_error(void* p) { return ((Problem*)p)->err.c_str(); }
 size_t orc_state_length(void* p) { Problem* P = (Problem*)p; return P->npt_state() * NV * P->nb; }
 size_t orc_work_length(void* p) { Problem* P = (Problem*)p; return P->npt_work() * NV * P->nb; }
 void orc_set_threads(int n) { omp_set_num_threads(n); }
+// The right-hand side's SIMD width: 1 (point by point) or the build's ORC_SIMD_W; returns the width set.
+int orc_set_simd_width(void* p, int w) {
+  ((Problem*)p)->simd = w == ORC_SIMD_W ? ORC_SIMD_W : 1;
+  return ((Problem*)p)->simd;
+}
+int orc_simd_lanes(void) { return ORC_SIMD_W; }
 int orc_get_threads(void) { return omp_get_max_threads(); }
 
 int orc_prepare(void* p, const double* u, double t) {
@@ -1470,6 +1547,7 @@ static inline Cnt operator/(Cnt a, Cnt b) { ++Cnt::ndiv; return Cnt(a.v / b.v); 
 static inline bool operator!=(Cnt a, Cnt b) { return a.v != b.v; }
 static inline Cnt sqrt(Cnt a) { ++Cnt::nsqrt; return Cnt(std::sqrt(a.v)); }
 static inline double dval(Cnt a) { return a.v; }
+static inline Cnt select_pos(Cnt c, Cnt a, Cnt b) { return c.v > 0 ? a : b; }
 }  // namespace orc
 
 extern "C" {

@@ -364,6 +364,8 @@ static inline KSSource make_ks_source(double M, const double spin[3], const doub
 }
 // the value of a scalar for the branch conditions (an op-counting scalar overloads it)
 static inline double dval(double x) { return x; }
+// a where c > 0, else b (both formed; per lane for SIMD lanes)
+static inline double select_pos(double c, double a, double b) { return c > 0 ? a : b; }
 
 // src/gauge.jl:302-326 (+ _algebraic_dH :330-336); dHl[c][a] = d_c H_a. Templated on the
 // scalar so the op-counting instantiation sees its arithmetic.
@@ -384,7 +386,7 @@ static inline void algebraic_gauge_source(const KSSource& src, const T* h, const
   T sw = T(src.S[0]) * w[0];
   for (int a = 1; a < 4; ++a) sw = sw + T(src.S[a]) * w[a];
   T rad = T(src.M) * T(src.M) - sw * sw;
-  T root = dval(rad) > 0 ? sqrt(rad) : T(0.0);
+  T root = select_pos(rad, sqrt(rad), T(0.0));
   T D = T(src.M) + root;
   for (int a = 0; a < 4; ++a) Hl[a] = (-K / D) * w[a];
   const T* Dp[4] = {dth, dh[0], dh[1], dh[2]};
@@ -403,7 +405,7 @@ static inline void algebraic_gauge_source(const KSSource& src, const T* h, const
     for (int a = 1; a < 4; ++a) dK = dK + T(src.u[a]) * dw[c][a];
     T Sdw = T(src.S[0]) * dw[c][0];
     for (int a = 1; a < 4; ++a) Sdw = Sdw + T(src.S[a]) * dw[c][a];
-    T dD = dval(root) > 0 ? -sw * Sdw / root : T(0.0);
+    T dD = select_pos(root, -sw * Sdw / root, T(0.0));
     for (int a = 0; a < 4; ++a) dHl[c][a] = -(dK * w[a] + K * dw[c][a]) / D + K * w[a] * dD / (D * D);
   }
 }

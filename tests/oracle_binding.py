@@ -9,6 +9,14 @@ from conftest import load_package
 
 ROOT = Path(__file__).resolve().parent.parent
 LIB = ROOT / "oracle" / "_build" / "liboracle.so"
+LIB_V4 = ROOT / "oracle" / "_build" / "liboracle_v4.so"  # AVX-512 build, 8 SIMD lanes
+
+
+def host_has_avx512():
+    try:
+        return " avx512f" in Path("/proc/cpuinfo").read_text()
+    except OSError:
+        return False
 
 _D = ctypes.c_double
 _VP = ctypes.c_void_p
@@ -34,6 +42,8 @@ class Oracle:
             "orc_state_length": (ctypes.c_size_t, [_VP]),
             "orc_work_length": (ctypes.c_size_t, [_VP]),
             "orc_set_threads": (None, [ctypes.c_int]),
+            "orc_set_simd_width": (ctypes.c_int, [_VP, ctypes.c_int]),
+            "orc_simd_lanes": (ctypes.c_int, []),
             "orc_get_threads": (ctypes.c_int, []),
             "orc_prepare": (ctypes.c_int, [_VP, _DP, _D]),
             "orc_rhs": (ctypes.c_int, [_VP, _DP, _D, _DP]),
@@ -95,6 +105,23 @@ class Oracle:
                 subprocess.run(["make", "-C", str(ROOT / "oracle")], check=True, capture_output=True)
             cls._inst = cls(ctypes.CDLL(str(LIB)))
         return cls._inst
+
+    _inst_v4 = None
+
+    @classmethod
+    def load_widest(cls):
+        """The build with the host's widest SIMD lanes: the AVX-512 one (8 lanes) where the CPU
+        has AVX-512, else the AVX2 one (4 lanes)."""
+        if not host_has_avx512():
+            return cls.load()
+        if cls._inst_v4 is None:
+            if not LIB_V4.exists():
+                subprocess.run(["make", "-C", str(ROOT / "oracle")], check=True, capture_output=True)
+            cls._inst_v4 = cls(ctypes.CDLL(str(LIB_V4)))
+        return cls._inst_v4
+
+    def lanes(self):
+        return int(self.lib.orc_simd_lanes())
 
     def problem(self, case, forest, q, margin_check=False):
         return OracleProblem(self, case, forest, q, margin_check)
@@ -213,6 +240,10 @@ class OracleProblem:
 
     def statevector(self):
         return np.zeros(self.L)
+
+    def set_simd_width(self, w):
+        """1 (point by point) or the build's lane count; returns the width set."""
+        return int(self.lib.orc_set_simd_width(self.h, int(w)))
 
     def initial_state(self, u, t):
         self.lib.orc_initial_state(self.h, _dp(u), t)
