@@ -392,14 +392,24 @@ def time_monitors(P, u, stream, gauge, n1pts, peak, reps=5):
     return out
 
 
+def e2e_buffers(nbytes):
+    """Three device buffers (and three pinned host result buffers) where both memories hold them
+    with room to spare, else two."""
+    import torch
+    import psutil
+    free_dev, _ = torch.cuda.mem_get_info()
+    host = psutil.virtual_memory().available
+    return 3 if free_dev > 3 * nbytes + (4 << 30) and host > 4 * nbytes + (16 << 30) else 2
+
+
 def end_to_end(P, uh, dt, K, world, pts, stream, dist, NB=3):
     """The metric through the public API with host buffers: per step the state is copied in
     from pinned host memory (uh), stepped, and copied back, all inside the timed region. The
     steps are independent requests, pipelined over NB device buffers: step n+1's upload (one
     copy stream) and step n-1's download (another) run while step n computes; with NB = 3 no
-    upload waits for the download of the buffer it refills (step n-2's, long finished), with
-    NB = 2 (the hierarchy, whose state is 14 GB) the upload of step n+1 waits for step n-1's
-    download."""
+    upload waits for the download of the buffer it refills (step n-2's, long finished), so the two
+    directions run at once; with NB = 2 (where memory holds no third buffer) the upload of step
+    n+1 waits for step n-1's download."""
     import torch
     res_h = [torch.empty(uh.numel(), dtype=uh.dtype, pin_memory=True) for _ in range(NB)]
     ud = [torch.empty(uh.numel(), dtype=uh.dtype, device="cuda") for _ in range(NB)]
@@ -600,9 +610,9 @@ def main():
     uh.copy_(u0)
     del u
     if big:
-        del u0  # the hierarchy's state is 14 GB: two device buffers beside the batched problem's
+        del u0  # the hierarchy's state is 14 GB: its device buffers sit beside the batched problem's
         torch.cuda.empty_cache()
-    e2e = end_to_end(P, uh, dt, K, world, pts, stream, dist, NB=2 if big else 3)
+    e2e = end_to_end(P, uh, dt, K, world, pts, stream, dist, NB=e2e_buffers(uh.numel() * 8))
     if big:
         # the plain forms' own buffers (k, acc, y) do not fit beside the batched form's: a problem
         # of their own once the batched one is released

@@ -155,6 +155,10 @@ size_t tgh_state_length(const tgh_problem* p);
 /* doubles in the ghosted working array: (N+2G+1)^3 * 20 * blocks held (a rank of a sharded
  * problem holds its own leaves and its halo) */
 size_t tgh_work_length(const tgh_problem* p);
+/* the fill plan's sizes (points per fill of the batched form): counts[0] copied points (ghosts
+ * from their primary, owned copies that are not primary), [1] Dirichlet ghosts, [2] prolonged
+ * points of all levels, [3] prolongation tiles (0 where a level runs point by point) */
+int tgh_fill_counts(const tgh_problem* p, long long counts[4]);
 /* copy the working array (device to device) for inspection */
 int tgh_copy_work(tgh_problem* p, double* dst);
 /* the same for the blocks b0 .. b0 + nblocks - 1 of the working array (each (N+2G+1)^3 * 20

@@ -79,6 +79,7 @@ SIGNATURES = {
     "tgh_step_limit": (ctypes.c_int, [_VP, _VP, _D]),
     "tgh_max_speed": (ctypes.c_int, [_VP, _VP, _D, ctypes.POINTER(_D)]),
     "tgh_initial_state": (ctypes.c_int, [_VP, _VP, _D]),
+    "tgh_fill_counts": (ctypes.c_int, [_VP, ctypes.POINTER(ctypes.c_longlong)]),
     "tgh_set_target": (ctypes.c_int, [_VP, _VP, _D]),
     "tgh_fill_target_snapshot": (ctypes.c_int, [_VP, _VP, _D, _D]),
     "tgh_fill_target_analytic": (ctypes.c_int, [_VP, _D, _D, _D]),

@@ -1131,6 +1131,16 @@ void tgh_problem_destroy(tgh_problem* p) {
 
 const char* tgh_last_error(const tgh_problem* p) { return p ? p->err.c_str() : "no problem"; }
 size_t tgh_state_length(const tgh_problem* p) { return (size_t)p->S * NV * p->nb; }
+
+int tgh_fill_counts(const tgh_problem* p, long long counts[4]) {
+  if (!p || !counts) return TGH_ERR_ARG;
+  counts[0] = p->ngpts;
+  counts[1] = p->nhooks;
+  counts[2] = counts[3] = 0;
+  for (size_t l = 0; l < p->nprol.size(); ++l) counts[2] += p->nprol[l];
+  for (size_t l = 0; l < p->ntile.size(); ++l) counts[3] += std::max(0, p->ntile[l]);
+  return TGH_OK;
+}
 // The ABI's view of the working array is the reference's layout, (N+2G+1)^3 points per block
 // and variable; the problem stores rows padded to the even pitch Wx.
 size_t tgh_work_length(const tgh_problem* p) { return (size_t)p->Wd * p->Wd * p->Wd * NV * p->nwb; }

@@ -37,8 +37,8 @@ namespace pitma {
 constexpr int N1 = 33, G = 3, SR = 2, KR = 3;  // q = 4, N = 32
 constexpr int TY = 11, TZ = 2, NPAIR = 17;
 constexpr int XB = 50;                                   // box width: x = -2 .. 47 (see below)
-constexpr int HY = TY + 2 * SR, HZ = TZ + 2 * SR;          // 15, 7
-constexpr int PY = TY + 2 * KR, PZ = TZ + 2 * KR;        // 17, 9
+constexpr int HY = TY + 2 * SR, HZ = TZ + 2 * SR;          // 15, 6
+constexpr int PY = TY + 2 * KR, PZ = TZ + 2 * KR;        // 17, 8
 constexpr int HN = XB * HY * HZ, PN = XB * PY * PZ;      // doubles per box
 constexpr int HBYTES = HN * 8, PBYTES = PN * 8;
 constexpr int HOFF = 0;                                  // byte offsets inside one stage

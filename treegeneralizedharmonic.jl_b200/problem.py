@@ -142,6 +142,12 @@ class GHProblem:
         self._check(self.lib.tgh_initial_state(self._h, _ptr(u), float(t)))
         return u
 
+    def fill_counts(self):
+        """The fill plan's sizes: copied points, Dirichlet ghosts, prolonged points, prolongation tiles."""
+        c = (ctypes.c_longlong * 4)()
+        self._check(self.lib.tgh_fill_counts(self._h, c))
+        return {"copies": c[0], "hooks": c[1], "prolonged": c[2], "tiles": c[3]}
+
     # ---- the :fitted target cache (src/fit.jl:1030-1285) ----
 
     def target_length(self):
