@@ -26,6 +26,11 @@ Workloads (seeded synthetic inputs, fully specified by their parameters):
                       [-1,1]^3, 8 blocks of 32^3, q = 4, eps_KO = 1/2, gamma0 = 1, dt = h/4
   hierarchy_small     the same hole on [-6,6]^3 refined in 2 levels (radii 3.0, 1.6) to 120
                       blocks of 32^3: one coarse-fine interface, a few GB, for ncu captures
+  g5                  the reference's G5 chart: Kerr M=1, a=7/10 in harmonic coordinates (no gauge
+                      source) on [-5/4,5/4]^3, one root of 8^3 refined with radii 10, 8/5, 13/10, 1
+                      to 2472 blocks of 8^3 (1,265,664 points, h = 5/256), :fitted interior
+                      r_0 = 0.8, r_1 = 1 relaxing toward the analytic cache; the CPU baseline runs
+                      on this same mesh
 """
 import argparse
 import ctypes
@@ -102,7 +107,29 @@ def workload(tgh, name):
                "boundary": "dirichlet", "interior": "damped moving core r0=0.8 r1=1.3",
                "gauge_source": "algebraic", "eps_ko": 0.5, "cfl": 0.25}
         return case, forest, sample, sample_forest, cfg, "algebraic", False
+    if name == "g5":
+        case = tgh.harmonic_kerr_case(M=1.0, a=0.7, halfwidth=1.25, r0=0.8, r1=1.0, rho_max=4.0,
+                                      variant="fitted", eps_ko=0.5)
+        radii = [10.0, 1.6, 1.3, 1.0]
+        forest = tgh.hole_forest(case, 8, 1, radii)
+        counts = [int(c) for c in __import__("numpy").bincount(forest.level)]
+        cfg = {"workload": "g5_harmonic_kerr", "M": 1.0, "a": 0.7, "chart": "harmonic", "domain": "[-1.25,1.25]^3",
+               "blocks": forest.nblocks, "blocks_per_level": counts, "block": "8^3",
+               "h_min": forest.h0 / 2 ** int(forest.level.max()), "refinement_radii": radii, "q": 4,
+               "boundary": "dirichlet", "interior": "fitted r0=0.8 r1=1.0, analytic cache",
+               "gauge_source": "none", "eps_ko": 0.5, "cfl": 0.25}
+        return case, forest, case, forest, cfg, "none", False
     raise SystemExit(f"unknown workload {name}")
+
+
+def ready(case, P, forest):
+    """A :fitted problem relaxes toward its target cache: fill it from the analytic state (the
+    stand-in for the fit) before the first step."""
+    if case.interior and case.interior.get("variant") == "fitted":
+        if not hasattr(P, "fill_target_analytic"):
+            raise SystemExit("the sharded path takes no :fitted interior")
+        P.fill_target_analytic(0.0, case.interior["r1"] + h_min(forest), 0.0)
+    return P
 
 
 def h_min(forest):
@@ -179,7 +206,7 @@ def simd_oracle(case, forest):
     import oracle_binding  # noqa: E402  (test infrastructure, loaded for the baseline only)
     orc = oracle_binding.Oracle.load_widest()
     orc.lib.orc_set_threads(os.cpu_count() or 1)
-    O = orc.problem(case, forest, 4)
+    O = ready(case, orc.problem(case, forest, 4), forest)
     O.set_simd_width(orc.lanes())
     return orc, O
 
@@ -265,7 +292,7 @@ def run_sharded(args, tgh, world, rank, local, case, forest, cfg, gauge, perturb
     import torch.distributed as dist
     stream = torch.cuda.current_stream()
     owner = tgh.partition(forest, world)
-    S = tgh.ShardedGHProblem(case, forest, 4, rank, world, owner=owner, margin_check=False)
+    S = ready(case, tgh.ShardedGHProblem(case, forest, 4, rank, world, owner=owner, margin_check=False), forest)
     u0 = S.initial_state(S.statevector(), 0.0)
     if perturbed:
         u0 += S.local(torch.from_numpy(tgh.perturbation(forest, amplitude=1e-4)).cuda())
@@ -490,7 +517,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="hierarchy", choices=["hierarchy", "kerr_schild_static", "fourier",
-                                                                       "hierarchy_small"])
+                                                                       "hierarchy_small", "g5"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"],
                     help="mixed: FP32 stencil sums and algebra on the FP64 state (one GPU)")
@@ -529,7 +556,7 @@ def main():
     if world > 1 or args.shard:
         return run_sharded(args, tgh, world, rank, local, case, forest, cfg, gauge, perturbed)
     stream = torch.cuda.current_stream()
-    P = tgh.GHProblem(case, forest, 4, margin_check=False, precision=args.precision)
+    P = ready(case, tgh.GHProblem(case, forest, 4, margin_check=False, precision=args.precision), forest)
     if args.pi != "auto":
         P.set_variant(pi=args.pi)
     u0 = initial(tgh, P, forest, perturbed)
@@ -618,7 +645,7 @@ def main():
         # of their own once the batched one is released
         P.close()
         torch.cuda.empty_cache()
-        P = tgh.GHProblem(case, forest, 4, margin_check=False, precision=args.precision)
+        P = ready(case, tgh.GHProblem(case, forest, 4, margin_check=False, precision=args.precision), forest)
         if args.pi != "auto":
             P.set_variant(pi=args.pi)
         u0 = uh.cuda()
