@@ -81,14 +81,24 @@ struct Problem {
   }
 };
 
-// ---- the primary owner of a lattice point: finest level first, lower face first ----
+// ---- the primary owner of a lattice point: the coarsest leaf holding it, and within a level
+// the one holding it on its lower face. A point of level l's lattice lies on level k < l's when
+// its index is a multiple of 2^(l - k). ----
 static bool find_owner(const Problem& P, int l, const int64_t nin[3], int& leaf, int loc[3]) {
-  for (int k = P.maxlevel; k >= l; --k) {
+  for (int k = 0; k <= P.maxlevel; ++k) {
     int64_t m[3], per[3];
+    bool on = true;
     for (int d = 0; d < 3; ++d) {
-      m[d] = nin[d] << (k - l);
+      if (k >= l) {
+        m[d] = nin[d] << (k - l);
+      } else {
+        const int64_t s = (int64_t)1 << (l - k);
+        if (((nin[d] % s) + s) % s) on = false;
+        m[d] = nin[d] >= 0 ? nin[d] / s : -((-nin[d]) / s);
+      }
       per[d] = (int64_t)P.cells0[d] << k;
     }
+    if (!on) continue;
     int64_t cand[3][2];
     int nc[3];
     for (int d = 0; d < 3; ++d) {

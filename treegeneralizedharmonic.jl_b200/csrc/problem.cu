@@ -191,14 +191,27 @@ static void work_overwritten(tgh_problem* p, const char* who) {
 // ---- the forest: owners, positions ----
 static inline int64_t bkey(int64_t bx, int64_t by, int64_t bz) { return ((bx * 1048576) + by) * 1048576 + bz; }
 
-// The primary owner of lattice point n of level l: the finest leaf of level >= l holding the
-// point (closed blocks), and among a level's leaves the one with the point on its lower face.
+// The primary owner of lattice point n of level l: the coarsest leaf holding the point (closed
+// blocks; a point of level l lies on a coarser level k's lattice when n is a multiple of
+// 2^(l - k)), and among a level's leaves the one with the point on its lower face. With the
+// coarsest leaf primary the reference's driver record on a refined hole (the hole fixture,
+// err_l2 = 1.690514e-06) is met to 0.2 %; with the finest, to 3.9 %.
 static bool find_owner(const tgh_problem* p, int l, const int64_t n[3], int& leaf, int loc[3], int& lev) {
-  for (int k = p->maxlevel; k >= l; --k) {
+  for (int k = 0; k <= p->maxlevel; ++k) {
     int64_t m[3], cand[3][2];
     int nc[3];
+    bool on = true;
     for (int d = 0; d < 3; ++d) {
-      m[d] = n[d] << (k - l);
+      if (k >= l) {
+        m[d] = n[d] << (k - l);
+      } else {
+        const int64_t s = (int64_t)1 << (l - k);
+        if (n[d] % s) on = false;
+        m[d] = n[d] / s;
+      }
+    }
+    if (!on) continue;
+    for (int d = 0; d < 3; ++d) {
       int64_t c = m[d] / p->N;
       nc[d] = 0;
       cand[d][nc[d]++] = c;
@@ -371,7 +384,9 @@ static bool plan_rank(const tgh_problem* p, int r, bool entries, HostPlan& hp, s
           const int w = i + Wx * (j + Wd * k);
           int leaf = -1, loc[3], lev = -1;
           if (!outside && find_owner(p, l, n, leaf, loc, lev)) {
-            const int step = 1 << (lev - l);
+            // a run along x steps 2^(lev - l) source points a point; a coarser owner holds only
+            // every other point of the run, so its points stand alone (step 0)
+            const int step = lev >= l ? 1 << (lev - l) : 0;
             const bool own = i >= G && i <= G + p->N && j >= G && j <= G + p->N && k >= G && k <= G + p->N;
             const int sw = (loc[0] + G) + Wx * ((loc[1] + G) + Wd * (loc[2] + G));
             if (own && leaf == gb) {
@@ -381,7 +396,7 @@ static bool plan_rank(const tgh_problem* p, int r, bool entries, HostPlan& hp, s
               if (entries) gpts.push_back(CopyPt{b, w, intern(leaf), sw});
             }
             if (entries && one) {
-              if (open && cur.src_b == leaf && cur.step == step && cur.sj == loc[1] && cur.sk == loc[2] &&
+              if (open && step > 0 && cur.src_b == leaf && cur.step == step && cur.sj == loc[1] && cur.sk == loc[2] &&
                   cur.si + cur.len * step == loc[0] && cur.dst_w + cur.len == w) {
                 cur.len++;
               } else {
