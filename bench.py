@@ -5,13 +5,15 @@ One "step" is one classical RK4 step (four right-hand sides with Kreiss-Oliger d
 the ghost fill before each, the stage arithmetic) over the whole mesh of the workload. A
 point is an owned point counted N^3 per block, as the reference counts it.
 
-    python bench.py [--gpus N] [--steps K] [--warmup W] [--workload hierarchy|kerr_schild_static|fourier]
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--workload hierarchy|kerr_schild_static|fourier|g5]
     python bench.py --impl reference ...   # the CPU restatement of the reference's path
 
 One GPU: the batched form (the whole K-step run one CUDA graph). N GPUs (torchrun, one rank
 per GPU): the workload's mesh sharded over the ranks, per-level Morton partition, one NCCL
 all-to-all of halo points before each fill phase; the mesh is the same for every N (strong
-scaling). --shard runs that sharded path on one GPU.
+scaling). --shard runs that sharded path on one GPU. On one GPU the default (hierarchy) line
+also carries `g5_chart`: the reference's G5 chart (the g5 workload) stepped the same way, with
+its device time per M of evolution.
 
 Workloads (seeded synthetic inputs, fully specified by their parameters):
   hierarchy           (the default) the hole of kerr_schild_static boosted to v = 0.1 along x,
@@ -419,6 +421,34 @@ def time_monitors(P, u, stream, gauge, n1pts, peak, reps=5):
     return out
 
 
+def g5_chart(tgh, K, stream):
+    """The reference's G5 chart beside the headline (harmonic Kerr a = 7/10 on its 2472-block mesh
+    of 8^3, the `g5` workload): the batched step timed the same way, K steps after one warm-up
+    run, and the device time per M of evolution at dt = h/(4 lambda)."""
+    import torch
+    case, forest, *_ = workload(tgh, "g5")
+    P = ready(case, tgh.GHProblem(case, forest, 4, margin_check=False), forest)
+    u0 = P.initial_state(P.statevector(), 0.0)
+    dt = 0.25 * h_min(forest) / P.max_speed(u0, 0.0)
+    u = u0.clone()
+    P.step_batched(u, 0.0, dt, K)
+    u.copy_(u0)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    P.step_batched(u, 0.0, dt, K)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / K
+    finite = bool(torch.isfinite(u).all())
+    P.close()
+    return {"workload": "g5_harmonic_kerr", "blocks": forest.nblocks, "points": forest.points(), "steps": K,
+            "ms_per_step": ms, "value": forest.points() / (ms * 1e-3), "unit": "point-updates/s",
+            "steps_per_M": 1.0 / dt, "device_seconds_per_M": ms * 1e-3 / dt, "finite": finite,
+            "reference": "630 s of a 64-core node per M for the reference's G5 runs, horizon finder and fits "
+                         "included (SINGULARITY_HANDLING.md:1272)"}
+
+
 def e2e_buffers(nbytes):
     """Three device buffers (and three pinned host result buffers) where both memories hold them
     with room to spare, else two."""
@@ -675,9 +705,12 @@ def main():
            "gpu_launches": launches, "clocks": ck}
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         out["cpu_baseline"] = cpu_baseline(tgh, scase, sforest, perturbed)
+    P.close()
+    if big and world == 1:
+        torch.cuda.empty_cache()
+        out["g5_chart"] = g5_chart(tgh, K, stream)
     if rank == 0:
         print(json.dumps(out))
-    P.close()
     if world > 1:
         dist.destroy_process_group()
     return 0
