@@ -421,7 +421,7 @@ def time_monitors(P, u, stream, gauge, n1pts, peak, reps=5):
     return out
 
 
-def g5_chart(tgh, K, stream):
+def g5_chart(tgh, K, stream, with_cpu=True):
     """The reference's G5 chart beside the headline (harmonic Kerr a = 7/10 on its 2472-block mesh
     of 8^3, the `g5` workload): the batched step timed the same way, K steps after one warm-up
     run, and the device time per M of evolution at dt = h/(4 lambda)."""
@@ -442,9 +442,15 @@ def g5_chart(tgh, K, stream):
     ms = e0.elapsed_time(e1) / K
     finite = bool(torch.isfinite(u).all())
     P.close()
-    return {"workload": "g5_harmonic_kerr", "blocks": forest.nblocks, "points": forest.points(), "steps": K,
-            "ms_per_step": ms, "value": forest.points() / (ms * 1e-3), "unit": "point-updates/s",
-            "steps_per_M": 1.0 / dt, "device_seconds_per_M": ms * 1e-3 / dt, "finite": finite,
+    out = {"workload": "g5_harmonic_kerr", "blocks": forest.nblocks, "points": forest.points(), "steps": K,
+           "ms_per_step": ms, "value": forest.points() / (ms * 1e-3), "unit": "point-updates/s",
+           "steps_per_M": 1.0 / dt, "device_seconds_per_M": ms * 1e-3 / dt, "finite": finite}
+    if with_cpu:
+        # the oracle on SIMD lanes on this same mesh: the CPU baseline with the same configuration
+        cb = cpu_baseline(tgh, case, forest, False, seconds=8.0, max_steps=4)
+        cb.pop("monitors", None)
+        out["cpu_baseline_same_mesh"] = cb
+    return {**out,
             "reference": "630 s of a 64-core node per M for the reference's G5 runs, horizon finder and fits "
                          "included (SINGULARITY_HANDLING.md:1272)"}
 
@@ -708,7 +714,7 @@ def main():
     P.close()
     if big and world == 1:
         torch.cuda.empty_cache()
-        out["g5_chart"] = g5_chart(tgh, K, stream)
+        out["g5_chart"] = g5_chart(tgh, K, stream, with_cpu=not args.no_cpu_baseline)
     if rank == 0:
         print(json.dumps(out))
     if world > 1:
