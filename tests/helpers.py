@@ -31,25 +31,6 @@ def rhs_scale(work, forest, q):
     return out
 
 
-def roundoff_floor(work, forest, q):
-    """Per owned point, the size of the roundoff two correct evaluations of the right-hand side
-    may differ by: eps times the largest second-difference magnitude the point's stencils sum,
-    sum_k |w_k| max_v |u_v| / h^2, times 8 (a few such stencils contracted with O(1)
-    coefficients). Two summation orders of a q = 4 second difference at h = 5/256 on data of
-    order one differ by ~1e-12 absolute, the reference's own bound on coarser meshes; this floor
-    is where the comparison of any two FP64 implementations stops at fine spacing."""
-    N, G = forest.N, q // 2 + 1
-    W, N1 = N + 2 * G + 1, N + 1
-    wsum = {2: 4.0, 4: 16 / 3, 6: 1 / 45 + 3 / 10 + 3 + 49 / 18, 8: 2 * (1 / 560 + 8 / 315 + 1 / 5 + 8 / 5) + 205 / 72}[q]
-    w = work.reshape(forest.nblocks, 20, W, W, W)
-    out = np.zeros((forest.nblocks, N1, N1, N1))
-    for b in range(forest.nblocks):
-        h = forest.h0 / 2 ** int(forest.level[b])
-        own = w[b, :, G:G + N1, G:G + N1, G:G + N1]
-        out[b] = 8 * np.finfo(float).eps * wsum * np.max(np.abs(own), axis=0) / h ** 2
-    return out
-
-
 def rhs_error(du_gpu, du_ref, scale, forest):
     """max over points of max_v |du_gpu - du_ref| / rhs_scale."""
     N1 = forest.N + 1

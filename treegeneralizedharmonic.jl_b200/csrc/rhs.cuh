@@ -13,6 +13,8 @@
 //   MODE_STAGE  the RK4 stage update in place of du: acc and the next stage's ghosted
 //               working array are written, u_n read (the batched form)
 #pragma once
+#include <type_traits>
+
 #include "algebra.cuh"
 #include "tangent.cuh"
 
@@ -67,9 +69,10 @@ template <> __device__ __forceinline__ Tan ld<Tan>(const double* p) { return Tan
 // a value that carries no tangent (the sampled gauge source, the matter term)
 template <class T> __device__ __forceinline__ T ldk(const double* p) { return T(__ldg(p)); }
 
-// The stencils. With T = double (and its tangent) the sums are the reference's, term by term.
-// With T = float (the mixed form) every difference of state values is formed in FP64, where
-// it cancels, and rounded once; the weighted sum then runs in FP32. The symmetric stencils use
+// The stencils. With T = double the second differences are the reference's sums, term by
+// term (below); the first differences and the dissipation pair the taps at +-k. With
+// T = float (the mixed form) every difference of state values is formed in FP64, where it
+// cancels, and rounded once; the weighted sum then runs in FP32. The symmetric stencils use
 // that their weights sum to zero: w_0 c + sum_k w_k (u_k + u_-k) = sum_k w_k ((u_k - c) + (u_-k - c)).
 template <class T> __host__ __device__ constexpr bool is_fp32() { return sizeof(T) == sizeof(float); }
 
@@ -83,8 +86,50 @@ template <int Q, class T> __device__ __forceinline__ T st_d1(const double* p, lo
   }
   return acc;
 }
+// The first-derivative weight at a signed offset (the table holds k > 0; d1(-k) = -d1(k) exactly).
+template <int Q> __device__ __forceinline__ constexpr double d1s(int k) { return k > 0 ? W<Q>::d1(k) : -W<Q>::d1(-k); }
+
+// The second differences in FP64 are the reference's sums term by term (axis_stencil and
+// mixed_stencil, src/evolution.jl:192-219): from the lowest offset to the highest, each
+// product and each sum rounded on its own (no fused multiply-add), so that they are the
+// reference's bits. Their terms are O(|u|) and their value O(h^2 |u''|), so any other order
+// or rounding differs by eps |u| / h^2, which at fine spacing is above 1e-12 of the right-hand
+// side's scale. Terms of zero weight (the centre of a first-derivative table) are exact zeros
+// there and are left out. The first differences and the dissipation, whose rounding is scaled
+// by 1/h only, keep the paired form with fused multiply-adds.
+template <int Q> __device__ __forceinline__ double st_d2_ref(const double* p, long s, double c) {
+  constexpr int R = W<Q>::R;
+  double acc = __dmul_rn(W<Q>::d2(R), __ldg(p - R * s));
+#pragma unroll
+  for (int k = -R + 1; k <= R; ++k) {
+    const double u = k == 0 ? c : __ldg(p + k * s);
+    acc = __dadd_rn(acc, __dmul_rn(W<Q>::d2(k < 0 ? -k : k), u));
+  }
+  return acc;
+}
+// outer sum along s1, inner along s2
+template <int Q> __device__ __forceinline__ double st_mixed_ref(const double* p, long s1, long s2) {
+  constexpr int R = W<Q>::R;
+  double outer = 0.0;
+#pragma unroll
+  for (int a = -R; a <= R; ++a) {
+    if (a == 0) continue;
+    const double* pa = p + a * s1;
+    double in = __dmul_rn(d1s<Q>(-R), __ldg(pa - R * s2));
+#pragma unroll
+    for (int e = -R + 1; e <= R; ++e) {
+      if (e == 0) continue;
+      in = __dadd_rn(in, __dmul_rn(d1s<Q>(e), __ldg(pa + e * s2)));
+    }
+    outer = a == -R ? __dmul_rn(d1s<Q>(a), in) : __dadd_rn(outer, __dmul_rn(d1s<Q>(a), in));
+  }
+  return outer;
+}
+
 template <int Q, class T> __device__ __forceinline__ T st_d2(const double* p, long s, T c) {
-  if constexpr (!is_fp32<T>()) {
+  if constexpr (std::is_same<T, double>::value) {
+    return st_d2_ref<Q>(p, s, c);
+  } else if constexpr (!is_fp32<T>()) {
     T acc = T(W<Q>::d2(0)) * c;
 #pragma unroll
     for (int k = 1; k <= W<Q>::R; ++k) acc = fma(T(W<Q>::d2(k)), ld<T>(p + k * s) + ld<T>(p - k * s), acc);
@@ -115,6 +160,7 @@ template <int Q, class T> __device__ __forceinline__ T st_ko(const double* p, lo
 }
 // d_1 d_2 as the tensor product of two first-derivative stencils
 template <int Q, class T> __device__ __forceinline__ T st_mixed(const double* p, long s1, long s2) {
+  if constexpr (std::is_same<T, double>::value) return st_mixed_ref<Q>(p, s1, s2);
   T acc = T(0.0);
 #pragma unroll
   for (int a = 1; a <= W<Q>::R; ++a) {

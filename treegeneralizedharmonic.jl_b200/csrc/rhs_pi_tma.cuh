@@ -278,6 +278,9 @@ __global__ void __launch_bounds__(pitma::THREADS)
         hx[2 * t] = q.x;
         hx[2 * t + 1] = q.y;
       }
+      // first differences paired at +-k with fused multiply-adds, second differences as the
+      // reference's sums term by term (st_d2_ref, st_mixed_ref: lowest offset first, every
+      // product and sum rounded on its own), so that they carry the reference's bits
       double hcen[2], hd1x[2], hd2x[2];
 #pragma unroll
       for (int e = 0; e < 2; ++e) {
@@ -287,28 +290,41 @@ __global__ void __launch_bounds__(pitma::THREADS)
 #pragma unroll
         for (int kx = 1; kx <= SR; ++kx) a = fma(W<4>::d1(kx), u[kx] - u[-kx], a);
         hd1x[e] = a;
-        double c = W<4>::d2(0) * u[0];
+        double c = __dmul_rn(W<4>::d2(SR), u[-SR]);
 #pragma unroll
-        for (int kx = 1; kx <= SR; ++kx) c = fma(W<4>::d2(kx), u[kx] + u[-kx], c);
+        for (int kx = -SR + 1; kx <= SR; ++kx) c = __dadd_rn(c, __dmul_rn(W<4>::d2(kx < 0 ? -kx : kx), u[kx]));
         hd2x[e] = c;
       }
       double hd1y[2] = {0, 0}, hd1z[2] = {0, 0}, hd2y[2], hd2z[2];
-      hd2y[0] = hd2z[0] = W<4>::d2(0) * hcen[0];
-      hd2y[1] = hd2z[1] = W<4>::d2(0) * hcen[1];
+      {
+        double2 ry[2 * SR + 1], rz[2 * SR + 1];  // rows y + k and planes z + k, k = -SR .. SR
 #pragma unroll
-      for (int kt = 1; kt <= SR; ++kt) {
-        const double2 a = *reinterpret_cast<const double2*>(hc + kt * s2x);
-        const double2 c = *reinterpret_cast<const double2*>(hc - kt * s2x);
-        const double2 d = *reinterpret_cast<const double2*>(hc + kt * s3h);
-        const double2 f = *reinterpret_cast<const double2*>(hc - kt * s3h);
-        hd1y[0] = fma(W<4>::d1(kt), a.x - c.x, hd1y[0]);
-        hd1y[1] = fma(W<4>::d1(kt), a.y - c.y, hd1y[1]);
-        hd1z[0] = fma(W<4>::d1(kt), d.x - f.x, hd1z[0]);
-        hd1z[1] = fma(W<4>::d1(kt), d.y - f.y, hd1z[1]);
-        hd2y[0] = fma(W<4>::d2(kt), a.x + c.x, hd2y[0]);
-        hd2y[1] = fma(W<4>::d2(kt), a.y + c.y, hd2y[1]);
-        hd2z[0] = fma(W<4>::d2(kt), d.x + f.x, hd2z[0]);
-        hd2z[1] = fma(W<4>::d2(kt), d.y + f.y, hd2z[1]);
+        for (int k = -SR; k <= SR; ++k) {
+          if (k == 0) continue;
+          ry[k + SR] = *reinterpret_cast<const double2*>(hc + k * s2x);
+          rz[k + SR] = *reinterpret_cast<const double2*>(hc + k * s3h);
+        }
+        ry[SR] = rz[SR] = make_double2(hcen[0], hcen[1]);
+#pragma unroll
+        for (int kt = 1; kt <= SR; ++kt) {
+          hd1y[0] = fma(W<4>::d1(kt), ry[SR + kt].x - ry[SR - kt].x, hd1y[0]);
+          hd1y[1] = fma(W<4>::d1(kt), ry[SR + kt].y - ry[SR - kt].y, hd1y[1]);
+          hd1z[0] = fma(W<4>::d1(kt), rz[SR + kt].x - rz[SR - kt].x, hd1z[0]);
+          hd1z[1] = fma(W<4>::d1(kt), rz[SR + kt].y - rz[SR - kt].y, hd1z[1]);
+        }
+        const double wR = W<4>::d2(SR);
+        hd2y[0] = __dmul_rn(wR, ry[0].x);
+        hd2y[1] = __dmul_rn(wR, ry[0].y);
+        hd2z[0] = __dmul_rn(wR, rz[0].x);
+        hd2z[1] = __dmul_rn(wR, rz[0].y);
+#pragma unroll
+        for (int k = -SR + 1; k <= SR; ++k) {
+          const double wk = W<4>::d2(k < 0 ? -k : k);
+          hd2y[0] = __dadd_rn(hd2y[0], __dmul_rn(wk, ry[k + SR].x));
+          hd2y[1] = __dadd_rn(hd2y[1], __dmul_rn(wk, ry[k + SR].y));
+          hd2z[0] = __dadd_rn(hd2z[0], __dmul_rn(wk, rz[k + SR].x));
+          hd2z[1] = __dadd_rn(hd2z[1], __dmul_rn(wk, rz[k + SR].y));
+        }
       }
 #pragma unroll
       for (int e = 0; e < 2; ++e) {
@@ -320,48 +336,61 @@ __global__ void __launch_bounds__(pitma::THREADS)
         a = fma(c[CF_AYY], hd2y[e], a);
         p2[e] = fma(c[CF_AZZ], hd2z[e], a);
       }
-      // mixed x-y and x-z: per offset row (plane) three loads give x - 2 .. x + 3 for both points
-      double mxy[2] = {0, 0}, mxz[2] = {0, 0}, myz[2] = {0, 0};
+      // mixed x-y and x-z: outer sum over the x offsets a, inner over the y rows (z planes)
+      // e; each row (plane) e, from three loads, serves every a of both points
+      double mxy[2], mxz[2], myz[2];
 #pragma unroll
-      for (int a = 1; a <= SR; ++a) {
-        double inxy[2] = {0, 0}, inxz[2] = {0, 0}, inyz[2] = {0, 0};
+      for (int pl = 0; pl < 2; ++pl) {
+        const long se = pl == 0 ? s2x : s3h;
+        double in[2][2 * SR];  // [point][a = -SR .. -1, 1 .. SR]
 #pragma unroll
-        for (int ee = 1; ee <= SR; ++ee) {
-          // x-y: rows +-ee, x offsets +-a (first axis x, second y, as st_mixed(p, s1, s2))
-          double rp[6], rm[6], zpv[6], zmv[6];
+        for (int e = -SR; e <= SR; ++e) {
+          if (e == 0) continue;
+          double r[6];  // x - 2 .. x + 3 of row (plane) e
 #pragma unroll
           for (int t = 0; t < 3; ++t) {
-            const double2 q1 = *reinterpret_cast<const double2*>(hc - 2 + 2 * t + ee * s2x);
-            const double2 q2 = *reinterpret_cast<const double2*>(hc - 2 + 2 * t - ee * s2x);
-            const double2 q3 = *reinterpret_cast<const double2*>(hc - 2 + 2 * t + ee * s3h);
-            const double2 q4 = *reinterpret_cast<const double2*>(hc - 2 + 2 * t - ee * s3h);
-            rp[2 * t] = q1.x; rp[2 * t + 1] = q1.y;
-            rm[2 * t] = q2.x; rm[2 * t + 1] = q2.y;
-            zpv[2 * t] = q3.x; zpv[2 * t + 1] = q3.y;
-            zmv[2 * t] = q4.x; zmv[2 * t + 1] = q4.y;
+            const double2 q = *reinterpret_cast<const double2*>(hc - 2 + 2 * t + e * se);
+            r[2 * t] = q.x;
+            r[2 * t + 1] = q.y;
           }
+          const double we = d1s<4>(e);
 #pragma unroll
-          for (int e = 0; e < 2; ++e) {
-            const int o = 2 + e;
-            const double dxy = (rp[o + a] - rm[o + a]) - (rp[o - a] - rm[o - a]);
-            const double dxz = (zpv[o + a] - zmv[o + a]) - (zpv[o - a] - zmv[o - a]);
-            inxy[e] = fma(W<4>::d1(ee), dxy, inxy[e]);
-            inxz[e] = fma(W<4>::d1(ee), dxz, inxz[e]);
-          }
-          // y-z: rows +-a, planes +-ee
-          const double2 c1 = *reinterpret_cast<const double2*>(hc + a * s2x + ee * s3h);
-          const double2 c2 = *reinterpret_cast<const double2*>(hc + a * s2x - ee * s3h);
-          const double2 c3 = *reinterpret_cast<const double2*>(hc - a * s2x + ee * s3h);
-          const double2 c4 = *reinterpret_cast<const double2*>(hc - a * s2x - ee * s3h);
-          inyz[0] = fma(W<4>::d1(ee), (c1.x - c2.x) - (c3.x - c4.x), inyz[0]);
-          inyz[1] = fma(W<4>::d1(ee), (c1.y - c2.y) - (c3.y - c4.y), inyz[1]);
+          for (int pt = 0; pt < 2; ++pt)
+#pragma unroll
+            for (int ia = 0; ia < 2 * SR; ++ia) {
+              const int a = ia < SR ? ia - SR : ia - SR + 1;
+              const double term = __dmul_rn(we, r[2 + pt + a]);
+              in[pt][ia] = e == -SR ? term : __dadd_rn(in[pt][ia], term);
+            }
         }
 #pragma unroll
-        for (int e = 0; e < 2; ++e) {
-          mxy[e] = fma(W<4>::d1(a), inxy[e], mxy[e]);
-          mxz[e] = fma(W<4>::d1(a), inxz[e], mxz[e]);
-          myz[e] = fma(W<4>::d1(a), inyz[e], myz[e]);
+        for (int pt = 0; pt < 2; ++pt) {
+          double o = __dmul_rn(d1s<4>(-SR), in[pt][0]);
+#pragma unroll
+          for (int ia = 1; ia < 2 * SR; ++ia) {
+            const int a = ia < SR ? ia - SR : ia - SR + 1;
+            o = __dadd_rn(o, __dmul_rn(d1s<4>(a), in[pt][ia]));
+          }
+          if (pl == 0) mxy[pt] = o;
+          else mxz[pt] = o;
         }
+      }
+      // mixed y-z: outer sum over the y rows a, inner over the z planes e
+#pragma unroll
+      for (int a = -SR; a <= SR; ++a) {
+        if (a == 0) continue;
+        double in0 = 0.0, in1 = 0.0;
+#pragma unroll
+        for (int e = -SR; e <= SR; ++e) {
+          if (e == 0) continue;
+          const double2 q = *reinterpret_cast<const double2*>(hc + a * s2x + e * s3h);
+          const double t0 = __dmul_rn(d1s<4>(e), q.x), t1 = __dmul_rn(d1s<4>(e), q.y);
+          in0 = e == -SR ? t0 : __dadd_rn(in0, t0);
+          in1 = e == -SR ? t1 : __dadd_rn(in1, t1);
+        }
+        const double o0 = __dmul_rn(d1s<4>(a), in0), o1 = __dmul_rn(d1s<4>(a), in1);
+        myz[0] = a == -SR ? o0 : __dadd_rn(myz[0], o0);
+        myz[1] = a == -SR ? o1 : __dadd_rn(myz[1], o1);
       }
 #pragma unroll
       for (int e = 0; e < 2; ++e) {
