@@ -58,6 +58,36 @@ def test_rhs_matches_oracle(tgh, oracle, row):
     assert err < RHS_TOL, f"{name}: {err}"
 
 
+@pytest.mark.parametrize("n32", [False, True])
+def test_second_differences_are_the_references_sums_at_fine_spacing(tgh, oracle, n32):
+    """A Kerr-Schild hole's exterior at h = 1/2048 (r ~ 1.6): a second difference's rounding,
+    eps |u| sum|w| / h^2, is ~6e-10 of rhs_scale there, so a summation order or rounding other
+    than the reference's (axis_stencil, mixed_stencil, src/evolution.jl:192-219) would miss the
+    1e-12 bound by orders of magnitude. Blocks of 8^3 (the general kernels) and of 32^3 (the
+    N = 32 kernels: the one-point Pi kernel and the TMA-staged one)."""
+    c = tgh.kerr_schild_case(M=1.0, a=0.7, halfwidth=4.0, r0=0.8, r1=1.3, gauge="algebraic")
+    N = 32 if n32 else 8
+    leaves = sorted((0, (x, y, z)) for z in (0, N) for y in (0, N) for x in (0, N))
+    f = tgh.Forest(N, (1.5, 0.3, 0.2), 1.0 / 2048, (2 * N, 2 * N, 2 * N), (False, False, False),
+                   np.array([l for l, _ in leaves], dtype=np.int32),
+                   np.array([c_ for _, c_ in leaves], dtype=np.int32))
+    P = tgh.GHProblem(c, f, 4, margin_check=False)
+    O = oracle.problem(c, f, 4)
+    u = O.initial_state(O.statevector(), 0.0) + tgh.perturbation(f, amplitude=1e-9, seed=3)
+    du_ref = np.zeros(O.L)
+    O.gh_rhs(du_ref, u, 0.0)
+    scale = rhs_scale(O.work(), f, 4)
+    ug = _to_gpu(u)
+    for pi in ("l1", "tma") if n32 else ("l1",):
+        P.set_variant(pi=pi)
+        dug = torch.full_like(ug, float("nan"))
+        P.gh_rhs(dug, ug, 0.0)
+        torch.cuda.synchronize()
+        err = rhs_error(dug.cpu().numpy(), du_ref, scale, f)
+        assert err < RHS_TOL, (pi, err)
+    P.close()
+
+
 def test_matter_source_matches_oracle(tgh, oracle):
     c = tgh.gauge_wave_case(eps_ko=0.5, gamma0=1.0, gamma2=-0.5)
     f = tgh.gh_forest(c, 8, 2)
