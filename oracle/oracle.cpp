@@ -1455,6 +1455,18 @@ int orc_weights_double(int q, int m, double* out) {
   for (size_t i = 0; i < d.size(); ++i) out[i] = d[i];
   return (int)d.size();
 }
+// The right-hand side's stencil sums on a caller's array, for the tests that pin their order:
+// which 1 = first derivative, 2 = second derivative, 0 = dissipation (axis_stencil at `base`
+// along `stride`); orc_mixed_stencil is the first-derivative tensor product, outer along s1.
+double orc_axis_stencil(int q, int which, const double* data, long base, long stride) {
+  const Stencils st(q);
+  const std::vector<double>& w = which == 1 ? st.w1 : which == 2 ? st.w2 : st.wD;
+  return axis_stencil<double>(w, data, (size_t)base, stride);
+}
+double orc_mixed_stencil(int q, const double* data, long base, long s1, long s2) {
+  const Stencils st(q);
+  return mixed_stencil<double>(st.w1, data, (size_t)base, s1, s2);
+}
 // out: g4[16], gu4[16], alpha, beta[3], gamu[9], sqrtg
 void orc_metric_quantities(const double* h, double* out) {
   Coef<double> C;

@@ -66,6 +66,8 @@ class Oracle:
             "orc_weights": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_int64),
                                            ctypes.POINTER(ctypes.c_int64)]),
             "orc_weights_double": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, _DP]),
+            "orc_axis_stencil": (_D, [ctypes.c_int, ctypes.c_int, _DP, ctypes.c_long, ctypes.c_long]),
+            "orc_mixed_stencil": (_D, [ctypes.c_int, _DP, ctypes.c_long, ctypes.c_long, ctypes.c_long]),
             "orc_metric_quantities": (None, [_DP, _DP]),
             "orc_source": (None, [ctypes.c_int, _DP, _DP, _DP, _DP, _DP, _D, _D, _DP]),
             "orc_divergences": (None, [ctypes.c_int, _DP, _DP, _DP]),
@@ -137,6 +139,13 @@ class Oracle:
         out = np.zeros(16)
         n = self.lib.orc_weights_double(q, m, _dp(out))
         return out[:n]
+
+    def axis_stencil(self, q, which, data, base, stride):
+        """The oracle's stencil sum (which: 1 first, 2 second derivative, 0 dissipation)."""
+        return float(self.lib.orc_axis_stencil(q, which, _dp(data), int(base), int(stride)))
+
+    def mixed_stencil(self, q, data, base, s1, s2):
+        return float(self.lib.orc_mixed_stencil(q, _dp(data), int(base), int(s1), int(s2)))
 
     def metric_quantities(self, h):
         out = np.zeros(46)
